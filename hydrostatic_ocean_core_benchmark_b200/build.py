@@ -1,0 +1,75 @@
+"""Build the sm_100a library ``lib/libocean_b200.so`` and the ``bin/ocean3d5_b200``
+executable in-tree with nvcc (cross-compiles without a GPU).
+
+FP contraction is disabled (``-fmad=false``, ``-ffp-contract=off``): the step is
+bit-for-bit equal to the reference's NumPy arithmetic only when every multiply
+and add rounds separately.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+LIB_DIR = PKG / "lib"
+BIN_DIR = PKG / "bin"
+LIB = LIB_DIR / "libocean_b200.so"
+EXE = BIN_DIR / "ocean3d5_b200"
+SOURCES = ["step_kernels.cu", "helmholtz.cu", "capi.cu", "protocol.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--extended-lambda",
+         "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{ROOT / 'include'}", f"-I{CSRC}"]
+
+
+def nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "ocean_b200.h",
+                                                                      CSRC / "ocean3d5_main.cpp"]
+    if not force and not _stale(LIB, deps) and not _stale(EXE, deps):
+        return LIB
+    LIB_DIR.mkdir(exist_ok=True)
+    BIN_DIR.mkdir(exist_ok=True)
+    obj_dir = PKG / "_build"
+    obj_dir.mkdir(exist_ok=True)
+    objs = []
+    cc = nvcc()
+    for src in SOURCES:
+        obj = obj_dir / (Path(src).stem + ".o")
+        cmd = [cc, *ARCH, *FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
+        if src.endswith(".cpp"):
+            cmd = [cc, *FLAGS, "-x", "c++", "-c", str(CSRC / src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(str(obj))
+    tmp = LIB.with_suffix(".so.tmp")
+    subprocess.run([cc, *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
+    os.replace(tmp, LIB)
+    subprocess.run([cc, *FLAGS, "-x", "c++", str(CSRC / "ocean3d5_main.cpp"), "-o", str(EXE),
+                    f"-L{LIB_DIR}", "-locean_b200", "-Xlinker", "-rpath,$ORIGIN/../lib", "-lcudart"],
+                   check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(LIB)

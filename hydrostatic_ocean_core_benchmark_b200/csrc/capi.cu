@@ -1,0 +1,840 @@
+// C ABI of the ocean-core step: handle, geometry, state, step orchestration.
+//
+// The step follows reference libs/core/model3d_v05.py Stepper3DV05.step
+// (lines 337-415; split-explicit 417-463; tracers 466-533) as a fixed
+// sequence of fused column kernels plus one persistent Helmholtz solve per
+// Picard iteration; state lives in ping-pong buffers so no step ever copies a
+// 3D field.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "helmholtz.cuh"
+#include "oc_internal.cuh"
+#include "ocean_b200.h"
+#include "step_kernels.cuh"
+
+namespace oc {
+
+__global__ void k_fill(double* a, double v, int64_t n) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) a[t] = v;
+}
+
+__global__ void k_absmax_partial(const double* a, int64_t n, double* part) {
+    __shared__ double sh[256];
+    double m = 0.0;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const double x = fabs(a[t]);
+        if (!(x <= m)) m = x;
+    }
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) {
+            const double x = sh[threadIdx.x + k];
+            if (!(x <= sh[threadIdx.x])) sh[threadIdx.x] = x;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+static void fill(double* a, double v, int64_t n, cudaStream_t s) {
+    if (n > 0) k_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, v, n);
+}
+
+}  // namespace oc
+
+using namespace oc;
+
+struct oc_handle {
+    oc_config cfg{};
+    std::string err;
+    bool has_domain = false, has_state = false;
+    KP P{};
+    int nx = 0, ny = 0, nz = 0;
+    size_t n2 = 0, n3 = 0, n3i = 0;
+    double h_max = 0.0;
+    int n_split = 0;
+    // host geometry (for oc_get_field and the stress fields)
+    std::vector<double> H, mask, mask_u, mask_v, dzr, dz3, mask3, mask3u, mask3v, dz3u, dz3v, zc;
+    std::vector<double> taux_c, tauy_c;
+    bool stress_field = false;
+    // device memory
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    double *d_H = nullptr, *d_mask = nullptr, *d_mask_u = nullptr, *d_mask_v = nullptr;
+    double *d_tau_u = nullptr, *d_tau_v = nullptr, *d_ustar2 = nullptr;
+    double *U[2] = {}, *V[2] = {}, *B[2] = {}, *Tt[2] = {}, *Ss[2] = {}, *ETA[2] = {};
+    int cur = 0;
+    double *e = nullptr, *km = nullptr, *kh = nullptr, *q = nullptr, *w = nullptr;
+    double *phi = nullptr, *pgx = nullptr, *pgy = nullptr, *avpv = nullptr, *avpu = nullptr;
+    double *dzu = nullptr, *dzv = nullptr, *stu = nullptr, *stv = nullptr;
+    double *ghu = nullptr, *ghv = nullptr, *uit = nullptr, *vit = nullptr;
+    double *Ku = nullptr, *Kv = nullptr, *gx2 = nullptr, *gy2 = nullptr, *Uold = nullptr,
+           *Vold = nullptr, *div_old = nullptr, *Ug = nullptr, *Vg = nullptr, *rhs2 = nullptr;
+    double *bt[12] = {};  // split-explicit 2D work
+    double* d_part = nullptr;
+    int* d_status = nullptr;
+    HelmSolver* solver = nullptr;
+    // host counters (model3d_v05.py:89-94)
+    long long steps = 0, tridiag = 0, rebuilds = 0, substeps = 0, solves = 0;
+    cudaStream_t last_stream = nullptr;
+};
+
+namespace {
+
+int fail(oc_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_fail(oc_handle* h, cudaError_t e, const char* where) {
+    return fail(h, OC_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+double* dalloc(oc_handle* h, size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMalloc(&p, n * sizeof(double)) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, n * sizeof(double));
+    h->allocs.push_back(p);
+    h->bytes += n * sizeof(double);
+    return (double*)p;
+}
+
+int check_launch(oc_handle* h, const char* where) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(h, e, where);
+    return OC_OK;
+}
+
+int validate(const oc_config* c, std::string& err) {
+    if (c->nx < 1 || c->ny < 1 || c->nz < 1) return err = "nx, ny, nz must be >= 1", OC_ERR_ARG;
+    if (c->nz > OC_MAXNZ) return err = "nz above the supported maximum of 128", OC_ERR_UNSUPPORTED;
+    if (!(c->lx > 0.0) || !(c->ly > 0.0)) return err = "lx, ly must be > 0", OC_ERR_ARG;
+    if (c->scheme < 0 || c->scheme > 2) return err = "unknown scheme (expected fb|theta|split_explicit)", OC_ERR_ARG;
+    if (c->scheme == OC_SCHEME_THETA && !(c->theta > 0.0 && c->theta <= 1.0))
+        return err = "theta must lie in (0,1]", OC_ERR_ARG;
+    if (c->n_picard < 1) return err = "n_picard must be >= 1", OC_ERR_ARG;
+    if (!(c->dt > 0.0)) return err = "dt must be > 0", OC_ERR_ARG;
+    if (c->solver < 0 || c->solver > 3) return err = "unknown Helmholtz solver", OC_ERR_ARG;
+    if (c->max_iter < 1) return err = "max_iter must be >= 1", OC_ERR_ARG;
+    if (c->bc_x < 0 || c->bc_x > 1 || c->bc_y < 0 || c->bc_y > 1)
+        return err = "bc must be periodic|closed (open boundaries are not supported)", OC_ERR_UNSUPPORTED;
+    if (c->face_rule < 0 || c->face_rule > 2) return err = "face_rule must be min|mean|harmonic", OC_ERR_ARG;
+    if (c->eos < 0 || c->eos > 2) return err = "eos must be linear|seos|teos10", OC_ERR_ARG;
+    if (c->pgf < 0 || c->pgf > 1) return err = "pgf must be remove|keep", OC_ERR_ARG;
+    if (c->advection < 0 || c->advection > 4) return err = "unknown advection scheme", OC_ERR_ARG;
+    if (c->tracers < 0 || c->tracers > 1) return err = "tracers must be buoyancy|TS", OC_ERR_ARG;
+    if (c->closure < 0 || c->closure > 1) return err = "closure must be none|tke", OC_ERR_ARG;
+    if (c->mxl < 0 || c->mxl > 1) return err = "mxl must be integral|recursive", OC_ERR_ARG;
+    if (c->barotropic_average < 0 || c->barotropic_average > 1)
+        return err = "barotropic_average must be none|mean", OC_ERR_ARG;
+    return OC_OK;
+}
+
+// scalar constants of the step, formed in the reference's operation order
+void fill_scalars(oc_handle* h) {
+    const oc_config& c = h->cfg;
+    KP& P = h->P;
+    P.nx = c.nx;
+    P.ny = c.ny;
+    P.nz = c.nz;
+    P.n2 = c.nx * c.ny;
+    P.n3 = P.n2 * c.nz;
+    P.n3i = P.n2 * (c.nz + 1);
+    P.dx = c.lx / c.nx;
+    P.dy = c.ly / c.ny;
+    P.eos = c.eos;
+    P.pgf_remove = c.pgf == OC_PGF_REMOVE;
+    P.pgf_correction = c.pgf_correction != 0;
+    P.advection = c.advection;
+    P.tracers_ts = c.tracers == OC_TRACERS_TS;
+    P.closure_tke = c.closure == OC_CLOSURE_TKE;
+    P.mxl_recursive = c.mxl == OC_MXL_RECURSIVE;
+    P.scheme = c.scheme;
+    P.face_rule = c.face_rule;
+    P.dt = c.dt;
+    P.g = c.g;
+    P.f0 = c.f0;
+    P.rho0 = c.rho0;
+    P.N2 = c.n2;
+    P.nu = c.nu;
+    P.kappa = c.kappa;
+    P.bottom_drag = c.bottom_drag;
+    P.a_h = c.a_h;
+    P.k_h = c.k_h;
+    P.alpha_t = c.alpha_t;
+    P.beta_s = c.beta_s;
+    P.t0 = c.t0;
+    P.s0 = c.s0;
+    P.c_k = c.c_k;
+    P.c_eps = c.c_eps;
+    P.pr_t = c.pr_t;
+    P.z_0 = c.z_0;
+    P.e_min = c.e_min;
+    P.l_min = c.l_min;
+    P.e_bb = c.e_bb;
+    P.n2_min = c.n2_min;
+    const double th = (c.scheme == OC_SCHEME_THETA) ? c.theta : 0.0;
+    P.theta = th;
+    P.theta_cor = c.theta_cor;
+    P.theta_v = c.theta_v;
+    P.thv_dt = c.theta_v * c.dt;
+    P.thv_dt_drag = (c.theta_v * c.dt) * c.bottom_drag;
+    P.thv_dt_zero = (c.theta_v * c.dt) * 0.0;
+    P.c1 = (c.g * c.dt) * (1.0 - th);
+    P.c2 = (c.g * c.dt) * th;
+    P.c3 = (1.0 - c.theta_v) * c.dt;
+    P.one_m_tc = 1.0 - c.theta_cor;
+    P.one_m_th = 1.0 - th;
+    P.neg_f0 = -c.f0;
+    P.neg_g = -c.g;
+    P.neg_n2 = -c.n2;
+    P.dz_nom = c.h0 / c.nz;
+    P.flux_t = c.q_heat / (c.rho0 * c.cp);
+    P.flux_s = c.q_salt;
+    const double kap = 1.0 / 3.0;
+    P.one_m_kappa3 = 1.0 - kap;
+    P.one_p_kappa3 = 1.0 + kap;
+}
+
+double face_host(int rule, double a, double b) {
+    if (rule == 0) return std::min(a, b);
+    if (rule == 1) return 0.5 * (a + b);
+    const double tot = a + b;
+    return tot > 0.0 ? 2.0 * a * b / tot : 0.0;
+}
+
+// host geometry, same operations as the device's on-the-fly form
+// (reference domain.py:60-154)
+void build_host_geometry(oc_handle* h) {
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    const size_t n2 = h->n2, n3 = h->n3;
+    const KP& P = h->P;
+    h->dz3.assign(n3, 0.0);
+    h->mask3.assign(n3, 0.0);
+    for (int k = 0; k < nz; ++k)
+        for (size_t c = 0; c < n2; ++c) {
+            const double rem = h->H[c] - P.edge[k];
+            double dz = std::min(std::max(rem, 0.0), P.dzr[k]);
+            if (dz > 0.0 && dz < P.thin[k]) dz = 0.0;
+            const double m3 = (dz > 0.0 ? 1.0 : 0.0) * h->mask[c];
+            h->dz3[k * n2 + c] = dz * m3;
+            h->mask3[k * n2 + c] = m3;
+        }
+    h->mask3u.assign(n3, 0.0);
+    h->mask3v.assign(n3, 0.0);
+    h->dz3u.assign(n3, 0.0);
+    h->dz3v.assign(n3, 0.0);
+    h->zc.assign(n3, 0.0);
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const size_t c = (size_t)j * nx + i, o = k * n2;
+                const size_t ce = (size_t)j * nx + (i + 1) % nx, cn = (size_t)((j + 1) % ny) * nx + i;
+                h->mask3u[o + c] = h->mask3[o + c] * h->mask3[o + ce] * h->mask_u[c];
+                h->mask3v[o + c] = h->mask3[o + c] * h->mask3[o + cn] * h->mask_v[c];
+                h->dz3u[o + c] = h->mask3u[o + c] * face_host(P.face_rule, h->dz3[o + c], h->dz3[o + ce]);
+                h->dz3v[o + c] = h->mask3v[o + c] * face_host(P.face_rule, h->dz3[o + c], h->dz3[o + cn]);
+            }
+    for (size_t c = 0; c < n2; ++c) {
+        double above = 0.0;
+        for (int k = 0; k < nz; ++k) {
+            h->zc[k * n2 + c] = above + 0.5 * h->dz3[k * n2 + c];
+            above = (k == 0) ? h->dz3[c] : above + h->dz3[k * n2 + c];
+        }
+    }
+}
+
+// surface stress at the faces and u*^2 (model3d_v05.py:176, 355-356; field form
+// reduces to it for a uniform field)
+int upload_stress(oc_handle* h) {
+    const int nx = h->nx, ny = h->ny;
+    const size_t n2 = h->n2;
+    const oc_config& c = h->cfg;
+    std::vector<double> tu(n2), tv(n2), us(n2);
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const size_t k = (size_t)j * nx + i;
+            const size_t ke = (size_t)j * nx + (i + 1) % nx, kn = (size_t)((j + 1) % ny) * nx + i;
+            if (!h->stress_field) {
+                tu[k] = (c.tau_x / c.rho0) * h->mask3u[k];
+                tv[k] = (c.tau_y / c.rho0) * h->mask3v[k];
+                us[k] = std::hypot(c.tau_x, c.tau_y) / c.rho0;
+            } else {
+                tu[k] = (0.5 * (h->taux_c[k] + h->taux_c[ke])) / c.rho0 * h->mask3u[k];
+                tv[k] = (0.5 * (h->tauy_c[k] + h->tauy_c[kn])) / c.rho0 * h->mask3v[k];
+                us[k] = std::hypot(h->taux_c[k], h->tauy_c[k]) / c.rho0;
+            }
+        }
+    cudaMemcpy(h->d_tau_u, tu.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_tau_v, tv.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
+    const cudaError_t e = cudaMemcpy(h->d_ustar2, us.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(h, e, "stress upload");
+    return OC_OK;
+}
+
+// q, Ku, Kv and the Helmholtz levels for the current K_m (model3d_v05.py:141-167)
+int build_coefficients(oc_handle* h, cudaStream_t s, bool count_rebuild) {
+    launch_qsolve(h->P, h->km, h->q, s);
+    h->tridiag += 1;
+    launch_kukv(h->P, h->q, h->Ku, h->Kv, s);
+    if (h->solver) {
+        h->solver->rebuild(s);
+        if (count_rebuild) h->rebuilds += 1;
+    }
+    return check_launch(h, "coefficients");
+}
+
+int ensure_log(oc_handle* h, long long needed, cudaStream_t s) {
+    if (!h->solver) return OC_OK;
+    if (needed <= h->solver->log_capacity()) return OC_OK;
+    long long cap = h->solver->log_capacity();
+    while (cap < needed) cap *= 2;
+    return h->solver->grow_log((int)std::min<long long>(cap, 1 << 30), s, h->err);
+}
+
+// one step (model3d_v05.py:337-415)
+int step_once(oc_handle* h, cudaStream_t s) {
+    const oc_config& c = h->cfg;
+    const KP& P = h->P;
+    const int cur = h->cur, nxt = 1 - cur;
+    double *u = h->U[cur], *v = h->V[cur], *b = h->B[cur], *eta = h->ETA[cur];
+    double *un = h->U[nxt], *vn = h->V[nxt], *etan = h->ETA[nxt];
+    const bool theta = c.scheme == OC_SCHEME_THETA, split = c.scheme == OC_SCHEME_SPLIT;
+    if (c.closure == OC_CLOSURE_TKE) {
+        launch_closure(P, u, v, b, h->e, h->km, h->kh, h->q, s);
+        h->tridiag += 2;
+        launch_kukv(P, h->q, h->Ku, h->Kv, s);
+        if (theta) {
+            h->solver->rebuild(s);
+            h->rebuilds += 1;
+        }
+    }
+    launch_wcol(P, u, v, h->w, s);
+    launch_phi(P, b, h->phi, s);
+    launch_mom_explicit(P, u, v, b, h->phi, h->w, h->km, h->pgx, h->pgy, h->avpv, h->avpu, h->dzu,
+                        h->dzv, h->stu, h->stv, s);
+    if (!split) launch_grad2(P, eta, h->gx2, h->gy2, s);
+    if (theta) {
+        launch_transport(P, u, v, h->Uold, h->Vold, s);
+        launch_div2(P, h->Uold, h->Vold, h->div_old, s);
+    }
+    if (split) launch_transport(P, u, v, h->bt[0], h->bt[1], s);  // U0, V0
+    const double *uit = u, *vit = v;
+    double *last_gu = nullptr, *last_gv = nullptr;
+    for (int m = 0; m < c.n_picard; ++m) {
+        const bool last = m == c.n_picard - 1;
+        double *tu, *tv;
+        if (theta) {
+            tu = h->ghu;
+            tv = h->ghv;
+        } else if (last && !split) {
+            tu = un;
+            tv = vn;
+        } else {
+            tu = (m % 2 == 0) ? h->ghu : h->uit;
+            tv = (m % 2 == 0) ? h->ghv : h->vit;
+        }
+        launch_predictor(P, u, v, uit, vit, h->pgx, h->pgy, h->avpv, h->avpu, h->dzu, h->dzv, h->stu,
+                         h->stv, h->gx2, h->gy2, h->km, tu, tv, h->Ug, h->Vg, s);
+        h->tridiag += 2;
+        if (theta) {
+            launch_helm_rhs(P, eta, h->div_old, h->Ug, h->Vg, h->rhs2, s);
+            int rc = ensure_log(h, h->solves + 1, s);
+            if (rc) return rc;
+            rc = h->solver->solve(h->rhs2, etan, s, h->err);
+            if (rc) return rc;
+            h->solves += 1;
+            double* ou = last ? un : h->uit;
+            double* ov = last ? vn : h->vit;
+            launch_backsub(P, h->ghu, h->ghv, h->q, etan, ou, ov, s);
+            uit = ou;
+            vit = ov;
+        } else {
+            uit = tu;
+            vit = tv;
+            last_gu = tu;
+            last_gv = tv;
+        }
+    }
+    if (c.scheme == OC_SCHEME_FB) launch_eta_fb(P, eta, h->Ug, h->Vg, etan, s);
+    if (split) {
+        double *U0 = h->bt[0], *V0 = h->bt[1], *fx = h->bt[2], *fy = h->bt[3];
+        double *avv = h->bt[4], *avu = h->bt[5], *gxe = h->bt[6], *gye = h->bt[7];
+        double* Ub[3] = {h->bt[8], h->bt[10], h->Uold};
+        double* Vb[3] = {h->bt[9], h->bt[11], h->Vold};
+        double *accu = h->gx2, *accv = h->gy2;
+        launch_split_forcing(P, U0, V0, h->Ug, h->Vg, fx, fy, s);
+        cudaMemcpyAsync(etan, eta, h->n2 * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(Ub[0], U0, h->n2 * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(Vb[0], V0, h->n2 * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        const double ddt = c.dt / h->n_split;
+        int ib = 0;
+        for (int n = 0; n < h->n_split; ++n) {
+            launch_split_sub_avg(P, Ub[ib], Vb[ib], etan, avv, avu, gxe, gye, s);
+            int ii = ib;
+            for (int qi = 0; qi < c.n_picard; ++qi) {
+                int io = 0;
+                while (io == ib || io == ii) ++io;
+                launch_split_sub_mom(P, ddt, Ub[ib], Vb[ib], Ub[ii], Vb[ii], avv, avu, gxe, gye, h->Ku,
+                                     h->Kv, fx, fy, Ub[io], Vb[io], s);
+                ii = io;
+            }
+            ib = ii;
+            launch_split_sub_eta(P, ddt, Ub[ib], Vb[ib], etan, accu, accv, n == 0 ? 1 : 0, s);
+        }
+        h->substeps += h->n_split;
+        const double *Uf = Ub[ib], *Vf = Vb[ib];
+        if (c.barotropic_average == OC_BTAVG_MEAN) {
+            launch_split_mean(P, h->n_split, accu, accv, s);
+            Uf = accu;
+            Vf = accv;
+        }
+        launch_split_correct(P, last_gu, last_gv, h->Ug, h->Vg, Uf, Vf, un, vn, s);
+    }
+    launch_wcol(P, un, vn, h->w, s);
+    launch_tracers(P, h->Tt[cur], h->Ss[cur], b, un, vn, h->w, h->kh, h->Tt[nxt], h->Ss[nxt], h->B[nxt],
+                   s);
+    h->tridiag += (c.tracers == OC_TRACERS_TS) ? 2 : 1;
+    h->cur = nxt;
+    h->steps += 1;
+    return check_launch(h, "step");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* oc_version(void) { return "ocean_b200 1.0 (sm_100a, fp64, bit-parity with the NumPy reference)"; }
+
+int oc_create(const oc_config* cfg, oc_handle** out) {
+    if (!cfg || !out) return OC_ERR_ARG;
+    *out = nullptr;
+    std::string err;
+    const int rc = validate(cfg, err);
+    if (rc) {
+        std::fprintf(stderr, "oc_create: %s\n", err.c_str());
+        return rc;
+    }
+    cudaError_t e = cudaSetDevice(cfg->device);
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "oc_create: cudaSetDevice(%d): %s\n", cfg->device, cudaGetErrorString(e));
+        return OC_ERR_CUDA;
+    }
+    oc_handle* h = new oc_handle();
+    h->cfg = *cfg;
+    h->nx = cfg->nx;
+    h->ny = cfg->ny;
+    h->nz = cfg->nz;
+    h->n2 = (size_t)cfg->nx * cfg->ny;
+    h->n3 = h->n2 * cfg->nz;
+    h->n3i = h->n2 * (cfg->nz + 1);
+    fill_scalars(h);
+    *out = h;
+    return OC_OK;
+}
+
+int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const double* dzrh) {
+    if (!h || !Hh || !maskh) return fail(h, OC_ERR_ARG, "H and mask are required");
+    if (h->has_domain) return fail(h, OC_ERR_STATE, "the domain is already set");
+    cudaSetDevice(h->cfg.device);
+    const int nx = h->nx, ny = h->ny, nz = h->nz;
+    const size_t n2 = h->n2;
+    h->H.assign(Hh, Hh + n2);
+    h->mask.assign(maskh, maskh + n2);
+    bool any_wet = false;
+    double hmax = 0.0;
+    for (size_t c = 0; c < n2; ++c) {
+        if (h->mask[c] > 0.0) {
+            if (!(h->H[c] > 0.0)) return fail(h, OC_ERR_ARG, "bathymetry must be positive in every wet cell");
+            hmax = any_wet ? std::max(hmax, h->H[c]) : h->H[c];
+            any_wet = true;
+        }
+    }
+    if (!any_wet) return fail(h, OC_ERR_ARG, "the domain has no wet cell");
+    h->h_max = hmax;
+    h->mask_u.assign(n2, 0.0);
+    h->mask_v.assign(n2, 0.0);
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const size_t c = (size_t)j * nx + i;
+            h->mask_u[c] = h->mask[c] * h->mask[(size_t)j * nx + (i + 1) % nx];
+            h->mask_v[c] = h->mask[c] * h->mask[(size_t)((j + 1) % ny) * nx + i];
+            if (h->cfg.bc_x != OC_BC_PERIODIC && i == nx - 1) h->mask_u[c] = 0.0;
+            if (h->cfg.bc_y != OC_BC_PERIODIC && j == ny - 1) h->mask_v[c] = 0.0;
+        }
+    h->dzr.assign(nz, hmax / nz);
+    if (dzrh) {
+        for (int k = 0; k < nz; ++k) {
+            if (!(dzrh[k] > 0.0)) return fail(h, OC_ERR_ARG, "level thicknesses must be > 0");
+            h->dzr[k] = dzrh[k];
+        }
+    }
+    KP& P = h->P;
+    P.edge[0] = 0.0;
+    for (int k = 0; k < nz; ++k) {
+        P.edge[k + 1] = (k == 0) ? h->dzr[0] : P.edge[k] + h->dzr[k];
+        P.dzr[k] = h->dzr[k];
+        P.thin[k] = h->cfg.min_partial * h->dzr[k];
+    }
+    build_host_geometry(h);
+    if (h->cfg.scheme == OC_SCHEME_SPLIT) {
+        const double cc = std::sqrt(h->cfg.g * hmax);
+        const double dt_baro = 1.0 / (cc * std::sqrt(1.0 / std::pow(P.dx, 2.0) + 1.0 / std::pow(P.dy, 2.0)));
+        h->n_split = h->cfg.n_split > 0 ? h->cfg.n_split
+                                        : std::max(1, (int)std::ceil(1.2 * h->cfg.dt / dt_baro));
+        if (h->cfg.dt / h->n_split > dt_baro)
+            return fail(h, OC_ERR_ARG, "n_split leaves a barotropic substep above the gravity-wave limit");
+    }
+    // device buffers
+    const size_t n3 = h->n3, n3i = h->n3i;
+    h->d_H = dalloc(h, n2);
+    h->d_mask = dalloc(h, n2);
+    h->d_mask_u = dalloc(h, n2);
+    h->d_mask_v = dalloc(h, n2);
+    h->d_tau_u = dalloc(h, n2);
+    h->d_tau_v = dalloc(h, n2);
+    h->d_ustar2 = dalloc(h, n2);
+    const bool ts = h->cfg.tracers == OC_TRACERS_TS;
+    for (int t = 0; t < 2; ++t) {
+        h->U[t] = dalloc(h, n3);
+        h->V[t] = dalloc(h, n3);
+        h->B[t] = dalloc(h, n3);
+        h->Tt[t] = ts ? dalloc(h, n3) : nullptr;
+        h->Ss[t] = ts ? dalloc(h, n3) : nullptr;
+        h->ETA[t] = dalloc(h, n2);
+    }
+    h->e = dalloc(h, n3i);
+    h->km = dalloc(h, n3i);
+    h->kh = dalloc(h, n3i);
+    h->w = dalloc(h, n3i);
+    for (double** p : {&h->q, &h->phi, &h->pgx, &h->pgy, &h->avpv, &h->avpu, &h->dzu, &h->dzv, &h->stu,
+                       &h->stv, &h->ghu, &h->ghv, &h->uit, &h->vit})
+        *p = dalloc(h, n3);
+    for (double** p : {&h->Ku, &h->Kv, &h->gx2, &h->gy2, &h->Uold, &h->Vold, &h->div_old, &h->Ug, &h->Vg,
+                       &h->rhs2})
+        *p = dalloc(h, n2);
+    for (int t = 0; t < 12; ++t) h->bt[t] = (h->cfg.scheme == OC_SCHEME_SPLIT) ? dalloc(h, n2) : nullptr;
+    h->d_part = dalloc(h, 1024);
+    {
+        void* st = nullptr;
+        if (cudaMalloc(&st, sizeof(int)) != cudaSuccess) return fail(h, OC_ERR_CUDA, "cudaMalloc failed");
+        cudaMemset(st, 0, sizeof(int));
+        h->allocs.push_back(st);
+        h->d_status = (int*)st;
+    }
+    for (void* p : h->allocs)
+        if (!p) return fail(h, OC_ERR_CUDA, "device allocation failed");
+    if (!h->km || !h->ETA[1] || !h->rhs2) return fail(h, OC_ERR_CUDA, "device allocation failed");
+    cudaMemcpy(h->d_H, h->H.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_mask, h->mask.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_mask_u, h->mask_u.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_mask_v, h->mask_v.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
+    P.H = h->d_H;
+    P.mask = h->d_mask;
+    P.mask_u = h->d_mask_u;
+    P.mask_v = h->d_mask_v;
+    P.tau_u = h->d_tau_u;
+    P.tau_v = h->d_tau_v;
+    P.ustar2 = h->d_ustar2;
+    int rc = upload_stress(h);
+    if (rc) return rc;
+    fill(h->e, h->cfg.e_min, (int64_t)n3i, 0);
+    fill(h->km, h->cfg.nu, (int64_t)n3i, 0);
+    fill(h->kh, h->cfg.kappa, (int64_t)n3i, 0);
+    if (h->cfg.scheme == OC_SCHEME_THETA) {
+        h->solver = new HelmSolver();
+        const double coef = h->cfg.g * std::pow(h->cfg.theta, 2.0) * std::pow(h->cfg.dt, 2.0);
+        rc = h->solver->init(nx, ny, h->cfg.lx, h->cfg.ly, coef, h->cfg.solver, h->cfg.rtol,
+                             h->cfg.max_iter, h->mask.data(), h->Ku, h->Kv, 4096, h->d_status, h->err);
+        if (rc) return rc;
+    }
+    rc = build_coefficients(h, 0, false);
+    if (rc) return rc;
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(h, e, "oc_set_domain");
+    h->has_domain = true;
+    return OC_OK;
+}
+
+int oc_set_forcing(oc_handle* h, const double* taux_c, const double* tauy_c) {
+    if (!h) return OC_ERR_ARG;
+    if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain before the forcing");
+    cudaSetDevice(h->cfg.device);
+    if (!taux_c && !tauy_c) {
+        h->stress_field = false;
+    } else {
+        h->stress_field = true;
+        h->taux_c.assign(h->n2, 0.0);
+        h->tauy_c.assign(h->n2, 0.0);
+        if (taux_c) h->taux_c.assign(taux_c, taux_c + h->n2);
+        if (tauy_c) h->tauy_c.assign(tauy_c, tauy_c + h->n2);
+    }
+    return upload_stress(h);
+}
+
+static int copy_in(double* dst, const double* src, size_t n, int on_device, cudaStream_t s) {
+    return cudaMemcpyAsync(dst, src, n * sizeof(double),
+                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s) == cudaSuccess
+               ? 0
+               : 1;
+}
+
+int oc_set_state(oc_handle* h, const oc_state_view* s, int32_t on_device) {
+    if (!h || !s) return OC_ERR_ARG;
+    if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain before the state");
+    if (!s->eta || !s->u || !s->v) return fail(h, OC_ERR_ARG, "eta, u and v are required");
+    const bool ts = h->cfg.tracers == OC_TRACERS_TS;
+    if (ts && (!s->T || !s->S)) return fail(h, OC_ERR_ARG, "T and S are required with TS tracers");
+    if (!ts && !s->b) return fail(h, OC_ERR_ARG, "b is required with buoyancy tracers");
+    cudaSetDevice(h->cfg.device);
+    cudaStream_t st = 0;
+    const int c = h->cur;
+    int bad = 0;
+    bad |= copy_in(h->ETA[c], s->eta, h->n2, on_device, st);
+    bad |= copy_in(h->U[c], s->u, h->n3, on_device, st);
+    bad |= copy_in(h->V[c], s->v, h->n3, on_device, st);
+    if (ts) {
+        bad |= copy_in(h->Tt[c], s->T, h->n3, on_device, st);
+        bad |= copy_in(h->Ss[c], s->S, h->n3, on_device, st);
+    }
+    if (s->b)
+        bad |= copy_in(h->B[c], s->b, h->n3, on_device, st);
+    else
+        launch_diag_buoyancy(h->P, h->Tt[c], h->Ss[c], h->B[c], st);
+    if (s->e)
+        bad |= copy_in(h->e, s->e, h->n3i, on_device, st);
+    else
+        fill(h->e, h->cfg.e_min, (int64_t)h->n3i, st);
+    if (s->km) bad |= copy_in(h->km, s->km, h->n3i, on_device, st);
+    if (s->kh) bad |= copy_in(h->kh, s->kh, h->n3i, on_device, st);
+    if (bad) return fail(h, OC_ERR_CUDA, "state copy failed");
+    if (s->km) {
+        // coefficients of the given viscosity (model3d_v05.py:141-167)
+        launch_qsolve(h->P, h->km, h->q, st);
+        launch_kukv(h->P, h->q, h->Ku, h->Kv, st);
+        if (h->solver) h->solver->rebuild(st);
+    }
+    const cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(h, e, "oc_set_state");
+    h->has_state = true;
+    return OC_OK;
+}
+
+int oc_reset_mixing(oc_handle* h) {
+    if (!h) return OC_ERR_ARG;
+    if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain first");
+    cudaSetDevice(h->cfg.device);
+    fill(h->km, h->cfg.nu, (int64_t)h->n3i, 0);
+    fill(h->kh, h->cfg.kappa, (int64_t)h->n3i, 0);
+    launch_qsolve(h->P, h->km, h->q, 0);
+    launch_kukv(h->P, h->q, h->Ku, h->Kv, 0);
+    if (h->solver) h->solver->rebuild(0);
+    const cudaError_t e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? OC_OK : cuda_fail(h, e, "oc_reset_mixing");
+}
+
+static int device_status(oc_handle* h) {
+    int st = 0;
+    cudaMemcpy(&st, h->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    return st;
+}
+
+int oc_get_state(oc_handle* h, const oc_state_view* s, int32_t on_device) {
+    if (!h || !s) return OC_ERR_ARG;
+    if (!h->has_state) return fail(h, OC_ERR_STATE, "no state has been set");
+    cudaSetDevice(h->cfg.device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(h, e, "oc_get_state");
+    const int dst = device_status(h);
+    if (dst) return fail(h, dst, "a device-side wait ran out its bound");
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const int c = h->cur;
+    const bool ts = h->cfg.tracers == OC_TRACERS_TS;
+    struct {
+        double* dst;
+        const double* src;
+        size_t n;
+    } items[] = {{s->eta, h->ETA[c], h->n2}, {s->u, h->U[c], h->n3},   {s->v, h->V[c], h->n3},
+                 {s->b, h->B[c], h->n3},     {ts ? s->T : nullptr, h->Tt[c], h->n3},
+                 {ts ? s->S : nullptr, h->Ss[c], h->n3}, {s->e, h->e, h->n3i},
+                 {s->km, h->km, h->n3i},     {s->kh, h->kh, h->n3i}};
+    for (auto& it : items) {
+        if (!it.dst || !it.src) continue;
+        e = cudaMemcpy(it.dst, it.src, it.n * sizeof(double), kind);
+        if (e != cudaSuccess) return cuda_fail(h, e, "oc_get_state copy");
+    }
+    return OC_OK;
+}
+
+int oc_step(oc_handle* h, int32_t n_steps, void* stream) {
+    if (!h) return OC_ERR_ARG;
+    if (!h->has_state) return fail(h, OC_ERR_STATE, "set the state before stepping");
+    if (n_steps < 0) return fail(h, OC_ERR_ARG, "n_steps must be >= 0");
+    cudaSetDevice(h->cfg.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    h->last_stream = s;
+    for (int n = 0; n < n_steps; ++n) {
+        const int rc = step_once(h, s);
+        if (rc) return rc;
+    }
+    return OC_OK;
+}
+
+int oc_get_stats(oc_handle* h, oc_stats* out) {
+    if (!h || !out) return OC_ERR_ARG;
+    cudaSetDevice(h->cfg.device);
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(h, e, "oc_get_stats");
+    std::memset(out, 0, sizeof(*out));
+    out->steps = h->steps;
+    out->tridiagonal_solves = h->tridiag;
+    out->solver_rebuilds = h->rebuilds;
+    out->barotropic_substeps = h->substeps;
+    out->solves = h->solves;
+    out->n_split = h->n_split;
+    out->n_levels = h->solver ? h->solver->n_levels() : 0;
+    out->device_bytes = (int64_t)(h->bytes + (h->solver ? h->solver->bytes() : 0));
+    out->device_status = h->has_domain ? device_status(h) : 0;
+    if (h->solver && h->solves > 0) {
+        const int n = (int)std::min<long long>(h->solves, h->solver->log_capacity());
+        std::vector<int> it(n), cv(n);
+        cudaMemcpy(it.data(), h->solver->d_log_iters(), n * sizeof(int), cudaMemcpyDeviceToHost);
+        cudaMemcpy(cv.data(), h->solver->d_log_conv(), n * sizeof(int), cudaMemcpyDeviceToHost);
+        for (int k = 0; k < n; ++k) {
+            out->solver_iterations += std::max(0, it[k]);
+            out->solver_failures += cv[k] ? 0 : 1;
+        }
+    }
+    if (h->has_state) {
+        const int c = h->cur;
+        oc::k_absmax_partial<<<64, 256>>>(h->ETA[c], (int64_t)h->n2, h->d_part);
+        double part[64];
+        cudaMemcpy(part, h->d_part, sizeof(part), cudaMemcpyDeviceToHost);
+        double m = 0.0;
+        for (double x : part)
+            if (!(x <= m)) m = x;
+        out->diverged = !(m < 1.0e6);
+    }
+    return out->device_status ? fail(h, out->device_status, "a device-side wait ran out its bound") : OC_OK;
+}
+
+int oc_get_solve_log(oc_handle* h, int32_t* iterations, int32_t capacity, int32_t* n_out) {
+    if (!h || !n_out) return OC_ERR_ARG;
+    cudaSetDevice(h->cfg.device);
+    cudaDeviceSynchronize();
+    const int n = h->solver ? (int)std::min<long long>(h->solves, h->solver->log_capacity()) : 0;
+    *n_out = n;
+    if (iterations && capacity > 0 && n > 0)
+        cudaMemcpy(iterations, h->solver->d_log_iters(), std::min(n, capacity) * sizeof(int),
+                   cudaMemcpyDeviceToHost);
+    return OC_OK;
+}
+
+int oc_reset_stats(oc_handle* h) {
+    if (!h) return OC_ERR_ARG;
+    cudaSetDevice(h->cfg.device);
+    cudaDeviceSynchronize();
+    h->steps = h->tridiag = h->rebuilds = h->substeps = h->solves = 0;
+    if (h->solver) cudaMemset(h->solver->d_log_count(), 0, sizeof(int));
+    return OC_OK;
+}
+
+int oc_helmholtz_solve(oc_handle* h, const double* rhs, double* x, int32_t* iterations, void* stream) {
+    if (!h || !rhs || !x) return OC_ERR_ARG;
+    if (!h->solver) return fail(h, OC_ERR_STATE, "the Helmholtz solver exists for the theta scheme only");
+    cudaSetDevice(h->cfg.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = ensure_log(h, h->solves + 1, s);
+    if (rc) return rc;
+    rc = h->solver->solve(rhs, x, s, h->err);
+    if (rc) return rc;
+    const long long idx = h->solves;
+    h->solves += 1;
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "oc_helmholtz_solve");
+    const int dst = device_status(h);
+    if (dst) return fail(h, dst, "a device-side wait ran out its bound");
+    if (iterations) {
+        cudaMemcpy(iterations, h->solver->d_log_iters() + idx, sizeof(int), cudaMemcpyDeviceToHost);
+    }
+    return OC_OK;
+}
+
+int oc_thomas(const double* sub, const double* diag, const double* sup, const double* rhs, double* x,
+              int32_t n, int32_t ncols, void* stream) {
+    if (!sub || !diag || !sup || !rhs || !x || n < 1 || ncols < 1) return OC_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    double* cstar = nullptr;
+    if (cudaMallocAsync(&cstar, (size_t)n * ncols * sizeof(double), s) != cudaSuccess) return OC_ERR_CUDA;
+    launch_thomas(sub, diag, sup, rhs, x, cstar, n, ncols, s);
+    cudaFreeAsync(cstar, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? OC_OK : OC_ERR_CUDA;
+}
+
+int oc_buoyancy(oc_handle* h, const double* T, const double* S, const double* z, double* b, int64_t count,
+                void* stream) {
+    if (!h || !T || !S || !z || !b || count < 0) return OC_ERR_ARG;
+    cudaSetDevice(h->cfg.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    launch_buoyancy_flat(h->P, T, S, z, b, count, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? OC_OK : cuda_fail(h, e, "oc_buoyancy");
+}
+
+int oc_get_field(oc_handle* h, const char* name, double* out, int64_t count) {
+    if (!h || !name || !out) return OC_ERR_ARG;
+    if (!h->has_domain) return fail(h, OC_ERR_STATE, "no domain");
+    cudaSetDevice(h->cfg.device);
+    const std::string n(name);
+    const std::vector<double>* src = nullptr;
+    if (n == "dz3") src = &h->dz3;
+    else if (n == "mask3") src = &h->mask3;
+    else if (n == "mask3u") src = &h->mask3u;
+    else if (n == "mask3v") src = &h->mask3v;
+    else if (n == "dz3u") src = &h->dz3u;
+    else if (n == "dz3v") src = &h->dz3v;
+    else if (n == "zc") src = &h->zc;
+    else if (n == "mask_u") src = &h->mask_u;
+    else if (n == "mask_v") src = &h->mask_v;
+    if (src) {
+        if ((size_t)count != src->size()) return fail(h, OC_ERR_ARG, "wrong element count for " + n);
+        std::memcpy(out, src->data(), src->size() * sizeof(double));
+        return OC_OK;
+    }
+    const double* d = nullptr;
+    size_t cnt = 0;
+    if (n == "q") d = h->q, cnt = h->n3;
+    else if (n == "ku") d = h->Ku, cnt = h->n2;
+    else if (n == "kv") d = h->Kv, cnt = h->n2;
+    if (!d) return fail(h, OC_ERR_ARG, "unknown field " + n);
+    if ((size_t)count != cnt) return fail(h, OC_ERR_ARG, "wrong element count for " + n);
+    cudaDeviceSynchronize();
+    const cudaError_t e = cudaMemcpy(out, d, cnt * sizeof(double), cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? OC_OK : cuda_fail(h, e, "oc_get_field");
+}
+
+const char* oc_last_error(const oc_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+void oc_destroy(oc_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->cfg.device);
+    cudaDeviceSynchronize();
+    delete h->solver;
+    for (void* p : h->allocs) cudaFree(p);
+    delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,77 @@
+// Variable-coefficient free-surface Helmholtz solver, A = I - c D[K G[.]].
+#pragma once
+
+#include <vector>
+
+#include "oc_internal.cuh"
+
+namespace oc {
+
+enum { HK_PCG_JACOBI = 0, HK_PCG_RBGS = 1, HK_RBGS = 2, HK_MULTIGRID = 3 };
+
+struct HLevel {
+    int nx, ny, n;
+    double dx2, dy2;  // dx**2, dy**2 of the level
+    double cx, cy;    // coef * (1 / dx**2)
+    const double* mask;
+    double* Ku;
+    double* Kv;
+    double* inv_diag;
+    double* x;
+    double* b;
+};
+
+struct HelmParams {
+    int n_levels, kind, max_iter, coarse_from;
+    double coef, rtol;
+    HLevel lv[OC_MAX_LEVELS];
+    double *r, *z, *p, *Ap;  // level-0 work vectors
+    const double* rhs;
+    // NumPy pairwise-summation plan of the level-0 vectors
+    int n_leaves;
+    const int* leaf_start;    // n_leaves + 1
+    int n_heights;
+    const int* height_start;  // n_heights + 1 offsets into ops
+    const int2* ops;          // (lo, mid): value[lo] += value[mid]
+    double* leafA;
+    double* leafB;
+    // grid barrier and status
+    unsigned* bar_count;
+    unsigned* bar_gen;
+    int* status;
+    // per-solve log
+    int* log_iters;
+    int* log_conv;
+    int* log_count;
+    int log_cap;
+};
+
+class HelmSolver {
+   public:
+    ~HelmSolver();
+    // Ku/Kv/mask are device arrays of the fine level owned by the caller.
+    int init(int nx, int ny, double lx, double ly, double coef, int kind, double rtol, int max_iter,
+             const double* mask_host, double* Ku, double* Kv, int log_cap, int* status,
+             std::string& err);
+    // recompute coarse coefficients and inverse diagonals after Ku/Kv changed
+    void rebuild(cudaStream_t s);
+    // x = A^-1 rhs on the device, iteration count appended to the log
+    int solve(const double* rhs, double* x, cudaStream_t s, std::string& err);
+    int n_levels() const { return hp_.n_levels; }
+    int log_capacity() const { return hp_.log_cap; }
+    int* d_log_iters() const { return hp_.log_iters; }
+    int* d_log_conv() const { return hp_.log_conv; }
+    int* d_log_count() const { return hp_.log_count; }
+    int grow_log(int cap, cudaStream_t s, std::string& err);
+    size_t bytes() const { return bytes_; }
+
+   private:
+    HelmParams hp_{};
+    std::vector<void*> allocs_;
+    int grid_ = 0, block_ = 512;
+    size_t smem_ = 0;
+    size_t bytes_ = 0;
+    void* dalloc(size_t nbytes);
+};
+
+}  // namespace oc

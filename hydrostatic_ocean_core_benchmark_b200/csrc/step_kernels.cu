@@ -1,0 +1,1384 @@
+// Column and stencil kernels of the ocean-core step (sm_100a, fp64).
+//
+// Each kernel maps one thread to one water column (i, j) and marches over the
+// levels k, so every vertical recurrence of the reference (cumulative sums,
+// Thomas sweeps, the closure's mixing-length marches) runs in registers and
+// local memory in the reference's order, while the 32 threads of a warp read
+// 32 consecutive i of each level plane (coalesced 256-byte rows).
+//
+// Reference correspondence (paths inside the reference project):
+//   k_closure        libs/core/closure.py:43-205 + model3d_v05.py:141-157 (q = A^-1 1)
+//   k_qsolve         model3d_v05.py:147-153 (constant-coefficient q)
+//   k_kukv           model3d_v05.py:154-157
+//   k_wcol           vertical_var.py:109-121 + model3d_v05.py:232-235
+//   k_phi            vertical_var.py:132-145
+//   k_mom_explicit   model3d_v05.py:195-230, 241-260, 352-370; advection_v06.py:77-108;
+//                    advection.py:62-95; operators_masked.py:45-68; vertical_var.py:80-106
+//   k_predictor      model3d_v05.py:387-395, 426-433 + vertical.py:17-44
+//   k_backsub        model3d_v05.py:404-406
+//   k_tracers        model3d_v05.py:466-533 + eos.py:68-133
+//   2D kernels       model3d_v05.py:290-335, 376-384, 396-400, 410-413, 440-461
+
+#include "oc_internal.cuh"
+#include "step_kernels.cuh"
+
+namespace oc {
+
+// ------------------------------------------------------------------ helpers
+
+// Row k of A = I - thv dt Dz for a column (reference vertical_var.py:35-77).
+__device__ __forceinline__ void implicit_row(const KP& P, int k, double dzk, double m3k, double m3k1,
+                                             double dzi_k, double dzi_k1, double Kk, double Kk1,
+                                             double thv_dt_drag, double& sub, double& diag,
+                                             double& sup) {
+    const double inv_dz = inv_pos(dzk);
+    const double fac = P.thv_dt * inv_dz;
+    const double at = fac * Kk * inv_pos(dzi_k);
+    const double ab = fac * Kk1 * inv_pos(dzi_k1);
+    sub = -at;
+    sup = -ab;
+    diag = 1.0 + at + ab;
+    if (k == 0) {
+        diag = 1.0 + ab;
+        sub = 0.0;
+    }
+    if (m3k > 0.0 && m3k1 == 0.0) {
+        diag = 1.0 + at + thv_dt_drag * inv_dz;
+        sup = 0.0;
+    }
+    if (m3k == 0.0) {
+        diag = 1.0;
+        sub = 0.0;
+        sup = 0.0;
+    }
+}
+
+struct Nbr {
+    int i, j, c;
+    int nx, ny;
+    __device__ __forceinline__ int at(int dj, int di) const {
+        return wrapi(j + dj, ny) * nx + wrapi(i + di, nx);
+    }
+};
+
+__device__ __forceinline__ CellGeo geo_off(const KP& P, const Nbr& n, int dj, int di, int k) {
+    return cell_geo(P, n.at(dj, di), k);
+}
+
+// east face of column (j+dj, i+di): wet mask and thickness at level k
+__device__ __forceinline__ void ufacek(const KP& P, const Nbr& n, int dj, int di, int k, double& m3f,
+                                       double& dzf) {
+    const CellGeo a = geo_off(P, n, dj, di, k), b = geo_off(P, n, dj, di + 1, k);
+    face_geo(P, a, b, P.mask_u[n.at(dj, di)], m3f, dzf);
+}
+
+// north face of column (j+dj, i+di)
+__device__ __forceinline__ void vfacek(const KP& P, const Nbr& n, int dj, int di, int k, double& m3f,
+                                       double& dzf) {
+    const CellGeo a = geo_off(P, n, dj, di, k), b = geo_off(P, n, dj + 1, di, k);
+    face_geo(P, a, b, P.mask_v[n.at(dj, di)], m3f, dzf);
+}
+
+__device__ __forceinline__ double m3u_at(const KP& P, const Nbr& n, int dj, int di, int k) {
+    double m, d;
+    ufacek(P, n, dj, di, k, m, d);
+    return m;
+}
+
+__device__ __forceinline__ double m3v_at(const KP& P, const Nbr& n, int dj, int di, int k) {
+    double m, d;
+    vfacek(P, n, dj, di, k, m, d);
+    return m;
+}
+
+__device__ __forceinline__ double m3_at(const KP& P, const Nbr& n, int dj, int di, int k) {
+    return geo_off(P, n, dj, di, k).m3;
+}
+
+#define COLUMN_PROLOGUE                                  \
+    const int i = blockIdx.x * blockDim.x + threadIdx.x; \
+    const int j = blockIdx.y * blockDim.y + threadIdx.y; \
+    if (i >= P.nx || j >= P.ny) return;                  \
+    Nbr nb;                                              \
+    nb.i = i;                                            \
+    nb.j = j;                                            \
+    nb.nx = P.nx;                                        \
+    nb.ny = P.ny;                                        \
+    nb.c = j * P.nx + i;                                 \
+    const size_t n2 = (size_t)P.n2;                      \
+    (void)n2;
+
+// ------------------------------------------------------------------ q = A^-1 1 on a column
+// Momentum tridiagonal with a unit right-hand side for the column's interface
+// viscosity km[0..nz] (reference model3d_v05.py:147-153).
+__device__ __forceinline__ void column_q(const KP& P, int nz, const double* dz, const double* m3,
+                                         const double* dzi, const double* kmc, double* cs, double* ds,
+                                         double* __restrict__ q_out, size_t c, size_t n2) {
+    for (int k = 0; k < nz; ++k) {
+        double sub, diag, sup;
+        const double m3k1 = (k + 1 < nz) ? m3[k + 1] : 0.0;
+        implicit_row(P, k, dz[k], m3[k], m3k1, dzi[k], dzi[k + 1], kmc[k], kmc[k + 1], P.thv_dt_drag,
+                     sub, diag, sup);
+        if (k == 0) {
+            cs[0] = sup / diag;
+            ds[0] = 1.0 / diag;
+        } else {
+            const double den = diag - sub * cs[k - 1];
+            cs[k] = sup / den;
+            ds[k] = (1.0 - sub * ds[k - 1]) / den;
+        }
+    }
+    double x = ds[nz - 1];
+    q_out[(size_t)(nz - 1) * n2 + c] = x;
+    for (int k = nz - 2; k >= 0; --k) {
+        x = ds[k] - cs[k] * x;
+        q_out[(size_t)k * n2 + c] = x;
+    }
+}
+
+// column geometry: thickness, wet mask and interface spacing (closure.py:43-62)
+template <int NZM>
+__device__ __forceinline__ void column_geometry(const KP& P, size_t c, double* dz, double* m3,
+                                                double* dzi, double& depth) {
+    const int nz = P.nz;
+    const double Hc = P.H[c], mc = P.mask[c];
+    depth = 0.0;
+    for (int k = 0; k < nz; ++k) {
+        dz[k] = cell_dz(P, Hc, mc, k, m3[k]);
+        depth = (k == 0) ? dz[0] : depth + dz[k];
+    }
+    dzi[0] = dz[0];
+    for (int k = 1; k < nz; ++k) dzi[k] = 0.5 * (dz[k - 1] + dz[k]);
+    dzi[nz] = dz[nz - 1];
+}
+
+template <int NZM>
+__global__ void __launch_bounds__(128) k_qsolve(KP P, const double* __restrict__ km,
+                                                double* __restrict__ q) {
+    COLUMN_PROLOGUE
+    const int nz = P.nz;
+    const size_t c = nb.c;
+    double dz[NZM], m3[NZM], dzi[NZM + 1], kmc[NZM + 1], cs[NZM], ds[NZM];
+    double depth;
+    column_geometry<NZM>(P, c, dz, m3, dzi, depth);
+    for (int k = 0; k <= nz; ++k) kmc[k] = km[(size_t)k * n2 + c];
+    column_q(P, nz, dz, m3, dzi, kmc, cs, ds, q, c, n2);
+}
+
+// ------------------------------------------------------------------ TKE closure
+// One thread per column: shear and N^2 on interfaces, the mixing lengths, the
+// implicit TKE tridiagonal (nz+1 rows), K_m/K_h, then q for the new K_m.
+template <int NZM>
+__global__ void __launch_bounds__(128) k_closure(KP P, const double* __restrict__ u,
+                                                 const double* __restrict__ v,
+                                                 const double* __restrict__ b,
+                                                 double* __restrict__ e, double* __restrict__ km,
+                                                 double* __restrict__ kh, double* __restrict__ q) {
+    COLUMN_PROLOGUE
+    const int nz = P.nz;
+    const size_t c = nb.c;
+    const size_t cw = nb.at(0, -1), cs_ = nb.at(-1, 0);
+    double dz[NZM], m3[NZM], dzi[NZM + 1], nn2[NZM + 1], sh2[NZM + 1], lk[NZM + 1], le[NZM + 1];
+    double cst[NZM + 1], dst[NZM + 1];
+    double depth;
+    column_geometry<NZM>(P, c, dz, m3, dzi, depth);
+    // shear^2 and N^2 on interfaces (closure.py:150-161)
+    double uc_prev = 0.0, vc_prev = 0.0, b_prev = 0.0;
+    for (int k = 0; k < nz; ++k) {
+        const size_t o = (size_t)k * n2;
+        const double uc = 0.5 * (u[o + c] + u[o + cw]);
+        const double vc = 0.5 * (v[o + c] + v[o + cs_]);
+        const double bk = b[o + c];
+        if (k >= 1) {
+            const double wk = m3[k - 1] * m3[k];
+            const double idz = inv_pos(dzi[k]);
+            const double du = (uc_prev - uc) * idz;
+            const double dv = (vc_prev - vc) * idz;
+            const double db = (b_prev - bk) * idz;
+            sh2[k] = (du * du + dv * dv) * wk;
+            nn2[k] = db * wk;
+        }
+        uc_prev = uc;
+        vc_prev = vc;
+        b_prev = bk;
+    }
+    sh2[0] = 0.0;
+    nn2[0] = 0.0;
+    sh2[nz] = 0.0;
+    nn2[nz] = 0.0;
+    // mixing lengths (closure.py:65-129)
+    double zi = 0.0;
+    for (int k = 0; k <= nz; ++k) {
+        if (k >= 1) zi = (k == 1) ? dz[0] : zi + dz[k - 1];
+        const double wk = (k >= 1 && k <= nz - 1) ? m3[k - 1] * m3[k] : 0.0;
+        const double zb = fmax(depth - zi, 0.0);
+        const double ek = fmax(e[(size_t)k * n2 + c], P.e_min);
+        if (!P.mxl_recursive) {
+            // march away from interface k until the energy budget is spent; once
+            // the budget is zero the reference's remaining steps add exactly 0
+            double lu = 0.0, bud = ek;
+            for (int kk = k - 1; kk >= 0 && bud > 0.0; --kk) {
+                const double n2j = fmax(nn2[kk], 0.0), dzj = dzi[kk];
+                const double cost = n2j * dzj * (lu + 0.5 * dzj);
+                const bool full = cost <= bud;
+                double step = dzj;
+                if (!full && n2j > 0.0) {
+                    const double part = sqrt(fmax(lu * lu + 2.0 * bud / n2j, 0.0)) - lu;
+                    step = fmin(fmax(part, 0.0), dzj);
+                }
+                lu = lu + step;
+                bud = full ? bud - cost : 0.0;
+            }
+            double ld = 0.0;
+            bud = ek;
+            for (int kk = k + 1; kk <= nz && bud > 0.0; ++kk) {
+                const double n2j = fmax(nn2[kk], 0.0), dzj = dzi[kk];
+                const double cost = n2j * dzj * (ld + 0.5 * dzj);
+                const bool full = cost <= bud;
+                double step = dzj;
+                if (!full && n2j > 0.0) {
+                    const double part = sqrt(fmax(ld * ld + 2.0 * bud / n2j, 0.0)) - ld;
+                    step = fmin(fmax(part, 0.0), dzj);
+                }
+                ld = ld + step;
+                bud = full ? bud - cost : 0.0;
+            }
+            lu = fmin(lu, zi + P.z_0) * wk;
+            ld = fmin(ld, zb + P.z_0) * wk;
+            lk[k] = fmax(P.l_min, sqrt(lu * ld));
+            le[k] = fmax(P.l_min, fmin(lu, ld));
+        } else {
+            const double n2c = fmax(nn2[k], P.n2_min);
+            const double ell = sqrt(2.0 * ek / n2c);
+            le[k] = fmin(ell, fmin(zi + P.z_0, zb + P.z_0));
+        }
+    }
+    if (P.mxl_recursive) {
+        for (int k = 1; k <= nz; ++k) le[k] = fmin(le[k], le[k - 1] + dzi[k]);
+        for (int k = nz - 1; k >= 0; --k) le[k] = fmin(le[k], le[k + 1] + dzi[k + 1]);
+        for (int k = 0; k <= nz; ++k) {
+            const double wk = (k >= 1 && k <= nz - 1) ? m3[k - 1] * m3[k] : 0.0;
+            const double ell = le[k] * wk;
+            lk[k] = fmax(P.l_min, sqrt(ell * ell));
+            le[k] = fmax(P.l_min, fmin(ell, ell));
+        }
+    }
+    // implicit TKE rows and forward sweep (closure.py:171-198)
+    double rhs0 = 0.0;
+    double km_prev = 0.0, km_cur = km[c];
+    for (int k = 0; k <= nz; ++k) {
+        const size_t o = (size_t)k * n2 + c;
+        const double km_next = (k < nz) ? km[o + n2] : 0.0;
+        const double wk = (k >= 1 && k <= nz - 1) ? m3[k - 1] * m3[k] : 0.0;
+        const double e_old = e[o];
+        const double prod = (km_cur - P.nu) * sh2[k] - (kh[o] - P.kappa) * nn2[k];
+        const double diss = P.c_eps * sqrt(fmax(e_old, P.e_min)) / le[k];
+        double a_up = 0.0, a_dn = 0.0;
+        if (k >= 1 && k <= nz - 1) {
+            const double idzi = inv_pos(dzi[k]);
+            a_up = P.dt * (0.5 * (km_prev + km_cur)) * inv_pos(dz[k - 1]) * idzi;
+            a_dn = P.dt * (0.5 * (km_cur + km_next)) * inv_pos(dz[k]) * idzi;
+        }
+        double sub = -a_up, sup = -a_dn;
+        double diag = 1.0 + a_up + a_dn + P.dt * diss;
+        double rhs = e_old + P.dt * prod;
+        if (wk <= 0.0) {
+            diag = 1.0;
+            sub = 0.0;
+            sup = 0.0;
+            rhs = P.e_min;
+        }
+        if (k == 0) {
+            rhs = (m3[0] > 0.0) ? P.e_bb * P.ustar2[c] : P.e_min;
+            rhs0 = rhs;
+            cst[0] = sup / diag;
+            dst[0] = rhs / diag;
+        } else {
+            const double den = diag - sub * cst[k - 1];
+            cst[k] = sup / den;
+            dst[k] = (rhs - sub * dst[k - 1]) / den;
+        }
+        km_prev = km_cur;
+        km_cur = km_next;
+    }
+    // back substitution, e/K update (closure.py:198-205)
+    double x = 0.0;
+    for (int k = nz; k >= 0; --k) {
+        x = (k == nz) ? dst[nz] : dst[k] - cst[k] * x;
+        const double wk = (k >= 1 && k <= nz - 1) ? m3[k - 1] * m3[k] : 0.0;
+        double en = fmax(x, P.e_min);
+        en = (wk > 0.0) ? en : P.e_min;
+        if (k == 0) en = rhs0;
+        const double kmn = P.c_k * lk[k] * sqrt(en) * wk + P.nu;
+        const double khn = (kmn - P.nu) / P.pr_t + P.kappa;
+        const size_t o = (size_t)k * n2 + c;
+        e[o] = en;
+        km[o] = kmn;
+        kh[o] = khn;
+        lk[k] = kmn;
+    }
+    column_q(P, nz, dz, m3, dzi, lk, cst, dst, q, c, n2);
+}
+
+// ------------------------------------------------------------------ Ku, Kv
+// Ku = sum_k dz3u * min(q, q_east) * mask_u (model3d_v05.py:154-157)
+__global__ void k_kukv(KP P, const double* __restrict__ q, double* __restrict__ Ku,
+                       double* __restrict__ Kv) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c;
+    const size_t ce = nb.at(0, 1), cn = nb.at(1, 0);
+    double su = 0.0, sv = 0.0;
+    for (int k = 0; k < P.nz; ++k) {
+        const size_t o = (size_t)k * n2;
+        double m3f, dzf;
+        ufacek(P, nb, 0, 0, k, m3f, dzf);
+        const double tu = dzf * fmin(q[o + c], q[o + ce]);
+        vfacek(P, nb, 0, 0, k, m3f, dzf);
+        const double tv = dzf * fmin(q[o + c], q[o + cn]);
+        su = (k == 0) ? tu : su + tu;
+        sv = (k == 0) ? tv : sv + tv;
+    }
+    Ku[c] = su * P.mask_u[c];
+    Kv[c] = sv * P.mask_v[c];
+}
+
+// ------------------------------------------------------------------ w from transport divergence
+// w[k] = -sum_{k'>=k} div(dz3u u, dz3v v)[k'], accumulated from the bottom
+// (vertical_var.py:109-121); w[nz] = 0.
+__global__ void k_wcol(KP P, const double* __restrict__ u, const double* __restrict__ v,
+                       double* __restrict__ w) {
+    COLUMN_PROLOGUE
+    const int nz = P.nz;
+    const size_t c = nb.c, cw = nb.at(0, -1), cs_ = nb.at(-1, 0);
+    double acc = 0.0;
+    w[(size_t)nz * n2 + c] = 0.0;
+    for (int k = nz - 1; k >= 0; --k) {
+        const size_t o = (size_t)k * n2;
+        double m3f, dzu_c, dzu_w, dzv_c, dzv_s;
+        ufacek(P, nb, 0, 0, k, m3f, dzu_c);
+        ufacek(P, nb, 0, -1, k, m3f, dzu_w);
+        vfacek(P, nb, 0, 0, k, m3f, dzv_c);
+        vfacek(P, nb, -1, 0, k, m3f, dzv_s);
+        const double m3 = m3_at(P, nb, 0, 0, k);
+        const double td = m3 * ((dzu_c * u[o + c] - dzu_w * u[o + cw]) / P.dx +
+                                (dzv_c * v[o + c] - dzv_s * v[o + cs_]) / P.dy);
+        acc = (k == nz - 1) ? td : acc + td;
+        w[o + c] = -acc;
+    }
+}
+
+// ------------------------------------------------------------------ buoyancy potential
+// phi[k] = 0.5 dz3 b + sum_{k'<k} dz3 b, optionally minus its thickness-weighted
+// column mean (vertical_var.py:132-145).
+__global__ void k_phi(KP P, const double* __restrict__ b, double* __restrict__ phi) {
+    COLUMN_PROLOGUE
+    const int nz = P.nz;
+    const size_t c = nb.c;
+    const double Hc = P.H[c], mc = P.mask[c];
+    double above = 0.0, total = 0.0;
+    for (int k = 0; k < nz; ++k) {
+        const size_t o = (size_t)k * n2 + c;
+        double m3;
+        const double dz = cell_dz(P, Hc, mc, k, m3);
+        const double bk = b[o];
+        phi[o] = 0.5 * dz * bk + above;
+        const double t = dz * bk;
+        above = (k == 0) ? t : above + t;
+        total = (k == 0) ? dz : total + dz;
+    }
+    if (P.pgf_remove) {
+        double s = 0.0;
+        for (int k = 0; k < nz; ++k) {
+            double m3;
+            const double dz = cell_dz(P, Hc, mc, k, m3);
+            const double t = dz * phi[(size_t)k * n2 + c];
+            s = (k == 0) ? t : s + t;
+        }
+        const double mean = s * inv_pos(total);
+        for (int k = 0; k < nz; ++k) {
+            const size_t o = (size_t)k * n2 + c;
+            phi[o] = phi[o] - mean;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ Coriolis averages
+// v averaged onto u points over wet v faces (operators_masked.py:45-52)
+__device__ __forceinline__ double v_on_u(const KP& P, const Nbr& nb, const double* __restrict__ v,
+                                         size_t o, int k) {
+    const double f0 = v[o + nb.at(0, 0)], f1 = v[o + nb.at(-1, 0)];
+    const double f2 = v[o + nb.at(0, 1)], f3 = v[o + nb.at(-1, 1)];
+    const double w0 = m3v_at(P, nb, 0, 0, k), w1 = m3v_at(P, nb, -1, 0, k);
+    const double w2 = m3v_at(P, nb, 0, 1, k), w3 = m3v_at(P, nb, -1, 1, k);
+    double num = 0.0 + w0 * f0;
+    num = num + w1 * f1;
+    num = num + w2 * f2;
+    num = num + w3 * f3;
+    double den = 0.0 + w0;
+    den = den + w1;
+    den = den + w2;
+    den = den + w3;
+    const double avg = den > 0.0 ? num / den : 0.0;
+    return avg * m3u_at(P, nb, 0, 0, k);
+}
+
+// u averaged onto v points over wet u faces (operators_masked.py:55-61)
+__device__ __forceinline__ double u_on_v(const KP& P, const Nbr& nb, const double* __restrict__ u,
+                                         size_t o, int k) {
+    const double f0 = u[o + nb.at(0, 0)], f1 = u[o + nb.at(0, -1)];
+    const double f2 = u[o + nb.at(1, 0)], f3 = u[o + nb.at(1, -1)];
+    const double w0 = m3u_at(P, nb, 0, 0, k), w1 = m3u_at(P, nb, 0, -1, k);
+    const double w2 = m3u_at(P, nb, 1, 0, k), w3 = m3u_at(P, nb, 1, -1, k);
+    double num = 0.0 + w0 * f0;
+    num = num + w1 * f1;
+    num = num + w2 * f2;
+    num = num + w3 * f3;
+    double den = 0.0 + w0;
+    den = den + w1;
+    den = den + w2;
+    den = den + w3;
+    const double avg = den > 0.0 ? num / den : 0.0;
+    return avg * m3v_at(P, nb, 0, 0, k);
+}
+
+// ------------------------------------------------------------------ momentum advection
+// x-, y- and z-flux divergence of u at its east face (advection_v06.py:77-99 for
+// the kappa/TVD scheme, advection.py:62-79 for the centred one).
+__device__ double mom_adv_u(const KP& P, const Nbr& nb, const double* __restrict__ u,
+                            const double* __restrict__ v, const double* __restrict__ w, int k) {
+    const size_t n2 = P.n2;
+    const size_t o = (size_t)k * n2;
+    const int nz = P.nz;
+    auto U = [&](int dj, int di) { return u[o + nb.at(dj, di)]; };
+    auto V = [&](int dj, int di) { return v[o + nb.at(dj, di)]; };
+    auto Uk = [&](int kk) { return u[(size_t)kk * n2 + nb.c]; };
+    auto W = [&](int kk, int di) { return w[(size_t)kk * n2 + nb.at(0, di)]; };
+    const bool up3 = P.advection >= 3;
+    const bool lim = P.advection == 4;
+    double ax, ay, az;
+    if (up3) {
+        const double ub_c0 = 0.5 * (U(0, -1) + U(0, 0));
+        const double ub_c1 = 0.5 * (U(0, 0) + U(0, 1));
+        const double uc0 = kappa_face(P, U(0, -2), U(0, -1), U(0, 0), U(0, 1), ub_c0,
+                                      m3u_at(P, nb, 0, -2, k), m3u_at(P, nb, 0, 1, k), lim);
+        const double uc1 = kappa_face(P, U(0, -1), U(0, 0), U(0, 1), U(0, 2), ub_c1,
+                                      m3u_at(P, nb, 0, -1, k), m3u_at(P, nb, 0, 2, k), lim);
+        ax = (ub_c1 * uc1 - ub_c0 * uc0) / P.dx;
+        const double vb0 = 0.5 * (V(0, 0) + V(0, 1));
+        const double vbm = 0.5 * (V(-1, 0) + V(-1, 1));
+        const double fy0 = vb0 * kappa_face(P, U(-1, 0), U(0, 0), U(1, 0), U(2, 0), vb0,
+                                            m3u_at(P, nb, -1, 0, k), m3u_at(P, nb, 2, 0, k), lim);
+        const double fym = vbm * kappa_face(P, U(-2, 0), U(-1, 0), U(0, 0), U(1, 0), vbm,
+                                            m3u_at(P, nb, -2, 0, k), m3u_at(P, nb, 1, 0, k), lim);
+        ay = (fy0 - fym) / P.dy;
+        double fz[2];
+        for (int t = 0; t < 2; ++t) {
+            const int kk = k + t;
+            if (kk == 0 || kk == nz) {
+                fz[t] = 0.0;
+                continue;
+            }
+            const double wb = 0.5 * (W(kk, 0) + W(kk, 1));
+            const double fu = (kk >= 2) ? Uk(kk - 2) : 0.0;
+            const double fd = (kk + 1 <= nz - 1) ? Uk(kk + 1) : 0.0;
+            const bool hu = (kk >= 2) && m3u_at(P, nb, 0, 0, kk - 2) > 0.0;
+            const bool hd = (kk + 1 <= nz - 1) && m3u_at(P, nb, 0, 0, kk + 1) > 0.0;
+            fz[t] = wb * kappa_face_z(P, fu, Uk(kk - 1), Uk(kk), fd, wb, hu, hd, lim);
+        }
+        az = (fz[0] - fz[1]) / P.dz_nom;
+    } else {
+        const double ub_c0 = 0.5 * (U(0, -1) + U(0, 0));
+        const double ub_c1 = 0.5 * (U(0, 0) + U(0, 1));
+        ax = (ub_c1 * ub_c1 - ub_c0 * ub_c0) / P.dx;
+        const double vb0 = 0.5 * (V(0, 0) + V(0, 1));
+        const double vbm = 0.5 * (V(-1, 0) + V(-1, 1));
+        const double fy0 = vb0 * (0.5 * (U(0, 0) + U(1, 0)));
+        const double fym = vbm * (0.5 * (U(-1, 0) + U(0, 0)));
+        ay = (fy0 - fym) / P.dy;
+        double fz[2];
+        for (int t = 0; t < 2; ++t) {
+            const int kk = k + t;
+            if (kk == 0 || kk == nz) {
+                fz[t] = 0.0;
+                continue;
+            }
+            const double wb = 0.5 * (W(kk, 0) + W(kk, 1));
+            fz[t] = wb * 0.5 * (Uk(kk - 1) + Uk(kk));
+        }
+        az = (fz[0] - fz[1]) / P.dz_nom;
+    }
+    return ax + ay + az;
+}
+
+// the same for v at its north face (advection_v06.py:100-108, advection.py:81-95)
+__device__ double mom_adv_v(const KP& P, const Nbr& nb, const double* __restrict__ u,
+                            const double* __restrict__ v, const double* __restrict__ w, int k) {
+    const size_t n2 = P.n2;
+    const size_t o = (size_t)k * n2;
+    const int nz = P.nz;
+    auto U = [&](int dj, int di) { return u[o + nb.at(dj, di)]; };
+    auto V = [&](int dj, int di) { return v[o + nb.at(dj, di)]; };
+    auto Vk = [&](int kk) { return v[(size_t)kk * n2 + nb.c]; };
+    auto W = [&](int kk, int dj) { return w[(size_t)kk * n2 + nb.at(dj, 0)]; };
+    const bool up3 = P.advection >= 3;
+    const bool lim = P.advection == 4;
+    double bx, by, bz;
+    if (up3) {
+        const double vb_c0 = 0.5 * (V(-1, 0) + V(0, 0));
+        const double vb_c1 = 0.5 * (V(0, 0) + V(1, 0));
+        const double vc0 = kappa_face(P, V(-2, 0), V(-1, 0), V(0, 0), V(1, 0), vb_c0,
+                                      m3v_at(P, nb, -2, 0, k), m3v_at(P, nb, 1, 0, k), lim);
+        const double vc1 = kappa_face(P, V(-1, 0), V(0, 0), V(1, 0), V(2, 0), vb_c1,
+                                      m3v_at(P, nb, -1, 0, k), m3v_at(P, nb, 2, 0, k), lim);
+        by = (vb_c1 * vc1 - vb_c0 * vc0) / P.dy;
+        const double ub0 = 0.5 * (U(0, 0) + U(1, 0));
+        const double ubm = 0.5 * (U(0, -1) + U(1, -1));
+        const double fx0 = ub0 * kappa_face(P, V(0, -1), V(0, 0), V(0, 1), V(0, 2), ub0,
+                                            m3v_at(P, nb, 0, -1, k), m3v_at(P, nb, 0, 2, k), lim);
+        const double fxm = ubm * kappa_face(P, V(0, -2), V(0, -1), V(0, 0), V(0, 1), ubm,
+                                            m3v_at(P, nb, 0, -2, k), m3v_at(P, nb, 0, 1, k), lim);
+        bx = (fx0 - fxm) / P.dx;
+        double fz[2];
+        for (int t = 0; t < 2; ++t) {
+            const int kk = k + t;
+            if (kk == 0 || kk == nz) {
+                fz[t] = 0.0;
+                continue;
+            }
+            const double wb = 0.5 * (W(kk, 0) + W(kk, 1));
+            const double fu = (kk >= 2) ? Vk(kk - 2) : 0.0;
+            const double fd = (kk + 1 <= nz - 1) ? Vk(kk + 1) : 0.0;
+            const bool hu = (kk >= 2) && m3v_at(P, nb, 0, 0, kk - 2) > 0.0;
+            const bool hd = (kk + 1 <= nz - 1) && m3v_at(P, nb, 0, 0, kk + 1) > 0.0;
+            fz[t] = wb * kappa_face_z(P, fu, Vk(kk - 1), Vk(kk), fd, wb, hu, hd, lim);
+        }
+        bz = (fz[0] - fz[1]) / P.dz_nom;
+    } else {
+        const double vb_c0 = 0.5 * (V(-1, 0) + V(0, 0));
+        const double vb_c1 = 0.5 * (V(0, 0) + V(1, 0));
+        by = (vb_c1 * vb_c1 - vb_c0 * vb_c0) / P.dy;
+        const double ub0 = 0.5 * (U(0, 0) + U(1, 0));
+        const double ubm = 0.5 * (U(0, -1) + U(1, -1));
+        const double fx0 = ub0 * (0.5 * (V(0, 0) + V(0, 1)));
+        const double fxm = ubm * (0.5 * (V(0, -1) + V(0, 0)));
+        bx = (fx0 - fxm) / P.dx;
+        double fz[2];
+        for (int t = 0; t < 2; ++t) {
+            const int kk = k + t;
+            if (kk == 0 || kk == nz) {
+                fz[t] = 0.0;
+                continue;
+            }
+            const double wb = 0.5 * (W(kk, 0) + W(kk, 1));
+            fz[t] = wb * 0.5 * (Vk(kk - 1) + Vk(kk));
+        }
+        bz = (fz[0] - fz[1]) / P.dz_nom;
+    }
+    return bx + by + bz;
+}
+
+// horizontal Laplacian D o G with the given face masks (operators_masked.py:64-68);
+// which = 0: u (x-mask m3u, y-mask m3v, cell mask m3u), 1: v (cell mask m3v),
+// 2: tracer (cell mask m3)
+__device__ double hlap(const KP& P, const Nbr& nb, const double* __restrict__ f, int k, int which) {
+    const size_t o = (size_t)k * P.n2;
+    auto F = [&](int dj, int di) { return f[o + nb.at(dj, di)]; };
+    const double gx0 = m3u_at(P, nb, 0, 0, k) * (F(0, 1) - F(0, 0)) / P.dx;
+    const double gxw = m3u_at(P, nb, 0, -1, k) * (F(0, 0) - F(0, -1)) / P.dx;
+    const double gy0 = m3v_at(P, nb, 0, 0, k) * (F(1, 0) - F(0, 0)) / P.dy;
+    const double gys = m3v_at(P, nb, -1, 0, k) * (F(0, 0) - F(-1, 0)) / P.dy;
+    const double m = which == 0 ? m3u_at(P, nb, 0, 0, k)
+                                : (which == 1 ? m3v_at(P, nb, 0, 0, k) : m3_at(P, nb, 0, 0, k));
+    return m * ((gx0 - gxw) / P.dx + (gy0 - gys) / P.dy);
+}
+
+// explicit vertical diffusion of a face velocity (vertical_var.py:80-106) with
+// the column's interface viscosity, the face thickness table dzf[k-1..k+1], the
+// cell mask's bottom rule and surface flux `surf`
+__device__ __forceinline__ double explicit_dz(const KP& P, int k, double fkm1, double fk, double fkp1,
+                                              double Kk, double Kk1, double dzf_m1, double dzf_k,
+                                              double dzf_p1, double m3k_m1_bottom,
+                                              double m3k_bottom, double m3k, double surf,
+                                              double drag) {
+    const int nz = P.nz;
+    double flux_k, flux_k1;
+    if (k == 0) {
+        flux_k = surf;
+    } else {
+        const double dzi = 0.5 * (dzf_m1 + dzf_k);
+        flux_k = Kk * (fkm1 - fk) * inv_pos(dzi);
+        if (m3k_m1_bottom > 0.0) flux_k = 0.0;
+    }
+    if (k == nz - 1) {
+        flux_k1 = 0.0;
+    } else {
+        const double dzi = 0.5 * (dzf_k + dzf_p1);
+        flux_k1 = Kk1 * (fk - fkp1) * inv_pos(dzi);
+        if (m3k_bottom > 0.0) flux_k1 = 0.0;
+    }
+    const double idz = inv_pos(dzf_k);
+    const double out = (flux_k - flux_k1) * idz;
+    const double dragc = drag * fk * m3k_bottom;
+    return (out - dragc * idz) * (m3k > 0.0 ? 1.0 : 0.0);
+}
+
+// ------------------------------------------------------------------ explicit momentum terms
+// Everything of the predictor that depends on the old state only: the
+// common-depth pressure gradient, the old-state Coriolis average, the explicit
+// vertical diffusion and the stress + advection/viscosity increment.
+__global__ void __launch_bounds__(128) k_mom_explicit(
+    KP P, const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ b,
+    const double* __restrict__ phi, const double* __restrict__ w, const double* __restrict__ km,
+    double* __restrict__ pgx, double* __restrict__ pgy, double* __restrict__ avpv,
+    double* __restrict__ avpu, double* __restrict__ dzu, double* __restrict__ dzv,
+    double* __restrict__ stu, double* __restrict__ stv) {
+    COLUMN_PROLOGUE
+    const int nz = P.nz;
+    const size_t c = nb.c, ce = nb.at(0, 1), cn = nb.at(1, 0);
+    const double Hc = P.H[c], mc = P.mask[c];
+    const double He = P.H[ce], me = P.mask[ce];
+    const double Hn = P.H[cn], mn = P.mask[cn];
+    double above_c = 0.0, above_e = 0.0, above_n = 0.0;
+    // face-thickness and bottom flags of the previous / current / next level
+    double dzu_m1 = 0.0, dzv_m1 = 0.0;
+    double bottom_m1 = 0.0;
+    double m3_cur, m3_e, m3_n;
+    double dz_c = cell_dz(P, Hc, mc, 0, m3_cur);
+    double dz_e = cell_dz(P, He, me, 0, m3_e);
+    double dz_n = cell_dz(P, Hn, mn, 0, m3_n);
+    for (int k = 0; k < nz; ++k) {
+        const size_t o = (size_t)k * n2;
+        // next level's geometry (for bottom flags and face spacing)
+        double m3_cn = 0.0, m3_en = 0.0, m3_nn = 0.0, dz_cn = 0.0, dz_en = 0.0, dz_nn = 0.0;
+        if (k + 1 < nz) {
+            dz_cn = cell_dz(P, Hc, mc, k + 1, m3_cn);
+            dz_en = cell_dz(P, He, me, k + 1, m3_en);
+            dz_nn = cell_dz(P, Hn, mn, k + 1, m3_nn);
+        }
+        const double m3u_k = m3_cur * m3_e * P.mask_u[c];
+        const double m3v_k = m3_cur * m3_n * P.mask_v[c];
+        const double dzu_k = m3u_k * face_combine(P, dz_c, dz_e);
+        const double dzv_k = m3v_k * face_combine(P, dz_c, dz_n);
+        const double m3u_k1 = m3_cn * m3_en * P.mask_u[c];
+        const double m3v_k1 = m3_cn * m3_nn * P.mask_v[c];
+        const double dzu_p1 = m3u_k1 * face_combine(P, dz_cn, dz_en);
+        const double dzv_p1 = m3v_k1 * face_combine(P, dz_cn, dz_nn);
+        const double bottom_k = (m3_cur > 0.0 && m3_cn == 0.0) ? 1.0 : 0.0;
+        // ---- pressure gradient at a common depth (model3d_v05.py:211-230)
+        const double zc_c = above_c + 0.5 * dz_c;
+        const double zc_e = above_e + 0.5 * dz_e;
+        const double zc_n = above_n + 0.5 * dz_n;
+        const double phc = phi[o + c], phe = phi[o + ce], phn = phi[o + cn];
+        const double bc = b[o + c], be = b[o + ce], bn = b[o + cn];
+        double px, py;
+        if (P.pgf_correction) {
+            const double zfx = 0.5 * (zc_c + zc_e);
+            px = m3u_k * ((phe + be * (zfx - zc_e)) - (phc + bc * (zfx - zc_c))) / P.dx;
+            const double zfy = 0.5 * (zc_c + zc_n);
+            py = m3v_k * ((phn + bn * (zfy - zc_n)) - (phc + bc * (zfy - zc_c))) / P.dy;
+        } else {
+            px = m3u_k * (phe - phc) / P.dx * m3u_k;
+            py = m3v_k * (phn - phc) / P.dy * m3v_k;
+        }
+        pgx[o + c] = px;
+        pgy[o + c] = py;
+        // ---- Coriolis averages of the old state
+        avpv[o + c] = v_on_u(P, nb, v, o, k);
+        avpu[o + c] = u_on_v(P, nb, u, o, k);
+        // ---- explicit vertical diffusion (viscosity of the cell column)
+        const double K_k = km[o + c], K_k1 = km[o + n2 + c];
+        const double uk = u[o + c], vk = v[o + c];
+        const double ukm = (k > 0) ? u[o - n2 + c] : 0.0, vkm = (k > 0) ? v[o - n2 + c] : 0.0;
+        const double ukp = (k + 1 < nz) ? u[o + n2 + c] : 0.0;
+        const double vkp = (k + 1 < nz) ? v[o + n2 + c] : 0.0;
+        dzu[o + c] = explicit_dz(P, k, ukm, uk, ukp, K_k, K_k1, dzu_m1, dzu_k, dzu_p1, bottom_m1,
+                                 bottom_k, m3_cur, P.tau_u[c], P.bottom_drag);
+        dzv[o + c] = explicit_dz(P, k, vkm, vk, vkp, K_k, K_k1, dzv_m1, dzv_k, dzv_p1, bottom_m1,
+                                 bottom_k, m3_cur, P.tau_v[c], P.bottom_drag);
+        // ---- advection and horizontal viscosity, then the stress increment
+        double exu = 0.0, exv = 0.0;
+        if (P.advection != 0) {
+            exu = exu - mom_adv_u(P, nb, u, v, w, k) * m3u_k;
+            exv = exv - mom_adv_v(P, nb, u, v, w, k) * m3v_k;
+        }
+        if (P.a_h > 0.0) {
+            exu = exu + P.a_h * hlap(P, nb, u, k, 0);
+            exv = exv + P.a_h * hlap(P, nb, v, k, 1);
+        }
+        if (k == 0) {
+            stu[o + c] = P.thv_dt * P.tau_u[c] * inv_pos(dzu_k) + P.dt * exu;
+            stv[o + c] = P.thv_dt * P.tau_v[c] * inv_pos(dzv_k) + P.dt * exv;
+        } else {
+            stu[o + c] = 0.0 + P.dt * exu;
+            stv[o + c] = 0.0 + P.dt * exv;
+        }
+        // advance the column prefix sums and the level window
+        above_c = (k == 0) ? dz_c : above_c + dz_c;
+        above_e = (k == 0) ? dz_e : above_e + dz_e;
+        above_n = (k == 0) ? dz_n : above_n + dz_n;
+        dzu_m1 = dzu_k;
+        dzv_m1 = dzv_k;
+        bottom_m1 = bottom_k;
+        dz_c = dz_cn;
+        dz_e = dz_en;
+        dz_n = dz_nn;
+        m3_cur = m3_cn;
+        m3_e = m3_en;
+        m3_n = m3_nn;
+    }
+}
+
+// ------------------------------------------------------------------ predictor + column solves
+// For one Picard iteration: the explicit predictors Gu, Gv with the iterate's
+// Coriolis, both tridiagonal solves with the cell column's momentum rows, the
+// cell-mask multiply and the depth-integrated transports of the result.
+template <int NZM>
+__global__ void __launch_bounds__(128) k_predictor(
+    KP P, const double* __restrict__ u, const double* __restrict__ v,
+    const double* __restrict__ u_it, const double* __restrict__ v_it,
+    const double* __restrict__ pgx, const double* __restrict__ pgy,
+    const double* __restrict__ avpv, const double* __restrict__ avpu,
+    const double* __restrict__ dzu, const double* __restrict__ dzv,
+    const double* __restrict__ stu, const double* __restrict__ stv,
+    const double* __restrict__ gx2, const double* __restrict__ gy2, const double* __restrict__ km,
+    double* __restrict__ ghu, double* __restrict__ ghv, double* __restrict__ Ug,
+    double* __restrict__ Vg) {
+    COLUMN_PROLOGUE
+    const int nz = P.nz;
+    const size_t c = nb.c, ce = nb.at(0, 1), cn = nb.at(1, 0);
+    double dz[NZM], m3[NZM], dzi[NZM + 1], cs[NZM], dsu[NZM], dsv[NZM];
+    double depth;
+    column_geometry<NZM>(P, c, dz, m3, dzi, depth);
+    const double He = P.H[ce], me = P.mask[ce], Hn = P.H[cn], mn = P.mask[cn];
+    const bool split = P.scheme == 2;
+    const double gxe = split ? 0.0 : gx2[c], gye = split ? 0.0 : gy2[c];
+    double km_k = km[c];
+    for (int k = 0; k < nz; ++k) {
+        const size_t o = (size_t)k * n2;
+        const double km_k1 = km[o + n2 + c];
+        double m3e, m3n;
+        cell_dz(P, He, me, k, m3e);
+        cell_dz(P, Hn, mn, k, m3n);
+        const double m3u_k = m3[k] * m3e * P.mask_u[c];
+        const double m3v_k = m3[k] * m3n * P.mask_v[c];
+        const double vcor = P.one_m_tc * avpv[o + c] + P.theta_cor * v_on_u(P, nb, v_it, o, k);
+        const double ucor = P.one_m_tc * avpu[o + c] + P.theta_cor * u_on_v(P, nb, u_it, o, k);
+        double gu, gv;
+        if (!split) {
+            gu = u[o + c] + P.dt * (P.f0 * vcor + pgx[o + c]) - P.c1 * (gxe * m3u_k) + P.c3 * dzu[o + c];
+            gv = v[o + c] + P.dt * (P.neg_f0 * ucor + pgy[o + c]) - P.c1 * (gye * m3v_k) +
+                 P.c3 * dzv[o + c];
+        } else {
+            gu = u[o + c] + P.dt * (P.f0 * vcor + pgx[o + c]) + P.c3 * dzu[o + c];
+            gv = v[o + c] + P.dt * (P.neg_f0 * ucor + pgy[o + c]) + P.c3 * dzv[o + c];
+        }
+        const double ru = gu + stu[o + c];
+        const double rv = gv + stv[o + c];
+        double sub, diag, sup;
+        const double m3k1 = (k + 1 < nz) ? m3[k + 1] : 0.0;
+        implicit_row(P, k, dz[k], m3[k], m3k1, dzi[k], dzi[k + 1], km_k, km_k1, P.thv_dt_drag, sub,
+                     diag, sup);
+        if (k == 0) {
+            cs[0] = sup / diag;
+            dsu[0] = ru / diag;
+            dsv[0] = rv / diag;
+        } else {
+            const double den = diag - sub * cs[k - 1];
+            cs[k] = sup / den;
+            dsu[k] = (ru - sub * dsu[k - 1]) / den;
+            dsv[k] = (rv - sub * dsv[k - 1]) / den;
+        }
+        km_k = km_k1;
+    }
+    double xu = dsu[nz - 1], xv = dsv[nz - 1];
+    dsu[nz - 1] = xu;
+    dsv[nz - 1] = xv;
+    for (int k = nz - 2; k >= 0; --k) {
+        xu = dsu[k] - cs[k] * xu;
+        xv = dsv[k] - cs[k] * xv;
+        dsu[k] = xu;
+        dsv[k] = xv;
+    }
+    double su = 0.0, sv = 0.0;
+    for (int k = 0; k < nz; ++k) {
+        const size_t o = (size_t)k * n2;
+        const double hu = dsu[k] * m3[k];
+        const double hv = dsv[k] * m3[k];
+        ghu[o + c] = hu;
+        ghv[o + c] = hv;
+        double m3e, m3n;
+        const double dze = cell_dz(P, He, me, k, m3e);
+        const double dzn = cell_dz(P, Hn, mn, k, m3n);
+        const double m3u_k = m3[k] * m3e * P.mask_u[c];
+        const double m3v_k = m3[k] * m3n * P.mask_v[c];
+        const double tu = m3u_k * face_combine(P, dz[k], dze) * hu;
+        const double tv = m3v_k * face_combine(P, dz[k], dzn) * hv;
+        su = (k == 0) ? tu : su + tu;
+        sv = (k == 0) ? tv : sv + tv;
+    }
+    Ug[c] = su;
+    Vg[c] = sv;
+}
+
+// ------------------------------------------------------------------ back substitution
+// u = (gh_u - g dt theta q dx(eta_new) m3u) m3   (model3d_v05.py:404-406)
+__global__ void k_backsub(KP P, const double* __restrict__ ghu, const double* __restrict__ ghv,
+                          const double* __restrict__ q, const double* __restrict__ eta_new,
+                          double* __restrict__ u_out, double* __restrict__ v_out) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c, ce = nb.at(0, 1), cn = nb.at(1, 0);
+    const double gx = P.mask_u[c] * (eta_new[ce] - eta_new[c]) / P.dx;
+    const double gy = P.mask_v[c] * (eta_new[cn] - eta_new[c]) / P.dy;
+    const double Hc = P.H[c], mc = P.mask[c], He = P.H[ce], me = P.mask[ce];
+    const double Hn = P.H[cn], mn = P.mask[cn];
+    for (int k = 0; k < P.nz; ++k) {
+        const size_t o = (size_t)k * n2 + c;
+        double m3, m3e, m3n;
+        cell_dz(P, Hc, mc, k, m3);
+        cell_dz(P, He, me, k, m3e);
+        cell_dz(P, Hn, mn, k, m3n);
+        const double m3u_k = m3 * m3e * P.mask_u[c];
+        const double m3v_k = m3 * m3n * P.mask_v[c];
+        const double qk = q[o];
+        u_out[o] = (ghu[o] - P.c2 * qk * gx * m3u_k) * m3;
+        v_out[o] = (ghv[o] - P.c2 * qk * gy * m3v_k) * m3;
+    }
+}
+
+// ------------------------------------------------------------------ tracers + EOS
+// Flux-form advection with the face masks and real face thickness
+// (model3d_v05.py:482-512) of tracer C at level k
+__device__ double tracer_adv(const KP& P, const Nbr& nb, const double* __restrict__ C,
+                             const double* __restrict__ u, const double* __restrict__ v,
+                             const double* __restrict__ w, int k, double dzc, double m3c) {
+    const size_t n2 = P.n2;
+    const size_t o = (size_t)k * n2;
+    const int nz = P.nz;
+    auto F = [&](int dj, int di) { return C[o + nb.at(dj, di)]; };
+    auto Fk = [&](int kk) { return C[(size_t)kk * n2 + nb.c]; };
+    const int adv = P.advection;
+    const bool lim = adv == 4;
+    const double u0 = u[o + nb.c], uw = u[o + nb.at(0, -1)];
+    const double v0 = v[o + nb.c], vs = v[o + nb.at(-1, 0)];
+    double cx0, cxw, cy0, cys;
+    if (adv == 1) {
+        cx0 = 0.5 * (F(0, 0) + F(0, 1));
+        cxw = 0.5 * (F(0, -1) + F(0, 0));
+        cy0 = 0.5 * (F(0, 0) + F(1, 0));
+        cys = 0.5 * (F(-1, 0) + F(0, 0));
+    } else if (adv >= 3) {
+        cx0 = kappa_face(P, F(0, -1), F(0, 0), F(0, 1), F(0, 2), u0, m3_at(P, nb, 0, -1, k),
+                         m3_at(P, nb, 0, 2, k), lim);
+        cxw = kappa_face(P, F(0, -2), F(0, -1), F(0, 0), F(0, 1), uw, m3_at(P, nb, 0, -2, k),
+                         m3_at(P, nb, 0, 1, k), lim);
+        cy0 = kappa_face(P, F(-1, 0), F(0, 0), F(1, 0), F(2, 0), v0, m3_at(P, nb, -1, 0, k),
+                         m3_at(P, nb, 2, 0, k), lim);
+        cys = kappa_face(P, F(-2, 0), F(-1, 0), F(0, 0), F(1, 0), vs, m3_at(P, nb, -2, 0, k),
+                         m3_at(P, nb, 1, 0, k), lim);
+    } else {
+        cx0 = u0 > 0.0 ? F(0, 0) : F(0, 1);
+        cxw = uw > 0.0 ? F(0, -1) : F(0, 0);
+        cy0 = v0 > 0.0 ? F(0, 0) : F(1, 0);
+        cys = vs > 0.0 ? F(-1, 0) : F(0, 0);
+    }
+    double m, dzu0, dzuw, dzv0, dzvs;
+    ufacek(P, nb, 0, 0, k, m, dzu0);
+    ufacek(P, nb, 0, -1, k, m, dzuw);
+    vfacek(P, nb, 0, 0, k, m, dzv0);
+    vfacek(P, nb, -1, 0, k, m, dzvs);
+    const double fx0 = dzu0 * u0 * cx0, fxw = dzuw * uw * cxw;
+    const double fy0 = dzv0 * v0 * cy0, fys = dzvs * vs * cys;
+    const double inv = inv_pos(dzc);
+    const double hdiv = ((fx0 - fxw) / P.dx + (fy0 - fys) / P.dy) * inv;
+    double cf[2];
+    for (int t = 0; t < 2; ++t) {
+        const int kk = k + t;
+        if (kk == 0) {
+            cf[t] = Fk(0);
+        } else if (kk == nz) {
+            cf[t] = 0.0;
+        } else if (adv >= 3) {
+            const double fu = (kk >= 2) ? Fk(kk - 2) : 0.0;
+            const double fd = (kk + 1 <= nz - 1) ? Fk(kk + 1) : 0.0;
+            const bool hu = (kk >= 2) && m3_at(P, nb, 0, 0, kk - 2) > 0.0;
+            const bool hd = (kk + 1 <= nz - 1) && m3_at(P, nb, 0, 0, kk + 1) > 0.0;
+            cf[t] = kappa_face_z(P, fu, Fk(kk - 1), Fk(kk), fd, w[(size_t)kk * n2 + nb.c], hu, hd, lim);
+        } else {
+            cf[t] = 0.5 * (Fk(kk - 1) + Fk(kk));
+        }
+    }
+    const double vdiv = (w[o + nb.c] * cf[0] - w[o + n2 + nb.c] * cf[1]) * inv;
+    return (hdiv + vdiv) * m3c;
+}
+
+// right-hand side of the implicit tracer solve at level k (model3d_v05.py:466-479)
+__device__ __forceinline__ double tracer_rhs(const KP& P, const Nbr& nb, const double* __restrict__ C,
+                                             const double* __restrict__ u,
+                                             const double* __restrict__ v,
+                                             const double* __restrict__ w,
+                                             const double* __restrict__ kh, int k, double dzk,
+                                             double m3k, double dz_m1, double dz_p1, double m3_m1,
+                                             double m3_p1, double surf, double source) {
+    const size_t n2 = P.n2;
+    const size_t o = (size_t)k * n2 + nb.c;
+    const int nz = P.nz;
+    double tend = source;
+    if (P.advection != 0) tend = tend - tracer_adv(P, nb, C, u, v, w, k, dzk, m3k);
+    if (P.k_h > 0.0) tend = tend + P.k_h * hlap(P, nb, C, k, 2);
+    // explicit vertical diffusion with zero drag (vertical_var.py:80-106)
+    const double ck = C[o];
+    const double ckm = (k > 0) ? C[o - n2] : 0.0;
+    const double ckp = (k + 1 < nz) ? C[o + n2] : 0.0;
+    const double bottom_m1 = (k > 0 && m3_m1 > 0.0 && m3k == 0.0) ? 1.0 : 0.0;
+    const double bottom_k = (m3k > 0.0 && m3_p1 == 0.0) ? 1.0 : 0.0;
+    const double diff = explicit_dz(P, k, ckm, ck, ckp, kh[o], kh[o + n2], dz_m1, dzk, dz_p1,
+                                    bottom_m1, bottom_k, m3k, surf, 0.0);
+    double rhs = ck + P.dt * tend + P.c3 * diff;
+    if (k == 0) rhs = rhs + P.thv_dt * surf * inv_pos(dzk);
+    return rhs;
+}
+
+template <int NZM>
+__global__ void __launch_bounds__(128) k_tracers(KP P, const double* __restrict__ T,
+                                                 const double* __restrict__ S,
+                                                 const double* __restrict__ bold,
+                                                 const double* __restrict__ u,
+                                                 const double* __restrict__ v,
+                                                 const double* __restrict__ w,
+                                                 const double* __restrict__ kh,
+                                                 double* __restrict__ T_out,
+                                                 double* __restrict__ S_out,
+                                                 double* __restrict__ b_out) {
+    COLUMN_PROLOGUE
+    const int nz = P.nz;
+    const size_t c = nb.c;
+    double dz[NZM], m3[NZM], dzi[NZM + 1], cs[NZM], d1[NZM], d2[NZM];
+    double depth;
+    column_geometry<NZM>(P, c, dz, m3, dzi, depth);
+    const bool ts = P.tracers_ts;
+    double kh_k = kh[c];
+    for (int k = 0; k < nz; ++k) {
+        const size_t o = (size_t)k * n2 + c;
+        const double kh_k1 = kh[o + n2];
+        const double dz_m1 = (k > 0) ? dz[k - 1] : 0.0, m3_m1 = (k > 0) ? m3[k - 1] : 0.0;
+        const double dz_p1 = (k + 1 < nz) ? dz[k + 1] : 0.0, m3_p1 = (k + 1 < nz) ? m3[k + 1] : 0.0;
+        double r1, r2 = 0.0;
+        if (ts) {
+            r1 = tracer_rhs(P, nb, T, u, v, w, kh, k, dz[k], m3[k], dz_m1, dz_p1, m3_m1, m3_p1,
+                            P.flux_t, 0.0);
+            r2 = tracer_rhs(P, nb, S, u, v, w, kh, k, dz[k], m3[k], dz_m1, dz_p1, m3_m1, m3_p1,
+                            P.flux_s, 0.0);
+        } else {
+            const double src = P.neg_n2 * (0.5 * (w[o] + w[o + n2]));
+            r1 = tracer_rhs(P, nb, bold, u, v, w, kh, k, dz[k], m3[k], dz_m1, dz_p1, m3_m1, m3_p1,
+                            0.0, src);
+        }
+        double sub, diag, sup;
+        implicit_row(P, k, dz[k], m3[k], m3_p1, dzi[k], dzi[k + 1], kh_k, kh_k1, P.thv_dt_zero, sub,
+                     diag, sup);
+        if (k == 0) {
+            cs[0] = sup / diag;
+            d1[0] = r1 / diag;
+            d2[0] = r2 / diag;
+        } else {
+            const double den = diag - sub * cs[k - 1];
+            cs[k] = sup / den;
+            d1[k] = (r1 - sub * d1[k - 1]) / den;
+            d2[k] = (r2 - sub * d2[k - 1]) / den;
+        }
+        kh_k = kh_k1;
+    }
+    double x1 = d1[nz - 1], x2 = d2[nz - 1];
+    for (int k = nz - 1; k >= 0; --k) {
+        if (k < nz - 1) {
+            x1 = d1[k] - cs[k] * x1;
+            x2 = d2[k] - cs[k] * x2;
+        }
+        d1[k] = x1;
+        d2[k] = x2;
+    }
+    double above = 0.0;
+    for (int k = 0; k < nz; ++k) {
+        const size_t o = (size_t)k * n2 + c;
+        const double zc = above + 0.5 * dz[k];
+        above = (k == 0) ? dz[0] : above + dz[k];
+        if (ts) {
+            const double Tn = d1[k] * m3[k];
+            const double Sn = d2[k] * m3[k];
+            T_out[o] = Tn;
+            S_out[o] = Sn;
+            b_out[o] = buoyancy_of(P, Tn, Sn, zc) * m3[k];
+        } else {
+            b_out[o] = d1[k] * m3[k];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ EOS on a flat buffer
+__global__ void k_buoyancy(KP P, const double* __restrict__ T, const double* __restrict__ S,
+                           const double* __restrict__ z, double* __restrict__ b, int64_t n) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) b[t] = buoyancy_of(P, T[t], S[t], z[t]);
+}
+
+// diagnose b = EOS(T, S, zc) * m3 on the model grid (initial states)
+__global__ void k_diag_buoyancy(KP P, const double* __restrict__ T, const double* __restrict__ S,
+                                double* __restrict__ b) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c;
+    const double Hc = P.H[c], mc = P.mask[c];
+    double above = 0.0;
+    for (int k = 0; k < P.nz; ++k) {
+        const size_t o = (size_t)k * n2 + c;
+        double m3;
+        const double dz = cell_dz(P, Hc, mc, k, m3);
+        const double zc = above + 0.5 * dz;
+        above = (k == 0) ? dz : above + dz;
+        b[o] = buoyancy_of(P, T[o], S[o], zc) * m3;
+    }
+}
+
+// ------------------------------------------------------------------ 2D kernels
+// depth-integrated transports sum_k dz3u u, sum_k dz3v v
+__global__ void k_transport(KP P, const double* __restrict__ u, const double* __restrict__ v,
+                            double* __restrict__ U, double* __restrict__ V) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c;
+    double su = 0.0, sv = 0.0;
+    for (int k = 0; k < P.nz; ++k) {
+        const size_t o = (size_t)k * n2 + c;
+        double m, dzf;
+        ufacek(P, nb, 0, 0, k, m, dzf);
+        const double tu = dzf * u[o];
+        vfacek(P, nb, 0, 0, k, m, dzf);
+        const double tv = dzf * v[o];
+        su = (k == 0) ? tu : su + tu;
+        sv = (k == 0) ? tv : sv + tv;
+    }
+    U[c] = su;
+    V[c] = sv;
+}
+
+__device__ __forceinline__ double div2(const KP& P, const Nbr& nb, const double* __restrict__ U,
+                                       const double* __restrict__ V) {
+    const size_t c = nb.c;
+    return P.mask[c] * ((U[c] - U[nb.at(0, -1)]) / P.dx + (V[c] - V[nb.at(-1, 0)]) / P.dy);
+}
+
+__global__ void k_div2(KP P, const double* __restrict__ U, const double* __restrict__ V,
+                       double* __restrict__ out) {
+    COLUMN_PROLOGUE
+    out[nb.c] = div2(P, nb, U, V);
+}
+
+__global__ void k_grad2(KP P, const double* __restrict__ eta, double* __restrict__ gx,
+                        double* __restrict__ gy) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c;
+    gx[c] = P.mask_u[c] * (eta[nb.at(0, 1)] - eta[c]) / P.dx;
+    gy[c] = P.mask_v[c] * (eta[nb.at(1, 0)] - eta[c]) / P.dy;
+}
+
+// rhs = eta - dt ((1 - theta) div_old + theta div(Ug, Vg))  (model3d_v05.py:398-400)
+__global__ void k_helm_rhs(KP P, const double* __restrict__ eta, const double* __restrict__ div_old,
+                           const double* __restrict__ Ug, const double* __restrict__ Vg,
+                           double* __restrict__ rhs) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c;
+    const double dg = div2(P, nb, Ug, Vg);
+    rhs[c] = eta[c] - P.dt * (P.one_m_th * div_old[c] + P.theta * dg);
+}
+
+// forward-backward free surface eta_new = eta - dt div(U, V) (model3d_v05.py:410-413)
+__global__ void k_eta_fb(KP P, const double* __restrict__ eta, const double* __restrict__ U,
+                         const double* __restrict__ V, double* __restrict__ eta_new) {
+    COLUMN_PROLOGUE
+    eta_new[nb.c] = eta[nb.c] - P.dt * div2(P, nb, U, V);
+}
+
+// ---- split-explicit barotropic mode (model3d_v05.py:312-335, 440-461)
+__device__ __forceinline__ double v_on_u2(const KP& P, const Nbr& nb, const double* __restrict__ V) {
+    const double f0 = V[nb.at(0, 0)], f1 = V[nb.at(-1, 0)], f2 = V[nb.at(0, 1)], f3 = V[nb.at(-1, 1)];
+    const double w0 = P.mask_v[nb.at(0, 0)], w1 = P.mask_v[nb.at(-1, 0)];
+    const double w2 = P.mask_v[nb.at(0, 1)], w3 = P.mask_v[nb.at(-1, 1)];
+    double num = 0.0 + w0 * f0;
+    num = num + w1 * f1;
+    num = num + w2 * f2;
+    num = num + w3 * f3;
+    double den = 0.0 + w0;
+    den = den + w1;
+    den = den + w2;
+    den = den + w3;
+    return (den > 0.0 ? num / den : 0.0) * P.mask_u[nb.c];
+}
+
+__device__ __forceinline__ double u_on_v2(const KP& P, const Nbr& nb, const double* __restrict__ U) {
+    const double f0 = U[nb.at(0, 0)], f1 = U[nb.at(0, -1)], f2 = U[nb.at(1, 0)], f3 = U[nb.at(1, -1)];
+    const double w0 = P.mask_u[nb.at(0, 0)], w1 = P.mask_u[nb.at(0, -1)];
+    const double w2 = P.mask_u[nb.at(1, 0)], w3 = P.mask_u[nb.at(1, -1)];
+    double num = 0.0 + w0 * f0;
+    num = num + w1 * f1;
+    num = num + w2 * f2;
+    num = num + w3 * f3;
+    double den = 0.0 + w0;
+    den = den + w1;
+    den = den + w2;
+    den = den + w3;
+    return (den > 0.0 ? num / den : 0.0) * P.mask_v[nb.c];
+}
+
+// barotropic forcing with the Coriolis of the 2D transport operator removed
+__global__ void k_split_forcing(KP P, const double* __restrict__ U0, const double* __restrict__ V0,
+                                const double* __restrict__ Um, const double* __restrict__ Vm,
+                                double* __restrict__ fx, double* __restrict__ fy) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c;
+    const double corx = P.f0 * (P.one_m_tc * v_on_u2(P, nb, V0) + P.theta_cor * v_on_u2(P, nb, Vm));
+    const double cory = P.neg_f0 * (P.one_m_tc * u_on_v2(P, nb, U0) + P.theta_cor * u_on_v2(P, nb, Um));
+    fx[c] = (Um[c] - U0[c]) / P.dt - corx;
+    fy[c] = (Vm[c] - V0[c]) / P.dt - cory;
+}
+
+// substep set-up: the old-transport Coriolis averages and the surface gradient
+__global__ void k_split_sub_avg(KP P, const double* __restrict__ U, const double* __restrict__ V,
+                                const double* __restrict__ e, double* __restrict__ avv,
+                                double* __restrict__ avu, double* __restrict__ gxe,
+                                double* __restrict__ gye) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c;
+    avv[c] = v_on_u2(P, nb, V);
+    avu[c] = u_on_v2(P, nb, U);
+    gxe[c] = P.mask_u[c] * (e[nb.at(0, 1)] - e[c]) / P.dx;
+    gye[c] = P.mask_v[c] * (e[nb.at(1, 0)] - e[c]) / P.dy;
+}
+
+// one Picard pass of a substep: (Ui, Vi) from the previous iterate
+__global__ void k_split_sub_mom(KP P, double ddt, const double* __restrict__ U,
+                                const double* __restrict__ V, const double* __restrict__ Ui,
+                                const double* __restrict__ Vi, const double* __restrict__ avv,
+                                const double* __restrict__ avu, const double* __restrict__ gxe,
+                                const double* __restrict__ gye, const double* __restrict__ Ku,
+                                const double* __restrict__ Kv, const double* __restrict__ fx,
+                                const double* __restrict__ fy, double* __restrict__ Uo,
+                                double* __restrict__ Vo) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c;
+    const double vcor = P.one_m_tc * avv[c] + P.theta_cor * v_on_u2(P, nb, Vi);
+    const double ucor = P.one_m_tc * avu[c] + P.theta_cor * u_on_v2(P, nb, Ui);
+    Uo[c] = (U[c] + ddt * (P.f0 * vcor - P.g * Ku[c] * gxe[c] + fx[c])) * P.mask_u[c];
+    Vo[c] = (V[c] + ddt * (P.neg_f0 * ucor - P.g * Kv[c] * gye[c] + fy[c])) * P.mask_v[c];
+}
+
+// e -= ddt div(U, V); accumulate the substep transports
+__global__ void k_split_sub_eta(KP P, double ddt, const double* __restrict__ U,
+                                const double* __restrict__ V, double* __restrict__ e,
+                                double* __restrict__ acc_u, double* __restrict__ acc_v, int first) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c;
+    const double d = div2(P, nb, U, V);
+    e[c] = e[c] - ddt * d;
+    acc_u[c] = first ? 0.0 + U[c] : acc_u[c] + U[c];
+    acc_v[c] = first ? 0.0 + V[c] : acc_v[c] + V[c];
+}
+
+__global__ void k_split_mean(KP P, int n_split, double* __restrict__ acc_u,
+                             double* __restrict__ acc_v) {
+    COLUMN_PROLOGUE
+    acc_u[nb.c] = acc_u[nb.c] / n_split;
+    acc_v[nb.c] = acc_v[nb.c] / n_split;
+}
+
+// replace the depth mean of the baroclinic velocity with the barotropic result
+// (model3d_v05.py:452-461)
+__global__ void k_split_correct(KP P, const double* __restrict__ ghu, const double* __restrict__ ghv,
+                                const double* __restrict__ Ug, const double* __restrict__ Vg,
+                                const double* __restrict__ U, const double* __restrict__ V,
+                                double* __restrict__ u_out, double* __restrict__ v_out) {
+    COLUMN_PROLOGUE
+    const size_t c = nb.c;
+    double Hu = 0.0, Hv = 0.0;
+    for (int k = 0; k < P.nz; ++k) {
+        double m, du, dv;
+        ufacek(P, nb, 0, 0, k, m, du);
+        vfacek(P, nb, 0, 0, k, m, dv);
+        Hu = (k == 0) ? du : Hu + du;
+        Hv = (k == 0) ? dv : Hv + dv;
+    }
+    const double ihu = inv_pos(Hu), ihv = inv_pos(Hv);
+    for (int k = 0; k < P.nz; ++k) {
+        const size_t o = (size_t)k * n2 + c;
+        const double m3u_k = m3u_at(P, nb, 0, 0, k), m3v_k = m3v_at(P, nb, 0, 0, k);
+        u_out[o] = (ghu[o] - Ug[c] * ihu + U[c] * ihu) * m3u_k;
+        v_out[o] = (ghv[o] - Vg[c] * ihv + V[c] * ihv) * m3v_k;
+    }
+}
+
+// ------------------------------------------------------------------ batched Thomas (unit entry)
+__global__ void k_thomas_batched(const double* __restrict__ sub, const double* __restrict__ diag,
+                                 const double* __restrict__ sup, const double* __restrict__ rhs,
+                                 double* __restrict__ x, double* __restrict__ cstar, int n,
+                                 int64_t ncols) {
+    const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncols) return;
+    double c_prev = sup[col] / diag[col];
+    double d_prev = rhs[col] / diag[col];
+    cstar[col] = c_prev;
+    x[col] = d_prev;
+    for (int k = 1; k < n; ++k) {
+        const int64_t o = (int64_t)k * ncols + col;
+        const double den = diag[o] - sub[o] * c_prev;
+        c_prev = sup[o] / den;
+        d_prev = (rhs[o] - sub[o] * d_prev) / den;
+        cstar[o] = c_prev;
+        x[o] = d_prev;
+    }
+    double xn = x[(int64_t)(n - 1) * ncols + col];
+    for (int k = n - 2; k >= 0; --k) {
+        const int64_t o = (int64_t)k * ncols + col;
+        xn = x[o] - cstar[o] * xn;
+        x[o] = xn;
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+#define NZ_DISPATCH(NZ, CALL)                \
+    do {                                     \
+        if ((NZ) + 1 <= 33) {                \
+            constexpr int NZM = 33;          \
+            CALL;                            \
+        } else if ((NZ) + 1 <= 65) {         \
+            constexpr int NZM = 65;          \
+            CALL;                            \
+        } else {                             \
+            constexpr int NZM = OC_MAXNZ + 1; \
+            CALL;                            \
+        }                                    \
+    } while (0)
+
+static dim3 col_block() { return dim3(32, 4); }
+static dim3 col_grid(const KP& P) { return dim3((P.nx + 31) / 32, (P.ny + 3) / 4); }
+
+void launch_qsolve(const KP& P, const double* km, double* q, cudaStream_t s) {
+    NZ_DISPATCH(P.nz, (k_qsolve<NZM><<<col_grid(P), col_block(), 0, s>>>(P, km, q)));
+}
+
+void launch_closure(const KP& P, const double* u, const double* v, const double* b, double* e,
+                    double* km, double* kh, double* q, cudaStream_t s) {
+    NZ_DISPATCH(P.nz, (k_closure<NZM><<<col_grid(P), col_block(), 0, s>>>(P, u, v, b, e, km, kh, q)));
+}
+
+void launch_kukv(const KP& P, const double* q, double* Ku, double* Kv, cudaStream_t s) {
+    k_kukv<<<col_grid(P), col_block(), 0, s>>>(P, q, Ku, Kv);
+}
+
+void launch_wcol(const KP& P, const double* u, const double* v, double* w, cudaStream_t s) {
+    k_wcol<<<col_grid(P), col_block(), 0, s>>>(P, u, v, w);
+}
+
+void launch_phi(const KP& P, const double* b, double* phi, cudaStream_t s) {
+    k_phi<<<col_grid(P), col_block(), 0, s>>>(P, b, phi);
+}
+
+void launch_mom_explicit(const KP& P, const double* u, const double* v, const double* b,
+                         const double* phi, const double* w, const double* km, double* pgx,
+                         double* pgy, double* avpv, double* avpu, double* dzu, double* dzv,
+                         double* stu, double* stv, cudaStream_t s) {
+    k_mom_explicit<<<col_grid(P), col_block(), 0, s>>>(P, u, v, b, phi, w, km, pgx, pgy, avpv, avpu,
+                                                      dzu, dzv, stu, stv);
+}
+
+void launch_predictor(const KP& P, const double* u, const double* v, const double* u_it,
+                      const double* v_it, const double* pgx, const double* pgy, const double* avpv,
+                      const double* avpu, const double* dzu, const double* dzv, const double* stu,
+                      const double* stv, const double* gx2, const double* gy2, const double* km,
+                      double* ghu, double* ghv, double* Ug, double* Vg, cudaStream_t s) {
+    NZ_DISPATCH(P.nz, (k_predictor<NZM><<<col_grid(P), col_block(), 0, s>>>(
+                          P, u, v, u_it, v_it, pgx, pgy, avpv, avpu, dzu, dzv, stu, stv, gx2, gy2,
+                          km, ghu, ghv, Ug, Vg)));
+}
+
+void launch_backsub(const KP& P, const double* ghu, const double* ghv, const double* q,
+                    const double* eta_new, double* u_out, double* v_out, cudaStream_t s) {
+    k_backsub<<<col_grid(P), col_block(), 0, s>>>(P, ghu, ghv, q, eta_new, u_out, v_out);
+}
+
+void launch_tracers(const KP& P, const double* T, const double* S, const double* bold,
+                    const double* u, const double* v, const double* w, const double* kh,
+                    double* T_out, double* S_out, double* b_out, cudaStream_t s) {
+    NZ_DISPATCH(P.nz, (k_tracers<NZM><<<col_grid(P), col_block(), 0, s>>>(
+                          P, T, S, bold, u, v, w, kh, T_out, S_out, b_out)));
+}
+
+void launch_buoyancy_flat(const KP& P, const double* T, const double* S, const double* z, double* b,
+                          int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    k_buoyancy<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, T, S, z, b, n);
+}
+
+void launch_diag_buoyancy(const KP& P, const double* T, const double* S, double* b, cudaStream_t s) {
+    k_diag_buoyancy<<<col_grid(P), col_block(), 0, s>>>(P, T, S, b);
+}
+
+void launch_transport(const KP& P, const double* u, const double* v, double* U, double* V,
+                      cudaStream_t s) {
+    k_transport<<<col_grid(P), col_block(), 0, s>>>(P, u, v, U, V);
+}
+
+void launch_div2(const KP& P, const double* U, const double* V, double* out, cudaStream_t s) {
+    k_div2<<<col_grid(P), col_block(), 0, s>>>(P, U, V, out);
+}
+
+void launch_grad2(const KP& P, const double* eta, double* gx, double* gy, cudaStream_t s) {
+    k_grad2<<<col_grid(P), col_block(), 0, s>>>(P, eta, gx, gy);
+}
+
+void launch_helm_rhs(const KP& P, const double* eta, const double* div_old, const double* Ug,
+                     const double* Vg, double* rhs, cudaStream_t s) {
+    k_helm_rhs<<<col_grid(P), col_block(), 0, s>>>(P, eta, div_old, Ug, Vg, rhs);
+}
+
+void launch_eta_fb(const KP& P, const double* eta, const double* U, const double* V, double* eta_new,
+                   cudaStream_t s) {
+    k_eta_fb<<<col_grid(P), col_block(), 0, s>>>(P, eta, U, V, eta_new);
+}
+
+void launch_split_forcing(const KP& P, const double* U0, const double* V0, const double* Um,
+                          const double* Vm, double* fx, double* fy, cudaStream_t s) {
+    k_split_forcing<<<col_grid(P), col_block(), 0, s>>>(P, U0, V0, Um, Vm, fx, fy);
+}
+
+void launch_split_sub_avg(const KP& P, const double* U, const double* V, const double* e,
+                          double* avv, double* avu, double* gxe, double* gye, cudaStream_t s) {
+    k_split_sub_avg<<<col_grid(P), col_block(), 0, s>>>(P, U, V, e, avv, avu, gxe, gye);
+}
+
+void launch_split_sub_mom(const KP& P, double ddt, const double* U, const double* V, const double* Ui,
+                          const double* Vi, const double* avv, const double* avu, const double* gxe,
+                          const double* gye, const double* Ku, const double* Kv, const double* fx,
+                          const double* fy, double* Uo, double* Vo, cudaStream_t s) {
+    k_split_sub_mom<<<col_grid(P), col_block(), 0, s>>>(P, ddt, U, V, Ui, Vi, avv, avu, gxe, gye, Ku,
+                                                       Kv, fx, fy, Uo, Vo);
+}
+
+void launch_split_sub_eta(const KP& P, double ddt, const double* U, const double* V, double* e,
+                          double* acc_u, double* acc_v, int first, cudaStream_t s) {
+    k_split_sub_eta<<<col_grid(P), col_block(), 0, s>>>(P, ddt, U, V, e, acc_u, acc_v, first);
+}
+
+void launch_split_mean(const KP& P, int n_split, double* acc_u, double* acc_v, cudaStream_t s) {
+    k_split_mean<<<col_grid(P), col_block(), 0, s>>>(P, n_split, acc_u, acc_v);
+}
+
+void launch_split_correct(const KP& P, const double* ghu, const double* ghv, const double* Ug,
+                          const double* Vg, const double* U, const double* V, double* u_out,
+                          double* v_out, cudaStream_t s) {
+    k_split_correct<<<col_grid(P), col_block(), 0, s>>>(P, ghu, ghv, Ug, Vg, U, V, u_out, v_out);
+}
+
+void launch_thomas(const double* sub, const double* diag, const double* sup, const double* rhs,
+                   double* x, double* cstar, int n, int64_t ncols, cudaStream_t s) {
+    k_thomas_batched<<<(unsigned)((ncols + 127) / 128), 128, 0, s>>>(sub, diag, sup, rhs, x, cstar, n,
+                                                                    ncols);
+}
+
+}  // namespace oc

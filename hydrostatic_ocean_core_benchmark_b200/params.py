@@ -112,7 +112,9 @@ class OceanParams:
             bad.append("n_picard must be >= 1")
         if self.dt <= 0.0:
             bad.append("dt must be > 0")
-        if self.solver_kind not in ("pcg_jacobi", "pcg_rbgs", "rbgs", "multigrid"):
+        # only the theta scheme owns an elliptic solve (reference model3d_v05.py:99-101)
+        if self.scheme_name == "theta" and self.solver_kind not in (
+                "pcg_jacobi", "pcg_rbgs", "rbgs", "multigrid"):
             bad.append(f"unknown variable-coefficient solver {self.solver_kind!r} "
                        "(expected pcg_jacobi|pcg_rbgs|rbgs|multigrid)")
         if self.vcoord != "zlevel":

@@ -1,0 +1,182 @@
+/*
+ * ocean_b200.h - C ABI of the B200 (sm_100a) hydrostatic ocean-core time step.
+ *
+ * Plain C types only: the library owns its device state and workspace, the
+ * caller hands in host or device pointers with their sizes. Every function
+ * returns an int status (OC_OK = 0); oc_last_error() gives the message.
+ * A handle is not thread-safe; all GPU work of a handle is issued on the
+ * stream passed to oc_step (or the default stream) in issue order.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   - the backend process boundary `<binary> <prefix>.nml` ->
+ *     `<prefix>_state3d5.bin` + `<prefix>_metrics.json`
+ *     (tools/compare_backends3d5.py:69-78, libs/cuda/src/cfd_exp3d5_cuda.cu:1104-1237)
+ *     -> oc_run_namelist() and the `ocean3d5_b200` executable;
+ *   - the stepper object `Stepper3DV05(domain, physics, params, dt)` with
+ *     `.step` / `.integrate` and its counters (libs/core/model3d_v05.py:78-545;
+ *     CUDA twin Stepper5, cfd_exp3d5_cuda.cu:915-1097)
+ *     -> oc_create / oc_set_domain / oc_set_forcing / oc_set_state / oc_step /
+ *        oc_get_state / oc_get_stats / oc_destroy;
+ *   - the variable-coefficient Helmholtz solve `HelmholtzVar.solve`
+ *     (libs/core/solvers_var.py:162-197; HelmVar::solve, cfd_exp3d5_cuda.cu:374-412)
+ *     -> oc_helmholtz_solve;
+ *   - the batched column solve `thomas_batched` (libs/core/vertical.py:17-44;
+ *     k_thomas, cfd_exp3d5_cuda.cu:450-461) -> oc_thomas;
+ *   - the equation of state `buoyancy` (libs/core/eos.py:130-133; k3_eos,
+ *     cfd_exp3d5_cuda.cu:818-850) -> oc_buoyancy.
+ */
+#ifndef OCEAN_B200_H
+#define OCEAN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+enum {
+    OC_OK = 0,
+    OC_ERR_ARG = 1,         /* invalid argument or configuration */
+    OC_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    OC_ERR_UNSUPPORTED = 3, /* option the step refuses (open boundaries, moving coordinates) */
+    OC_ERR_STATE = 4,       /* call out of order (no domain / no state yet) */
+    OC_ERR_TIMEOUT = 5,     /* a device-side wait ran out its bound */
+    OC_ERR_IO = 6           /* file missing or of the wrong size */
+};
+
+/* option codes (the namelist strings of tools/toml2nml.py:209-264) */
+enum { OC_SCHEME_FB = 0, OC_SCHEME_THETA = 1, OC_SCHEME_SPLIT = 2 };
+enum { OC_SOLVER_PCG_JACOBI = 0, OC_SOLVER_PCG_RBGS = 1, OC_SOLVER_RBGS = 2, OC_SOLVER_MULTIGRID = 3 };
+enum { OC_BC_PERIODIC = 0, OC_BC_CLOSED = 1 };
+enum { OC_FACE_MIN = 0, OC_FACE_MEAN = 1, OC_FACE_HARMONIC = 2 };
+enum { OC_EOS_LINEAR = 0, OC_EOS_SEOS = 1, OC_EOS_TEOS10 = 2 };
+enum { OC_PGF_REMOVE = 0, OC_PGF_KEEP = 1 };
+enum { OC_ADV_NONE = 0, OC_ADV_CENTERED2 = 1, OC_ADV_UPWIND1 = 2, OC_ADV_UP3 = 3, OC_ADV_UP3_TVD = 4 };
+enum { OC_TRACERS_BUOYANCY = 0, OC_TRACERS_TS = 1 };
+enum { OC_CLOSURE_NONE = 0, OC_CLOSURE_TKE = 1 };
+enum { OC_MXL_INTEGRAL = 0, OC_MXL_RECURSIVE = 1 };
+enum { OC_BTAVG_NONE = 0, OC_BTAVG_MEAN = 1 };
+
+/* Every scalar of the step; field meaning and units as the reference namelist keys. */
+typedef struct oc_config {
+    int32_t nx, ny, nz;
+    double lx, ly;
+    double g, f0, h0, n2, nu, kappa, rho0, tau_x, tau_y, bottom_drag;
+    int32_t scheme;
+    double theta, theta_cor, theta_v;
+    int32_t n_picard, n_split, barotropic_average;
+    int32_t solver;
+    double rtol;
+    int32_t max_iter;
+    double dt;
+    int32_t bc_x, bc_y, face_rule;
+    double min_partial;
+    int32_t eos, pgf, pgf_correction, advection, tracers;
+    double alpha_t, beta_s, t0, s0, cp, a_h, k_h, q_heat, q_salt;
+    int32_t closure, mxl;
+    double c_k, c_eps, pr_t, z_0, e_min, l_min, e_bb, n2_min;
+    int32_t device;
+} oc_config;
+
+/* Pointers to one model state. eta [ny][nx]; u, v, b, T, S [nz][ny][nx];
+ * e, km, kh on interfaces [nz+1][ny][nx]. T and S are ignored when
+ * tracers = buoyancy. On oc_set_state a NULL e means the reference's start
+ * value e_min (State3D.e is None, model3d_v05.py:175); a NULL km/kh keeps the
+ * handle's current viscosity/diffusivity, which persist across steps like the
+ * reference stepper's self.nu/self.kappa (nu/kappa after oc_set_domain or
+ * oc_reset_mixing); a NULL b with TS tracers means "diagnose b from T and S
+ * with the EOS". On oc_get_state NULL entries are skipped. */
+typedef struct oc_state_view {
+    double *eta, *u, *v, *b, *T, *S, *e, *km, *kh;
+} oc_state_view;
+
+/* Counters of the reference stepper (model3d_v05.py:89-94) plus run status. */
+typedef struct oc_stats {
+    int64_t steps;
+    int64_t solver_iterations;
+    int64_t solver_failures;
+    int64_t solver_rebuilds;
+    int64_t tridiagonal_solves;
+    int64_t barotropic_substeps;
+    int64_t solves;
+    int32_t n_split;
+    int32_t n_levels;          /* multigrid levels (1 for the other solvers) */
+    int32_t diverged;          /* max|eta| >= 1e6 or NaN at the last check */
+    int32_t device_status;     /* 0, or the OC_ERR_* a device-side check raised */
+    int64_t device_bytes;      /* device memory held by the handle */
+} oc_stats;
+
+typedef struct oc_handle oc_handle;
+
+const char* oc_version(void);
+
+/* Validate the configuration and bind the handle to cfg->device. */
+int oc_create(const oc_config* cfg, oc_handle** out);
+
+/* Bathymetry H and land mask [ny][nx] (host, fp64); dzr [nz] optional level
+ * thicknesses (NULL = uniform max(H)/nz as the reference). Builds masks,
+ * partial cells, face thicknesses and the static coefficients. */
+int oc_set_domain(oc_handle* h, const double* H, const double* mask, const double* dzr);
+
+/* Optional surface stress field at cell centres [ny][nx] in N m-2 (host);
+ * NULL for both keeps the scalar tau_x/tau_y of the configuration. */
+int oc_set_forcing(oc_handle* h, const double* taux_c, const double* tauy_c);
+
+/* Copy a state in (on_device = 0: host pointers, 1: device pointers). */
+int oc_set_state(oc_handle* h, const oc_state_view* s, int32_t on_device);
+
+/* Restore the constant viscosity nu and diffusivity kappa of the
+ * configuration (the stepper's state at construction). */
+int oc_reset_mixing(oc_handle* h);
+
+/* Copy the current state out (host or device pointers). Synchronises the stream. */
+int oc_get_state(oc_handle* h, const oc_state_view* s, int32_t on_device);
+
+/* Advance n_steps on `stream` (a cudaStream_t, or NULL for the legacy default stream).
+ * Asynchronous: returns once the work is enqueued. */
+int oc_step(oc_handle* h, int32_t n_steps, void* stream);
+
+/* Wait for the handle's work, then fill the counters (synchronises). */
+int oc_get_stats(oc_handle* h, oc_stats* out);
+
+/* Per-solve Helmholtz iteration counts since creation (or the last reset). */
+int oc_get_solve_log(oc_handle* h, int32_t* iterations, int32_t capacity, int32_t* n_out);
+
+/* Zero the counters and the solve log (the state is kept). */
+int oc_reset_stats(oc_handle* h);
+
+/* One Helmholtz solve with the current face coefficients: x = A^-1 rhs on
+ * device buffers [ny][nx]. *iterations receives the count (synchronises). */
+int oc_helmholtz_solve(oc_handle* h, const double* rhs, double* x, int32_t* iterations,
+                       void* stream);
+
+/* Batched tridiagonal solve on device buffers laid out [n][ncols]: one system
+ * of n rows per column, sub[0] and sup[n-1] ignored. */
+int oc_thomas(const double* sub, const double* diag, const double* sup, const double* rhs,
+              double* x, int32_t n, int32_t ncols, void* stream);
+
+/* b = -g rho'(T, S, z) / rho0 on device buffers of `count` cells, with the EOS
+ * and constants of the handle's configuration. */
+int oc_buoyancy(oc_handle* h, const double* T, const double* S, const double* z, double* b,
+                int64_t count, void* stream);
+
+/* Copy a static geometry or coefficient field to host memory: names "dz3",
+ * "mask3", "mask3u", "mask3v", "dz3u", "dz3v", "zc" ([nz][ny][nx]), "q"
+ * ([nz][ny][nx]), "ku", "kv", "mask_u", "mask_v" ([ny][nx]). */
+int oc_get_field(oc_handle* h, const char* name, double* host_out, int64_t count);
+
+/* The full backend protocol of the reference binaries: read the namelist and
+ * its bundle files, run n_warmup + n_repeat repeats of n_steps, write
+ * <out_prefix>_state3d5.bin and <out_prefix>_metrics.json. */
+int oc_run_namelist(const char* nml_path);
+
+const char* oc_last_error(const oc_handle* h);
+
+void oc_destroy(oc_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OCEAN_B200_H */

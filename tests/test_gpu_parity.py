@@ -1,0 +1,140 @@
+"""The sm_100a step against the reference: every golden case, every step.
+
+Gate (the reference's, tools/compare_backends3d5.py:28-29, applied per step):
+relative L2 < 1e-12 for every field and the per-solve Helmholtz iteration
+counts identical. The stronger claim checked beside it: every field is
+bit-identical to the reference (fingerprints of the fp64 bytes).
+"""
+
+import numpy as np
+import pytest
+
+from harness import case_inputs, fixture_names, load_fixture
+from oracle import ocean_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+GATE_TOL = 1e-12
+CASES = fixture_names()
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    import torch
+    assert torch.cuda.is_available(), "gpu tests need a CUDA device"
+    torch.cuda.set_device(0)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_bit_identical_to_reference_every_step(name):
+    from gpu_util import gpu_case, gpu_hashes
+    meta, arrays = load_fixture(name)
+    p, st = gpu_case(meta, arrays)
+    for step, want in enumerate(meta["hashes"]):
+        st.step(1)
+        got = gpu_hashes(p, st.get_state())
+        bad = [f for f, h in want.items() if got[f] != h]
+        assert not bad, f"{name}: fields {bad} differ from the reference at step {step + 1}"
+    assert st.solve_log() == meta["solve_log"]
+    stats = st.stats()
+    c = meta["counters"]
+    assert stats["solver_iterations"] == c["solver_iterations"]
+    assert stats["solver_failures"] == c["solver_failures"]
+    assert stats["solver_rebuilds"] == c["solver_rebuilds"]
+    assert stats["tridiagonal_solves"] == c["tridiagonal_solves"]
+    assert stats["barotropic_substeps"] == c["barotropic_substeps"]
+    assert stats["n_split"] == c["n_split"]
+    st.close()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_reference_gate_per_step(name):
+    """rel L2 < 1e-12 per step against the oracle, identical iteration counts."""
+    from gpu_util import gpu_case, state_errors
+    meta, arrays = load_fixture(name)
+    p, H, mask, dzr, taux, tauy, s = case_inputs(meta, arrays)
+    ref = orc.OracleStepper(p, H, mask)
+    p2, st = gpu_case(meta, arrays)
+    for step in range(meta["n_steps"]):
+        s = ref.step(s)
+        st.step(1)
+        errs = state_errors(p, st.get_state(), s)
+        worst = max(errs.values())
+        assert worst < GATE_TOL, f"{name} step {step + 1}: {errs}"
+    assert st.solve_log() == ref.solve_log
+    st.close()
+
+
+@pytest.mark.parametrize("solver", ["multigrid", "pcg_jacobi"])
+def test_stretched_levels_and_wind_field_match_oracle(solver):
+    """The benchmark's extensions (stretched levels, stress field) against the oracle."""
+    from hydrostatic_ocean_core_benchmark_b200 import cases
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    s = cases.seamount_basin(nx=32, ny=48, nz=16, seed=11, solver_kind=solver)
+    p = s.params
+    geo = orc.Geometry(p, s.H, s.mask, s.dzr)
+    b = orc.buoyancy(p.eos, s.T, s.S, geo.zc, p.g, p.rho0, p.alpha_t, p.beta_s, p.t0, p.s0) * geo.mask3
+    ref = orc.OracleStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    st = OceanStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)   # b diagnosed on the GPU
+    assert np.array_equal(st.get_state(fields=("b",))["b"], b)
+    state = orc.OracleState(s.u, s.v, b, s.eta, s.T, s.S)
+    for step in range(5):
+        state = ref.step(state)
+        st.step(1)
+        got = st.get_state()
+        for f in ("eta", "u", "v", "b", "T", "S", "e", "km", "kh"):
+            want = {"km": ref.Km, "kh": ref.Kh}.get(f, None)
+            want = getattr(state, f) if want is None else want
+            assert np.array_equal(got[f], want), f"{solver} step {step + 1}: {f} differs"
+    assert st.solve_log() == ref.solve_log
+    st.close()
+
+
+def test_benchmark_size_first_step_matches_oracle():
+    """512 x 512 x 50 seamount basin: the first step bit-identical to the oracle."""
+    from hydrostatic_ocean_core_benchmark_b200 import cases
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    s = cases.seamount_basin()
+    p = s.params
+    geo = orc.Geometry(p, s.H, s.mask, s.dzr)
+    b = orc.buoyancy(p.eos, s.T, s.S, geo.zc, p.g, p.rho0, p.alpha_t, p.beta_s, p.t0, p.s0) * geo.mask3
+    ref = orc.OracleStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    want = ref.step(orc.OracleState(s.u, s.v, b, s.eta, s.T, s.S))
+    st = OceanStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    st.set_state(eta=s.eta, u=s.u, v=s.v, b=b, T=s.T, S=s.S)
+    st.step(1)
+    got = st.get_state()
+    for f in ("eta", "u", "v", "b", "T", "S", "e"):
+        assert np.array_equal(got[f], getattr(want, f)), f
+    assert st.solve_log() == ref.solve_log
+    st.close()
+
+
+def test_full_size_properties_over_ten_steps():
+    """At the benchmark size, ten steps: deterministic, finite, uniform T stays uniform."""
+    from hydrostatic_ocean_core_benchmark_b200 import cases
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    s = cases.seamount_basin()
+    p = s.params
+    runs = []
+    for _ in range(2):
+        st = OceanStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+        st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
+        st.step(10)
+        runs.append(st.get_state())
+        stats = st.stats()
+        assert stats["solver_failures"] == 0 and not stats["diverged"]
+        st.close()
+    for f in runs[0]:
+        assert np.array_equal(runs[0][f], runs[1][f]), f"{f} not reproducible run to run"
+        assert np.all(np.isfinite(runs[0][f]))
+    # constancy: a uniform tracer stays uniform where the ocean is wet
+    st = OceanStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    T = np.where(s.T != 0, 7.0, 0.0)
+    st.set_state(eta=s.eta, u=runs[0]["u"], v=runs[0]["v"], b=runs[0]["b"], T=T, S=s.S)
+    st.step(3)
+    Tn = st.get_state(fields=("T",))["T"]
+    wet = T != 0
+    assert np.max(np.abs(Tn[wet] - 7.0)) < 1e-10
+    st.close()

@@ -1,0 +1,110 @@
+"""Unit pieces of the C ABI against the oracle: Thomas, Helmholtz, EOS, the binary protocol."""
+
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from harness import case_inputs, load_fixture
+from oracle import ocean_oracle as orc
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parents[1]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    import torch
+    assert torch.cuda.is_available()
+    torch.cuda.set_device(0)
+
+
+def test_thomas_matches_oracle_bitwise():
+    from hydrostatic_ocean_core_benchmark_b200.stepper import thomas
+    rng = np.random.default_rng(3)
+    n, cols = 37, 5000
+    sub = rng.uniform(-1, 0, (n, cols))
+    sup = rng.uniform(-1, 0, (n, cols))
+    diag = 2.5 + rng.uniform(0, 1, (n, cols))
+    rhs = rng.standard_normal((n, cols))
+    # dry-style identity rows
+    sub[:, :100] = 0.0
+    sup[:, :100] = 0.0
+    diag[:, :100] = 1.0
+    assert np.array_equal(thomas(sub, diag, sup, rhs), orc.thomas(sub, diag, sup, rhs))
+
+
+@pytest.mark.parametrize("solver", ["pcg_jacobi", "pcg_rbgs", "rbgs", "multigrid"])
+def test_helmholtz_iterations_and_solution_match(solver):
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    meta, arrays = load_fixture("seamount_basin_ref_mg")
+    p, H, mask, *_ = case_inputs(meta, arrays)
+    p = p.replace(solver_kind=solver, max_iter=4000 if solver == "rbgs" else 2000)
+    st = OceanStepper(p, H, mask)
+    ku, kv = st.field("ku"), st.field("kv")
+    ref_step = orc.OracleStepper(p, H, mask)
+    assert np.array_equal(ku, ref_step.Ku) and np.array_equal(kv, ref_step.Kv)
+    rng = np.random.default_rng(5)
+    rhs = rng.standard_normal((p.ny, p.nx))
+    x, its = st.helmholtz_solve(rhs)
+    xr, itr, ok = ref_step.solver.solve(rhs)
+    assert its == itr
+    assert np.array_equal(x, xr)
+    st.close()
+
+
+@pytest.mark.parametrize("eos", ["linear", "seos", "teos10"])
+def test_eos_bitwise(eos):
+    from hydrostatic_ocean_core_benchmark_b200.params import OceanParams
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    p = OceanParams(nx=8, ny=8, nz=4, dt=1.0, eos=eos, tracers="TS")
+    st = OceanStepper(p, np.full((8, 8), 100.0), np.ones((8, 8)))
+    rng = np.random.default_rng(9)
+    T = rng.uniform(-2, 30, 100000)
+    S = rng.uniform(0, 42, 100000)
+    z = rng.uniform(0, 6000, 100000)
+    got = st.buoyancy(T, S, z)
+    want = orc.buoyancy(eos, T, S, z, p.g, p.rho0, p.alpha_t, p.beta_s, p.t0, p.s0)
+    assert np.array_equal(got, want)
+    if eos == "teos10":
+        b = st.buoyancy(np.array([10.0]), np.array([30.0]), np.array([1000.0]))[0]
+        rho = -b * p.rho0 / p.g + p.rho0
+        assert abs(rho - 1027.45140) < 1e-4
+    st.close()
+
+
+def test_drop_in_binary_protocol(tmp_path):
+    """The executable reads a reference bundle and writes the reference's outputs."""
+    from hydrostatic_ocean_core_benchmark_b200 import bundle
+    meta, arrays = load_fixture("gate_v06_seamount_tvd_tke_theta")
+    p, H, mask, dzr, taux, tauy, s = case_inputs(meta, arrays)
+    prefix = str(tmp_path / "run")
+    nml = bundle.write_bundle(prefix, p.replace(n_steps=4, n_repeat=1, n_warmup=0, out_prefix=prefix),
+                              H, mask, s)
+    exe = ROOT / "hydrostatic_ocean_core_benchmark_b200" / "bin" / "ocean3d5_b200"
+    proc = subprocess.run([str(exe), str(nml)], capture_output=True, text=True, timeout=300)
+    assert proc.returncode == 0, proc.stderr
+    got = bundle.read_state(prefix + "_state3d5.bin", p.nx, p.ny, p.nz, p.tracers == "TS")
+    ref = orc.OracleStepper(p, H, mask).integrate(s, 4)
+    for f in ("eta", "u", "v", "b", "T", "S"):
+        assert np.array_equal(got[f], getattr(ref, f)), f
+    import json
+    metrics = json.loads(Path(prefix + "_metrics.json").read_text())
+    for key in ("backend", "gpu", "nx", "ny", "nz", "cells", "n_steps", "scheme", "solver", "eos",
+                "advection", "tracers", "theta", "dt", "solver_iterations", "solver_failures",
+                "tridiagonal_solves", "solver_rebuilds", "n_split", "barotropic_substeps",
+                "device_bytes", "bytes_per_cell", "diverged", "wall_s", "wall_mad_s", "n_repeat",
+                "omp_num_threads"):
+        assert key in metrics, key
+    assert metrics["solver_iterations"] == sum(meta["solve_log"][:8])
+
+
+def test_binary_refuses_open_boundaries(tmp_path):
+    from hydrostatic_ocean_core_benchmark_b200.params import OceanParams, write_namelist
+    p = OceanParams(nx=8, ny=8, nz=4, dt=1.0, n_steps=1, bc_x="open")
+    nml = write_namelist(tmp_path / "x.nml", p)
+    exe = ROOT / "hydrostatic_ocean_core_benchmark_b200" / "bin" / "ocean3d5_b200"
+    proc = subprocess.run([str(exe), str(nml)], capture_output=True, text=True, timeout=60)
+    assert proc.returncode != 0
+    assert "FATAL" in proc.stderr
