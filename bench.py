@@ -1,0 +1,417 @@
+#!/usr/bin/env python3
+"""Benchmark of the ocean-core time step on B200.
+
+Workload: the seeded seamount basin (512 x 512 x 50 cells, 2000 km square,
+closed, stretched levels 10 -> 250 m, double-gyre wind, TKE closure, TVD3
+advection, polyTEOS10 EOS, theta = 0.5 with the multigrid Helmholtz solver,
+dt = 600 s). A "step" is one model time step over the whole grid.
+
+Prints one JSON line. ``value`` is cell-steps/s of the device-resident state
+(all ranks, max-over-ranks device time); ``e2e`` is the same metric through the
+C-ABI with host buffers (pinned-host -> device state upload, the step, device
+-> pinned-host download, every step); ``roofline`` is the dominant kernel's
+algorithmic bandwidth against the measured HBM peak; ``cpu_baseline`` times the
+CPU oracle (a NumPy port, bit-identical to the reference's NumPy stepper) on a
+bounded sample of the same recipe.
+
+Multi-GPU: replicas only (the theta step does not shard); each rank advances
+its own replica, ``scaling`` is "weak".
+
+``--impl reference`` times the reference's own CPU implementation of the path
+(its NumPy stepper, as the bit-identical port) on the host's cores instead.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = json.loads((ROOT / "BASELINE.json").read_text())["metric"] if (ROOT / "BASELINE.json").exists() \
+    else "cell-steps/s"
+UNIT = "cell-steps/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+# ------------------------------------------------------------------ helpers
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_hbm_peak():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        try:
+            return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int, path: Path | None = None):
+        self.gpu = gpu_index
+        self.rows: list[list[str]] = []
+        self.proc = None
+        self.path = path
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        if self.path is not None:
+            self.path.write_text("\n".join(",".join(r) for r in self.rows) + "\n")
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                power.append(float(r[3]))
+            except ValueError:
+                continue
+            for n, flag in zip(names, r[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------ algorithmic bytes
+# Per-launch algorithmic bytes of each kernel class: every logical array access
+# counted once (fp64, 8 B), static geometry excluded.
+ACCESSES_PER_CELL = {
+    "closure": 10,        # reads u, v, b, e, K_m, K_h; writes e, K_m, K_h, q
+    "mom_explicit": 14,   # reads u, v, b, phi, w, K_m; writes 8 explicit-term fields
+    "predictor": 15,      # reads u, v, u_it, v_it, 8 explicit terms, K_m; writes gh_u, gh_v
+    "tracers": 9,         # reads T, S, u, v, w, K_h; writes T, S, b
+    "backsub": 5,         # reads gh_u, gh_v, q; writes u, v
+    "wcol": 3,            # reads u, v; writes w
+    "phi": 2,             # reads b; writes phi
+    "transport": 2,       # reads u, v
+    "kukv": 1,            # reads q
+}
+
+
+def mg_level_cells(nx, ny, min_size=8):
+    cells = [nx * ny]
+    while nx % 2 == 0 and ny % 2 == 0 and nx // 2 >= min_size and ny // 2 >= min_size:
+        nx, ny = nx // 2, ny // 2
+        cells.append(nx * ny)
+    return cells
+
+
+def helm_bytes_per_iteration(p):
+    """Survey accounting: PCG-Jacobi 15 arrays per column, MG V(2,2) 32 arrays per
+    cell of every level plus 4 fine arrays for the residual check."""
+    n0 = p.nx * p.ny
+    if p.solver_kind == "multigrid":
+        return 8 * (32 * sum(mg_level_cells(p.nx, p.ny)) + 4 * n0)
+    return 8 * 15 * n0
+
+
+def step_algorithmic_bytes(p, iterations_per_step):
+    """Minimal-pass bytes of one step (44 or 29 accesses per cell + the solver)."""
+    n3 = p.nx * p.ny * p.nz
+    a3 = 44 if p.closure == "tke" else 29
+    return 8 * a3 * n3 + helm_bytes_per_iteration(p) * iterations_per_step
+
+
+def dram_traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    for path in sorted((ROOT / "profiles").glob("*.md")):
+        for line in path.read_text().splitlines():
+            key = f"dram_bytes_per_launch[{kernel}]"
+            if line.strip().startswith(key):
+                try:
+                    return float(line.split("=", 1)[1].split()[0])
+                except (IndexError, ValueError):
+                    return None
+    return None
+
+
+# ------------------------------------------------------------------ workloads
+def workload(args):
+    from hydrostatic_ocean_core_benchmark_b200 import cases
+    return cases.seamount_basin(nx=args.nx, ny=args.ny, nz=args.nz, seed=args.seed)
+
+
+def cpu_oracle_rate(args, steps: int, warmup: int):
+    """cell-steps/s of the CPU oracle on a bounded sample of the same recipe."""
+    import numpy as np
+
+    from hydrostatic_ocean_core_benchmark_b200 import cases
+    from oracle import ocean_oracle as orc
+    s = cases.seamount_basin(nx=args.cpu_nx, ny=args.cpu_nx, nz=args.nz, seed=args.seed)
+    p = s.params
+    geo = orc.Geometry(p, s.H, s.mask, s.dzr)
+    b = orc.buoyancy(p.eos, s.T, s.S, geo.zc, p.g, p.rho0, p.alpha_t, p.beta_s, p.t0, p.s0) * geo.mask3
+    st = orc.OracleStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    state = orc.OracleState(s.u, s.v, b, s.eta, s.T, s.S)
+    for _ in range(warmup):
+        state = st.step(state)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        state = st.step(state)
+    dt = time.perf_counter() - t0
+    cells = p.nx * p.ny * p.nz
+    assert np.all(np.isfinite(state.eta))
+    return cells * steps / dt, dt, p
+
+
+def reference_sample_nx(args) -> int:
+    """Largest sample (columns per side) whose W + K oracle steps fit ~150 s."""
+    per_step_64 = 1.1 * args.nz / 50.0          # seconds per step at 64 x 64 columns
+    for nx in (128, 96, 64, 48, 32, 16):
+        if per_step_64 * (nx / 64.0) ** 2 * (args.steps + args.warmup) <= 150.0:
+            return nx
+    return 16
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    args.cpu_nx = min(args.cpu_nx, reference_sample_nx(args))
+    rate, secs, p = cpu_oracle_rate(args, args.steps, args.warmup)
+    sample = (f"seamount-basin recipe at {p.nx}x{p.ny}x{p.nz} (same physics, solver and seed "
+              f"as the {args.nx}x{args.ny}x{args.nz} workload), {args.warmup} warm-up + "
+              f"{args.steps} timed steps, {secs:.1f} s")
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * secs / max(1, args.steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"seamount_basin {args.nx}x{args.ny}x{args.nz}",
+                       "sample": f"{p.nx}x{p.ny}x{p.nz}"},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local_rank}"))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device=f"cuda:{local_rank}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    s = workload(args)
+    p = s.params
+    n3 = p.nx * p.ny * p.nz
+    n2 = p.nx * p.ny
+    n3i = n2 * (p.nz + 1)
+    st = OceanStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c,
+                      device=local_rank)
+    st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
+    stream = torch.cuda.Stream(device=local_rank)
+    # warm-up
+    st.step(args.warmup, stream=stream)
+    stream.synchronize()
+    st.stats()
+    log0 = len(st.solve_log())
+    launches0 = st.stats()["kernel_launches"]
+    st.kernel_times()
+    # timed region: device-resident state, events on the launching stream
+    out_dir = ROOT / "gpurun_out"
+    clocks = ClockSampler(local_rank, out_dir / f"clocks_rank{rank}.csv" if out_dir.is_dir() else None)
+    clocks.start()
+    st.set_profiling(True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    st.step(args.steps, stream=stream)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    st.set_profiling(False)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms)
+    ktimes = st.kernel_times()
+    stats = st.stats()
+    log = st.solve_log()[log0:]
+    launches = stats["kernel_launches"] - launches0
+    if stats["solver_failures"] or stats["diverged"]:
+        raise RuntimeError(f"the timed run failed: {stats}")
+    value = world * n3 * args.steps / (ms_max / 1e3)
+
+    # end to end through the C ABI with pinned host buffers, every step
+    e2e = None
+    if args.e2e_steps > 0:
+        host = st.get_state()
+        pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+                  for k, v in host.items() if k in ("eta", "u", "v", "b", "T", "S", "e")}
+        outs = {k: torch.empty_like(v).pin_memory() for k, v in pinned.items()}
+        h2d = sum(v.numel() * 8 for v in pinned.values())
+        d2h = sum(v.numel() * 8 for v in outs.values())
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        for _ in range(args.e2e_steps):
+            st.set_state(**pinned)
+            st.step(1)
+            st.get_state(out=outs)
+            pinned, outs = outs, pinned
+        e1.record(torch.cuda.default_stream())
+        e1.synchronize()
+        barrier()
+        e_ms = max_over_ranks(e0.elapsed_time(e1))
+        e2e = {"value": world * n3 * args.e2e_steps / (e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "steps": args.e2e_steps, "ms_per_step": e_ms / args.e2e_steps,
+               "path": "OceanStepper.set_state/step/get_state (oc_set_state, oc_step, oc_get_state)"}
+
+    # roofline of the dominant kernel
+    peak, peak_kind = measured_hbm_peak()
+    top = max(ktimes.items(), key=lambda kv: kv[1][1])
+    name, (nlaunch, tot_ms) = top
+    iters_per_solve = (sum(log) / len(log)) if log else 0.0
+    if name == "helm_solve":
+        alg = helm_bytes_per_iteration(p) * iters_per_solve
+    else:
+        alg = 8 * ACCESSES_PER_CELL.get(name, 0) * n3
+    per_launch_ms = tot_ms / max(1, nlaunch)
+    achieved = alg / (per_launch_ms / 1e3) / 1e9
+    traffic = dram_traffic_from_profiles(name)
+    roofline = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_ms}
+    iters_per_step = sum(log) / args.steps
+    bstep = step_algorithmic_bytes(p, iters_per_step)
+    step_gbs = bstep / (ms / args.steps / 1e3) / 1e9
+    kernel_share = {k: {"launches": v[0], "ms": v[1], "share": v[1] / max(1e-12, sum(x[1] for x in ktimes.values()))}
+                    for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1][1])}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, secs, cp = cpu_oracle_rate(args, args.cpu_steps, 1)
+        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"CPU oracle (NumPy, bit-identical port of the reference stepper) on the "
+                         f"same recipe at {cp.nx}x{cp.ny}x{cp.nz}, 1 warm-up + {args.cpu_steps} "
+                         f"steps, {secs:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded seamount-basin recipe; inputs generated on the host)",
+            "config": {"workload": f"seamount_basin {p.nx}x{p.ny}x{p.nz}, TKE + TVD3 + polyTEOS10, "
+                                   f"theta={p.theta:g} + {p.solver_kind}, dt={p.dt:g} s, stretched levels, "
+                                   f"double-gyre wind",
+                       "cells": n3, "parallelism": f"replicas x{world}", "variant": "fp64 plain path",
+                       "l2": "working set of several GB per replica, far above the 126 MB L2"},
+            "roofline": roofline,
+            "step_roofline": {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
+                              "frac": step_gbs / peak, "algorithmic_bytes_per_step": bstep,
+                              "solver_iterations_per_step": iters_per_step},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "kernels": kernel_share,
+            "solver_iterations_per_solve": iters_per_solve,
+        }
+        print(json.dumps(line), flush=True)
+    st.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nx", type=int, default=512)
+    ap.add_argument("--ny", type=int, default=512)
+    ap.add_argument("--nz", type=int, default=50)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-nx", type=int, default=128)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local_rank = env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

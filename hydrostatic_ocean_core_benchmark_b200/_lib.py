@@ -68,8 +68,12 @@ class OcStats(C.Structure):
         ("solver_rebuilds", C.c_int64), ("tridiagonal_solves", C.c_int64),
         ("barotropic_substeps", C.c_int64), ("solves", C.c_int64),
         ("n_split", C.c_int32), ("n_levels", C.c_int32), ("diverged", C.c_int32),
-        ("device_status", C.c_int32), ("device_bytes", C.c_int64),
+        ("device_status", C.c_int32), ("device_bytes", C.c_int64), ("kernel_launches", C.c_int64),
     ]
+
+
+class OcKernelTime(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("total_ms", C.c_double)]
 
 
 # every exported symbol of include/ocean_b200.h with its ctypes signature
@@ -83,6 +87,8 @@ _SIGNATURES = {
     "oc_get_state": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.c_int32]),
     "oc_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "oc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(OcStats)]),
+    "oc_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
+    "oc_get_kernel_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     "oc_get_solve_log": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     "oc_reset_stats": (C.c_int, [C.c_void_p]),
     "oc_helmholtz_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),

@@ -86,8 +86,16 @@ struct oc_handle {
     int* d_status = nullptr;
     HelmSolver* solver = nullptr;
     // host counters (model3d_v05.py:89-94)
-    long long steps = 0, tridiag = 0, rebuilds = 0, substeps = 0, solves = 0;
+    long long steps = 0, tridiag = 0, rebuilds = 0, substeps = 0, solves = 0, launches = 0;
     cudaStream_t last_stream = nullptr;
+    // optional per-kernel event timing
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<int, size_t>> ev_marks;  // (kernel class, index of the start event)
+    std::vector<std::string> prof_names;
+    std::vector<long long> prof_launches;
+    std::vector<double> prof_ms;
 };
 
 namespace {
@@ -200,7 +208,6 @@ void fill_scalars(oc_handle* h) {
     P.neg_f0 = -c.f0;
     P.neg_g = -c.g;
     P.neg_n2 = -c.n2;
-    P.dz_nom = c.h0 / c.nz;
     P.flux_t = c.q_heat / (c.rho0 * c.cp);
     P.flux_s = c.q_salt;
     const double kap = 1.0 / 3.0;
@@ -304,6 +311,58 @@ int ensure_log(oc_handle* h, long long needed, cudaStream_t s) {
     return h->solver->grow_log((int)std::min<long long>(cap, 1 << 30), s, h->err);
 }
 
+// ---- per-kernel event timing
+void prof_harvest(oc_handle* h) {
+    if (h->ev_marks.empty()) return;
+    cudaEventSynchronize(h->ev_pool[h->ev_used - 1]);
+    for (const auto& m : h->ev_marks) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, h->ev_pool[m.second], h->ev_pool[m.second + 1]);
+        h->prof_ms[m.first] += ms;
+    }
+    h->ev_marks.clear();
+    h->ev_used = 0;
+}
+
+int prof_class(oc_handle* h, const char* name) {
+    for (size_t i = 0; i < h->prof_names.size(); ++i)
+        if (h->prof_names[i] == name) return (int)i;
+    h->prof_names.push_back(name);
+    h->prof_launches.push_back(0);
+    h->prof_ms.push_back(0.0);
+    return (int)h->prof_names.size() - 1;
+}
+
+// brackets one kernel (or one fixed group of kernels) with events
+struct Prof {
+    oc_handle* h;
+    cudaStream_t s;
+    int cls = -1;
+    size_t idx = 0;
+    Prof(oc_handle* h_, cudaStream_t s_, const char* name, int n_kernels = 1) : h(h_), s(s_) {
+        h->launches += n_kernels;
+        if (!h->profiling) return;
+        cls = prof_class(h, name);
+        h->prof_launches[cls] += n_kernels;
+        if (h->ev_used + 2 > h->ev_pool.size()) prof_harvest(h);
+        if (h->ev_pool.size() < h->ev_used + 2) {
+            cudaEvent_t a, b;
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            h->ev_pool.push_back(a);
+            h->ev_pool.push_back(b);
+        }
+        idx = h->ev_used;
+        h->ev_used += 2;
+        cudaEventRecord(h->ev_pool[idx], s);
+    }
+    ~Prof() {
+        if (cls < 0) return;
+        cudaEventRecord(h->ev_pool[idx + 1], s);
+        h->ev_marks.push_back({cls, idx});
+    }
+};
+
 // one step (model3d_v05.py:337-415)
 int step_once(oc_handle* h, cudaStream_t s) {
     const oc_config& c = h->cfg;
@@ -313,24 +372,27 @@ int step_once(oc_handle* h, cudaStream_t s) {
     double *un = h->U[nxt], *vn = h->V[nxt], *etan = h->ETA[nxt];
     const bool theta = c.scheme == OC_SCHEME_THETA, split = c.scheme == OC_SCHEME_SPLIT;
     if (c.closure == OC_CLOSURE_TKE) {
-        launch_closure(P, u, v, b, h->e, h->km, h->kh, h->q, s);
+        { Prof pr(h, s, "closure"); launch_closure(P, u, v, b, h->e, h->km, h->kh, h->q, s); }
         h->tridiag += 2;
-        launch_kukv(P, h->q, h->Ku, h->Kv, s);
+        { Prof pr(h, s, "kukv"); launch_kukv(P, h->q, h->Ku, h->Kv, s); }
         if (theta) {
-            h->solver->rebuild(s);
+            { Prof pr(h, s, "helm_rebuild", h->solver->n_levels()); h->solver->rebuild(s); }
             h->rebuilds += 1;
         }
     }
-    launch_wcol(P, u, v, h->w, s);
-    launch_phi(P, b, h->phi, s);
-    launch_mom_explicit(P, u, v, b, h->phi, h->w, h->km, h->pgx, h->pgy, h->avpv, h->avpu, h->dzu,
-                        h->dzv, h->stu, h->stv, s);
-    if (!split) launch_grad2(P, eta, h->gx2, h->gy2, s);
-    if (theta) {
-        launch_transport(P, u, v, h->Uold, h->Vold, s);
-        launch_div2(P, h->Uold, h->Vold, h->div_old, s);
+    { Prof pr(h, s, "wcol"); launch_wcol(P, u, v, h->w, s); }
+    { Prof pr(h, s, "phi"); launch_phi(P, b, h->phi, s); }
+    {
+        Prof pr(h, s, "mom_explicit");
+        launch_mom_explicit(P, u, v, b, h->phi, h->w, h->km, h->pgx, h->pgy, h->avpv, h->avpu, h->dzu,
+                            h->dzv, h->stu, h->stv, s);
     }
-    if (split) launch_transport(P, u, v, h->bt[0], h->bt[1], s);  // U0, V0
+    if (!split) { Prof pr(h, s, "grad2"); launch_grad2(P, eta, h->gx2, h->gy2, s); }
+    if (theta) {
+        { Prof pr(h, s, "transport"); launch_transport(P, u, v, h->Uold, h->Vold, s); }
+        { Prof pr(h, s, "div2"); launch_div2(P, h->Uold, h->Vold, h->div_old, s); }
+    }
+    if (split) { Prof pr(h, s, "transport"); launch_transport(P, u, v, h->bt[0], h->bt[1], s); }  // U0, V0
     const double *uit = u, *vit = v;
     double *last_gu = nullptr, *last_gv = nullptr;
     for (int m = 0; m < c.n_picard; ++m) {
@@ -346,19 +408,25 @@ int step_once(oc_handle* h, cudaStream_t s) {
             tu = (m % 2 == 0) ? h->ghu : h->uit;
             tv = (m % 2 == 0) ? h->ghv : h->vit;
         }
-        launch_predictor(P, u, v, uit, vit, h->pgx, h->pgy, h->avpv, h->avpu, h->dzu, h->dzv, h->stu,
-                         h->stv, h->gx2, h->gy2, h->km, tu, tv, h->Ug, h->Vg, s);
+        {
+            Prof pr(h, s, "predictor");
+            launch_predictor(P, u, v, uit, vit, h->pgx, h->pgy, h->avpv, h->avpu, h->dzu, h->dzv, h->stu,
+                             h->stv, h->gx2, h->gy2, h->km, tu, tv, h->Ug, h->Vg, s);
+        }
         h->tridiag += 2;
         if (theta) {
-            launch_helm_rhs(P, eta, h->div_old, h->Ug, h->Vg, h->rhs2, s);
+            { Prof pr(h, s, "helm_rhs"); launch_helm_rhs(P, eta, h->div_old, h->Ug, h->Vg, h->rhs2, s); }
             int rc = ensure_log(h, h->solves + 1, s);
             if (rc) return rc;
-            rc = h->solver->solve(h->rhs2, etan, s, h->err);
+            {
+                Prof pr(h, s, "helm_solve");
+                rc = h->solver->solve(h->rhs2, etan, s, h->err);
+            }
             if (rc) return rc;
             h->solves += 1;
             double* ou = last ? un : h->uit;
             double* ov = last ? vn : h->vit;
-            launch_backsub(P, h->ghu, h->ghv, h->q, etan, ou, ov, s);
+            { Prof pr(h, s, "backsub"); launch_backsub(P, h->ghu, h->ghv, h->q, etan, ou, ov, s); }
             uit = ou;
             vit = ov;
         } else {
@@ -368,44 +436,48 @@ int step_once(oc_handle* h, cudaStream_t s) {
             last_gv = tv;
         }
     }
-    if (c.scheme == OC_SCHEME_FB) launch_eta_fb(P, eta, h->Ug, h->Vg, etan, s);
+    if (c.scheme == OC_SCHEME_FB) { Prof pr(h, s, "eta_fb"); launch_eta_fb(P, eta, h->Ug, h->Vg, etan, s); }
     if (split) {
         double *U0 = h->bt[0], *V0 = h->bt[1], *fx = h->bt[2], *fy = h->bt[3];
         double *avv = h->bt[4], *avu = h->bt[5], *gxe = h->bt[6], *gye = h->bt[7];
         double* Ub[3] = {h->bt[8], h->bt[10], h->Uold};
         double* Vb[3] = {h->bt[9], h->bt[11], h->Vold};
         double *accu = h->gx2, *accv = h->gy2;
-        launch_split_forcing(P, U0, V0, h->Ug, h->Vg, fx, fy, s);
+        { Prof pr(h, s, "split_forcing"); launch_split_forcing(P, U0, V0, h->Ug, h->Vg, fx, fy, s); }
         cudaMemcpyAsync(etan, eta, h->n2 * sizeof(double), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(Ub[0], U0, h->n2 * sizeof(double), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(Vb[0], V0, h->n2 * sizeof(double), cudaMemcpyDeviceToDevice, s);
         const double ddt = c.dt / h->n_split;
         int ib = 0;
         for (int n = 0; n < h->n_split; ++n) {
-            launch_split_sub_avg(P, Ub[ib], Vb[ib], etan, avv, avu, gxe, gye, s);
+            { Prof pr(h, s, "split_sub_avg"); launch_split_sub_avg(P, Ub[ib], Vb[ib], etan, avv, avu, gxe, gye, s); }
             int ii = ib;
             for (int qi = 0; qi < c.n_picard; ++qi) {
                 int io = 0;
                 while (io == ib || io == ii) ++io;
+                Prof pr(h, s, "split_sub_mom");
                 launch_split_sub_mom(P, ddt, Ub[ib], Vb[ib], Ub[ii], Vb[ii], avv, avu, gxe, gye, h->Ku,
                                      h->Kv, fx, fy, Ub[io], Vb[io], s);
                 ii = io;
             }
             ib = ii;
-            launch_split_sub_eta(P, ddt, Ub[ib], Vb[ib], etan, accu, accv, n == 0 ? 1 : 0, s);
+            { Prof pr(h, s, "split_sub_eta"); launch_split_sub_eta(P, ddt, Ub[ib], Vb[ib], etan, accu, accv, n == 0 ? 1 : 0, s); }
         }
         h->substeps += h->n_split;
         const double *Uf = Ub[ib], *Vf = Vb[ib];
         if (c.barotropic_average == OC_BTAVG_MEAN) {
-            launch_split_mean(P, h->n_split, accu, accv, s);
+            { Prof pr(h, s, "split_mean"); launch_split_mean(P, h->n_split, accu, accv, s); }
             Uf = accu;
             Vf = accv;
         }
-        launch_split_correct(P, last_gu, last_gv, h->Ug, h->Vg, Uf, Vf, un, vn, s);
+        { Prof pr(h, s, "split_correct"); launch_split_correct(P, last_gu, last_gv, h->Ug, h->Vg, Uf, Vf, un, vn, s); }
     }
-    launch_wcol(P, un, vn, h->w, s);
-    launch_tracers(P, h->Tt[cur], h->Ss[cur], b, un, vn, h->w, h->kh, h->Tt[nxt], h->Ss[nxt], h->B[nxt],
-                   s);
+    { Prof pr(h, s, "wcol"); launch_wcol(P, un, vn, h->w, s); }
+    {
+        Prof pr(h, s, "tracers");
+        launch_tracers(P, h->Tt[cur], h->Ss[cur], b, un, vn, h->w, h->kh, h->Tt[nxt], h->Ss[nxt], h->B[nxt],
+                       s);
+    }
     h->tridiag += (c.tracers == OC_TRACERS_TS) ? 2 : 1;
     h->cur = nxt;
     h->steps += 1;
@@ -487,6 +559,7 @@ int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const dou
         P.edge[k + 1] = (k == 0) ? h->dzr[0] : P.edge[k] + h->dzr[k];
         P.dzr[k] = h->dzr[k];
         P.thin[k] = h->cfg.min_partial * h->dzr[k];
+        P.dz_nom[k] = h->cfg.h0 / nz;  // the reference's nominal H/nz (model3d_v05.py:247)
     }
     build_host_geometry(h);
     if (h->cfg.scheme == OC_SCHEME_SPLIT) {
@@ -707,6 +780,7 @@ int oc_get_stats(oc_handle* h, oc_stats* out) {
     out->n_levels = h->solver ? h->solver->n_levels() : 0;
     out->device_bytes = (int64_t)(h->bytes + (h->solver ? h->solver->bytes() : 0));
     out->device_status = h->has_domain ? device_status(h) : 0;
+    out->kernel_launches = h->launches;
     if (h->solver && h->solves > 0) {
         const int n = (int)std::min<long long>(h->solves, h->solver->log_capacity());
         std::vector<int> it(n), cv(n);
@@ -746,7 +820,7 @@ int oc_reset_stats(oc_handle* h) {
     if (!h) return OC_ERR_ARG;
     cudaSetDevice(h->cfg.device);
     cudaDeviceSynchronize();
-    h->steps = h->tridiag = h->rebuilds = h->substeps = h->solves = 0;
+    h->steps = h->tridiag = h->rebuilds = h->substeps = h->solves = h->launches = 0;
     if (h->solver) cudaMemset(h->solver->d_log_count(), 0, sizeof(int));
     return OC_OK;
 }
@@ -826,6 +900,34 @@ int oc_get_field(oc_handle* h, const char* name, double* out, int64_t count) {
     return e == cudaSuccess ? OC_OK : cuda_fail(h, e, "oc_get_field");
 }
 
+int oc_set_profiling(oc_handle* h, int32_t enable) {
+    if (!h) return OC_ERR_ARG;
+    cudaSetDevice(h->cfg.device);
+    if (!enable) prof_harvest(h);
+    h->profiling = enable != 0;
+    return OC_OK;
+}
+
+int oc_get_kernel_times(oc_handle* h, oc_kernel_time* out, int32_t capacity, int32_t* n_out) {
+    if (!h || !n_out) return OC_ERR_ARG;
+    cudaSetDevice(h->cfg.device);
+    cudaDeviceSynchronize();
+    prof_harvest(h);
+    const int n = (int)h->prof_names.size();
+    *n_out = n;
+    for (int i = 0; i < n && i < capacity && out; ++i) {
+        std::memset(out[i].name, 0, sizeof(out[i].name));
+        std::strncpy(out[i].name, h->prof_names[i].c_str(), sizeof(out[i].name) - 1);
+        out[i].launches = h->prof_launches[i];
+        out[i].total_ms = h->prof_ms[i];
+    }
+    for (int i = 0; i < n; ++i) {
+        h->prof_launches[i] = 0;
+        h->prof_ms[i] = 0.0;
+    }
+    return OC_OK;
+}
+
 const char* oc_last_error(const oc_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
 void oc_destroy(oc_handle* h) {
@@ -834,6 +936,7 @@ void oc_destroy(oc_handle* h) {
     cudaDeviceSynchronize();
     delete h->solver;
     for (void* p : h->allocs) cudaFree(p);
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     delete h;
 }
 

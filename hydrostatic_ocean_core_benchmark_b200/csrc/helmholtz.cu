@@ -22,7 +22,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/ocean_b200.h"
+#include "ocean_b200.h"
 #include "helmholtz.cuh"
 
 namespace oc {

@@ -46,13 +46,13 @@ struct KP {
     double neg_f0;        // -f0
     double neg_g;         // -g
     double neg_n2;        // -N2
-    double dz_nom;        // h0 / nz, the nominal spacing of momentum vertical advection
     double flux_t, flux_s;  // surface tracer fluxes
     double one_m_kappa3, one_p_kappa3;  // 1 - 1/3, 1 + 1/3
     // level table
     double edge[OC_MAXNZ + 1];   // depth of level tops, cumsum of dzr
     double dzr[OC_MAXNZ];
     double thin[OC_MAXNZ];       // min_partial * dzr
+    double dz_nom[OC_MAXNZ];     // spacing of the momentum vertical advection per level
     // static 2D fields
     const double* H;
     const double* mask;

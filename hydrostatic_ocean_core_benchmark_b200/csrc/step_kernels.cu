@@ -485,7 +485,7 @@ __device__ double mom_adv_u(const KP& P, const Nbr& nb, const double* __restrict
             const bool hd = (kk + 1 <= nz - 1) && m3u_at(P, nb, 0, 0, kk + 1) > 0.0;
             fz[t] = wb * kappa_face_z(P, fu, Uk(kk - 1), Uk(kk), fd, wb, hu, hd, lim);
         }
-        az = (fz[0] - fz[1]) / P.dz_nom;
+        az = (fz[0] - fz[1]) / P.dz_nom[k];
     } else {
         const double ub_c0 = 0.5 * (U(0, -1) + U(0, 0));
         const double ub_c1 = 0.5 * (U(0, 0) + U(0, 1));
@@ -505,7 +505,7 @@ __device__ double mom_adv_u(const KP& P, const Nbr& nb, const double* __restrict
             const double wb = 0.5 * (W(kk, 0) + W(kk, 1));
             fz[t] = wb * 0.5 * (Uk(kk - 1) + Uk(kk));
         }
-        az = (fz[0] - fz[1]) / P.dz_nom;
+        az = (fz[0] - fz[1]) / P.dz_nom[k];
     }
     return ax + ay + az;
 }
@@ -552,7 +552,7 @@ __device__ double mom_adv_v(const KP& P, const Nbr& nb, const double* __restrict
             const bool hd = (kk + 1 <= nz - 1) && m3v_at(P, nb, 0, 0, kk + 1) > 0.0;
             fz[t] = wb * kappa_face_z(P, fu, Vk(kk - 1), Vk(kk), fd, wb, hu, hd, lim);
         }
-        bz = (fz[0] - fz[1]) / P.dz_nom;
+        bz = (fz[0] - fz[1]) / P.dz_nom[k];
     } else {
         const double vb_c0 = 0.5 * (V(-1, 0) + V(0, 0));
         const double vb_c1 = 0.5 * (V(0, 0) + V(1, 0));
@@ -572,7 +572,7 @@ __device__ double mom_adv_v(const KP& P, const Nbr& nb, const double* __restrict
             const double wb = 0.5 * (W(kk, 0) + W(kk, 1));
             fz[t] = wb * 0.5 * (Vk(kk - 1) + Vk(kk));
         }
-        bz = (fz[0] - fz[1]) / P.dz_nom;
+        bz = (fz[0] - fz[1]) / P.dz_nom[k];
     }
     return bx + by + bz;
 }

@@ -150,6 +150,17 @@ class OceanStepper:
         self._call("oc_get_stats", self.lib.oc_get_stats, self.h, C.byref(st))
         return {name: getattr(st, name) for name, _ in st._fields_}
 
+    def set_profiling(self, enable: bool = True):
+        self._call("oc_set_profiling", self.lib.oc_set_profiling, self.h, 1 if enable else 0)
+
+    def kernel_times(self) -> dict:
+        """{kernel class: (launches, total device ms)} since the last call; synchronises."""
+        buf = (_lib.OcKernelTime * 64)()
+        n = C.c_int32()
+        self._call("oc_get_kernel_times", self.lib.oc_get_kernel_times, self.h, buf, 64, C.byref(n))
+        return {buf[i].name.decode(): (int(buf[i].launches), float(buf[i].total_ms))
+                for i in range(min(n.value, 64))}
+
     def solve_log(self) -> list[int]:
         n = C.c_int32()
         self._call("oc_get_solve_log", self.lib.oc_get_solve_log, self.h, None, 0, C.byref(n))

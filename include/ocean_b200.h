@@ -105,7 +105,15 @@ typedef struct oc_stats {
     int32_t diverged;          /* max|eta| >= 1e6 or NaN at the last check */
     int32_t device_status;     /* 0, or the OC_ERR_* a device-side check raised */
     int64_t device_bytes;      /* device memory held by the handle */
+    int64_t kernel_launches;   /* kernels this library launched since creation / reset */
 } oc_stats;
+
+/* Accumulated device time of one kernel class (oc_set_profiling). */
+typedef struct oc_kernel_time {
+    char name[32];
+    int64_t launches;
+    double total_ms;
+} oc_kernel_time;
 
 typedef struct oc_handle oc_handle;
 
@@ -139,6 +147,12 @@ int oc_step(oc_handle* h, int32_t n_steps, void* stream);
 
 /* Wait for the handle's work, then fill the counters (synchronises). */
 int oc_get_stats(oc_handle* h, oc_stats* out);
+
+/* Per-kernel device timing: when enabled, every launch of oc_step is bracketed
+ * by CUDA events on its stream. oc_get_kernel_times synchronises, returns the
+ * accumulated times per kernel class and clears them. */
+int oc_set_profiling(oc_handle* h, int32_t enable);
+int oc_get_kernel_times(oc_handle* h, oc_kernel_time* out, int32_t capacity, int32_t* n_out);
 
 /* Per-solve Helmholtz iteration counts since creation (or the last reset). */
 int oc_get_solve_log(oc_handle* h, int32_t* iterations, int32_t capacity, int32_t* n_out);
