@@ -15,7 +15,7 @@ LIB_PATH = Path(__file__).resolve().parent / "lib" / "libocean_b200.so"
 
 OC_OK = 0
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "unsupported option", 4: "call out of order",
-          5: "device-side wait timed out", 6: "I/O error"}
+          5: "device-side wait timed out", 6: "I/O error", 7: "request above a fixed buffer size"}
 
 SCHEMES = {"fb": 0, "theta": 1, "split_explicit": 2}
 SOLVERS = {"pcg_jacobi": 0, "pcg_rbgs": 1, "rbgs": 2, "multigrid": 3}
@@ -95,6 +95,8 @@ _SIGNATURES = {
                                      C.c_void_p]),
     "oc_thomas": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                             C.c_int32, C.c_int32, C.c_void_p]),
+    "oc_thomas_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_int32, C.c_int32, C.c_void_p]),
     "oc_buoyancy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                               C.c_int64, C.c_void_p]),
     "oc_get_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),

@@ -21,7 +21,7 @@ LIB_DIR = PKG / "lib"
 BIN_DIR = PKG / "bin"
 LIB = LIB_DIR / "libocean_b200.so"
 EXE = BIN_DIR / "ocean3d5_b200"
-SOURCES = ["step_kernels.cu", "helmholtz.cu", "capi.cu", "protocol.cpp"]
+SOURCES = ["step_kernels.cu", "helmholtz.cu", "capi.cu", "thomas_noalloc.cu", "protocol.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--extended-lambda",
          "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{ROOT / 'include'}", f"-I{CSRC}"]

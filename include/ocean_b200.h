@@ -42,7 +42,8 @@ enum {
     OC_ERR_UNSUPPORTED = 3, /* option the step refuses (open boundaries, moving coordinates) */
     OC_ERR_STATE = 4,       /* call out of order (no domain / no state yet) */
     OC_ERR_TIMEOUT = 5,     /* a device-side wait ran out its bound */
-    OC_ERR_IO = 6           /* file missing or of the wrong size */
+    OC_ERR_IO = 6,          /* file missing or of the wrong size */
+    OC_ERR_TOO_LARGE = 7    /* request larger than a fixed-size buffer of the library */
 };
 
 /* option codes (the namelist strings of tools/toml2nml.py:209-264) */
@@ -169,6 +170,20 @@ int oc_helmholtz_solve(oc_handle* h, const double* rhs, double* x, int32_t* iter
  * of n rows per column, sub[0] and sup[n-1] ignored. */
 int oc_thomas(const double* sub, const double* diag, const double* sup, const double* rhs,
               double* x, int32_t n, int32_t ncols, void* stream);
+
+/* The batched tridiagonal solve of oc_thomas for callers that cannot allocate
+ * device memory (a host that fixes its device footprint at start-up, or an
+ * asynchronous pipeline that cannot afford the device-wide synchronisation of
+ * cudaMalloc/cudaFree). No counterpart in the reference. Its scratch is a fixed
+ * array of OC_THOMAS_NOALLOC_MAX_CELLS doubles (8 MiB) that every GPU loading
+ * the library holds until exit; n * ncols above that returns OC_ERR_TOO_LARGE.
+ * It calls no allocator. The first call on a device looks up the array's device
+ * address, so make it before any stream capture. Work is enqueued on `stream`
+ * and not waited for; calls that can overlap on the GPU share the array and
+ * race, so the caller serialises them. */
+#define OC_THOMAS_NOALLOC_MAX_CELLS 1048576
+int oc_thomas_noalloc(const double* sub, const double* diag, const double* sup, const double* rhs,
+                      double* x, int32_t n, int32_t ncols, void* stream);
 
 /* b = -g rho'(T, S, z) / rho0 on device buffers of `count` cells, with the EOS
  * and constants of the handle's configuration. */
