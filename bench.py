@@ -125,15 +125,17 @@ class ClockSampler:
 # Per-launch algorithmic bytes of each kernel class: every logical array access
 # counted once (fp64, 8 B), static geometry excluded.
 ACCESSES_PER_CELL = {
-    "closure": 10,        # reads u, v, b, e, K_m, K_h; writes e, K_m, K_h, q
-    "mom_explicit": 14,   # reads u, v, b, phi, w, K_m; writes 8 explicit-term fields
-    "predictor": 15,      # reads u, v, u_it, v_it, 8 explicit terms, K_m; writes gh_u, gh_v
-    "tracers": 9,         # reads T, S, u, v, w, K_h; writes T, S, b
-    "backsub": 5,         # reads gh_u, gh_v, q; writes u, v
-    "wcol": 3,            # reads u, v; writes w
-    "phi": 2,             # reads b; writes phi
-    "transport": 2,       # reads u, v
-    "kukv": 1,            # reads q
+    "closure": 10,          # reads u, v, b, e, K_m, K_h; writes e, K_m, K_h, q
+    "mom_explicit": 14,     # reads u, v, b, phi, w, K_m; writes 8 explicit-term fields
+    "predictor_rhs": 14,    # reads u, v, u_it, v_it, 8 explicit terms; writes r_u, r_v
+    "momentum_solve": 5,    # reads r_u, r_v, K_m; writes gh_u, gh_v
+    "tracer_rhs": 8,        # reads T, S, u, v, w, K_h; writes r_T, r_S
+    "tracer_solve": 6,      # reads r_T, r_S, K_h; writes T, S, b
+    "backsub": 5,           # reads gh_u, gh_v, q; writes u, v
+    "wcol": 3,              # reads u, v; writes w
+    "phi": 2,               # reads b; writes phi
+    "transport": 2,         # reads u, v
+    "kukv": 1,              # reads q
 }
 
 

@@ -409,10 +409,11 @@ int step_once(oc_handle* h, cudaStream_t s) {
             tv = (m % 2 == 0) ? h->ghv : h->vit;
         }
         {
-            Prof pr(h, s, "predictor");
-            launch_predictor(P, u, v, uit, vit, h->pgx, h->pgy, h->avpv, h->avpu, h->dzu, h->dzv, h->stu,
-                             h->stv, h->gx2, h->gy2, h->km, tu, tv, h->Ug, h->Vg, s);
+            Prof pr(h, s, "predictor_rhs");
+            launch_predictor_rhs(P, u, v, uit, vit, h->pgx, h->pgy, h->avpv, h->avpu, h->dzu, h->dzv,
+                                 h->stu, h->stv, h->gx2, h->gy2, tu, tv, s);
         }
+        { Prof pr(h, s, "momentum_solve"); launch_momentum_solve(P, h->km, tu, tv, h->Ug, h->Vg, s); }
         h->tridiag += 2;
         if (theta) {
             { Prof pr(h, s, "helm_rhs"); launch_helm_rhs(P, eta, h->div_old, h->Ug, h->Vg, h->rhs2, s); }
@@ -474,9 +475,13 @@ int step_once(oc_handle* h, cudaStream_t s) {
     }
     { Prof pr(h, s, "wcol"); launch_wcol(P, un, vn, h->w, s); }
     {
-        Prof pr(h, s, "tracers");
-        launch_tracers(P, h->Tt[cur], h->Ss[cur], b, un, vn, h->w, h->kh, h->Tt[nxt], h->Ss[nxt], h->B[nxt],
-                       s);
+        // the explicit momentum terms are dead by now: their buffers hold the tracer right-hand sides
+        Prof pr(h, s, "tracer_rhs");
+        launch_tracer_rhs(P, h->Tt[cur], h->Ss[cur], b, un, vn, h->w, h->kh, h->pgx, h->pgy, s);
+    }
+    {
+        Prof pr(h, s, "tracer_solve");
+        launch_tracer_solve(P, h->pgx, h->pgy, h->kh, h->Tt[nxt], h->Ss[nxt], h->B[nxt], s);
     }
     h->tridiag += (c.tracers == OC_TRACERS_TS) ? 2 : 1;
     h->cur = nxt;
@@ -562,6 +567,34 @@ int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const dou
         P.dz_nom[k] = h->cfg.h0 / nz;  // the reference's nominal H/nz (model3d_v05.py:247)
     }
     build_host_geometry(h);
+    // compact per-column form of the z-level geometry (kfull, kb, two explicit
+    // thicknesses), accepted only where it reproduces the formula exactly
+    std::vector<int2> kinfo(n2);
+    std::vector<double2> dzx(n2);
+    std::vector<int2> kface(n2);
+    for (size_t c = 0; c < n2; ++c) {
+        if (h->mask[c] != 0.0 && h->mask[c] != 1.0) return fail(h, OC_ERR_ARG, "mask values must be 0 or 1");
+        int kb = 0;
+        while (kb < nz && h->mask3[(size_t)kb * n2 + c] > 0.0) ++kb;
+        for (int k = kb; k < nz; ++k)
+            if (h->mask3[(size_t)k * n2 + c] > 0.0)
+                return fail(h, OC_ERR_UNSUPPORTED, "a column has a dry level above a wet one");
+        int kf = 0;
+        while (kf < kb && h->dz3[(size_t)kf * n2 + c] == h->dzr[kf]) ++kf;
+        if (kb - kf > 2)
+            return fail(h, OC_ERR_UNSUPPORTED, "a column has more than two partial levels");
+        kinfo[c] = make_int2(kf, kb);
+        int ku = 0, kv = 0;
+        while (ku < nz && h->mask3u[(size_t)ku * n2 + c] > 0.0) ++ku;
+        while (kv < nz && h->mask3v[(size_t)kv * n2 + c] > 0.0) ++kv;
+        for (int k = 0; k < nz; ++k)
+            if (h->mask3u[(size_t)k * n2 + c] != (k < ku ? 1.0 : 0.0) ||
+                h->mask3v[(size_t)k * n2 + c] != (k < kv ? 1.0 : 0.0))
+                return fail(h, OC_ERR_UNSUPPORTED, "a face mask is not a contiguous top block of 0/1 levels");
+        kface[c] = make_int2(ku, kv);
+        dzx[c] = make_double2(kf < kb ? h->dz3[(size_t)kf * n2 + c] : 0.0,
+                              kf + 1 < kb ? h->dz3[(size_t)(kf + 1) * n2 + c] : 0.0);
+    }
     if (h->cfg.scheme == OC_SCHEME_SPLIT) {
         const double cc = std::sqrt(h->cfg.g * hmax);
         const double dt_baro = 1.0 / (cc * std::sqrt(1.0 / std::pow(P.dx, 2.0) + 1.0 / std::pow(P.dy, 2.0)));
@@ -579,6 +612,9 @@ int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const dou
     h->d_tau_u = dalloc(h, n2);
     h->d_tau_v = dalloc(h, n2);
     h->d_ustar2 = dalloc(h, n2);
+    double* d_kinfo = dalloc(h, n2);
+    double* d_dzx = dalloc(h, 2 * n2);
+    double* d_kface = dalloc(h, n2);
     const bool ts = h->cfg.tracers == OC_TRACERS_TS;
     for (int t = 0; t < 2; ++t) {
         h->U[t] = dalloc(h, n3);
@@ -621,6 +657,12 @@ int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const dou
     P.tau_u = h->d_tau_u;
     P.tau_v = h->d_tau_v;
     P.ustar2 = h->d_ustar2;
+    cudaMemcpy(d_kinfo, kinfo.data(), n2 * sizeof(int2), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_dzx, dzx.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice);
+    P.kinfo = reinterpret_cast<const int2*>(d_kinfo);
+    P.dzx = reinterpret_cast<const double2*>(d_dzx);
+    cudaMemcpy(d_kface, kface.data(), n2 * sizeof(int2), cudaMemcpyHostToDevice);
+    P.kface = reinterpret_cast<const int2*>(d_kface);
     int rc = upload_stress(h);
     if (rc) return rc;
     fill(h->e, h->cfg.e_min, (int64_t)n3i, 0);

@@ -13,7 +13,9 @@
 // Grid-wide barriers are bounded spins: after ~1 s without progress a CTA sets
 // OC_ERR_TIMEOUT in the status word and every CTA leaves the solve.
 //
-// Multigrid levels up to 64x64 cells run inside CTA 0 with block barriers.
+// Multigrid fine levels run as shared-memory tiles with a redundant halo (two
+// grid barriers per level and V-cycle); levels of at most 32x32 cells run
+// inside CTA 0's shared memory.
 
 #include <cooperative_groups.h>
 
@@ -28,7 +30,13 @@
 namespace oc {
 
 static constexpr long long kBarrierCycles = 2000000000LL;
-static constexpr int kCoarseCells = 4096;
+static constexpr int kCoarseCells = 1024;
+// fine-level tiles: interior TILE x TILE cells plus a halo of HALO cells, enough
+// for four red-black half-sweeps and one residual on a shrinking region
+static constexpr int TILE = 32;
+static constexpr int HALO = 5;
+static constexpr int RW = TILE + 2 * HALO;
+static constexpr int RN = RW * RW;
 
 // ------------------------------------------------------------------ barrier
 __device__ __forceinline__ bool grid_sync(const HelmParams& H) {
@@ -98,20 +106,6 @@ __device__ __forceinline__ double gs_at(const HLevel& L, const double* x, const 
     return L.inv_diag[c.e] * (__ldcg(b + c.e) + nb);
 }
 
-// the same after the coarse correction x + prolong(xc) * mask of the neighbours
-__device__ __forceinline__ double corrected(const HLevel& L, const HLevel& C, const double* x, int e) {
-    const int j = e / L.nx, i = e - j * L.nx;
-    const double ec = __ldcg(C.x + (j >> 1) * C.nx + (i >> 1));
-    return __ldcg(x + e) + ec * L.mask[e];
-}
-
-__device__ __forceinline__ double gs_at_prolonged(const HLevel& L, const HLevel& C, const double* x,
-                                                  const double* b, const Cell& c) {
-    const double nb = L.cx * (L.Ku[c.e] * corrected(L, C, x, c.ie) + L.Ku[c.iw] * corrected(L, C, x, c.iw)) +
-                      L.cy * (L.Kv[c.e] * corrected(L, C, x, c.jn) + L.Kv[c.js] * corrected(L, C, x, c.js));
-    return L.inv_diag[c.e] * (__ldcg(b + c.e) + nb);
-}
-
 __device__ __forceinline__ bool is_colour(const HLevel& L, int e, int colour) {
     const int j = e / L.nx, i = e - j * L.nx;
     return ((i + j) & 1) == colour;
@@ -145,30 +139,6 @@ __device__ void colour_phase(const HLevel& L, double* x, const double* b, int co
         if (!is_colour(L, e, colour)) continue;
         const Cell c = cell_of(L, e);
         x[e] = gs_at(L, x, b, c) * L.mask[e];
-    }
-}
-
-__device__ void colour_phase_prolonged(const HLevel& L, const HLevel& C, double* x, const double* b,
-                                       int colour, Team t) {
-    for (int e = t.first; e < L.n; e += t.stride) {
-        if (!is_colour(L, e, colour)) continue;
-        const Cell c = cell_of(L, e);
-        x[e] = gs_at_prolonged(L, C, x, b, c) * L.mask[e];
-    }
-}
-
-// coarse rhs = restrict((b - A x) mask), coarse x = 0 (solvers_var.py:143-147)
-__device__ void restrict_phase(const HLevel& L, const HLevel& C, double coef, Team t) {
-    for (int ec = t.first; ec < C.n; ec += t.stride) {
-        const int J = ec / C.nx, I = ec - J * C.nx;
-        const int e00 = (2 * J) * L.nx + 2 * I, e01 = e00 + 1;
-        const int e10 = e00 + L.nx, e11 = e10 + 1;
-        const double r00 = (__ldcg(L.b + e00) - apply_at(L, coef, L.x, cell_of(L, e00))) * L.mask[e00];
-        const double r01 = (__ldcg(L.b + e01) - apply_at(L, coef, L.x, cell_of(L, e01))) * L.mask[e01];
-        const double r10 = (__ldcg(L.b + e10) - apply_at(L, coef, L.x, cell_of(L, e10))) * L.mask[e10];
-        const double r11 = (__ldcg(L.b + e11) - apply_at(L, coef, L.x, cell_of(L, e11))) * L.mask[e11];
-        C.b[ec] = 0.25 * (r00 + r01 + r10 + r11);
-        C.x[ec] = 0.0;
     }
 }
 
@@ -238,75 +208,346 @@ __device__ double tree_fold(const HelmParams& H, const double* leaf, double* sm)
     return r;
 }
 
-// ------------------------------------------------------------------ multigrid V-cycle
-// smoothing sweeps of one level: forward = red then black, reverse = black then red
-__device__ void smooth(const HLevel& L, int sweeps, bool reverse, bool grid, const HelmParams& H,
-                       bool& ok) {
-    for (int s = 0; s < sweeps && ok; ++s) {
-        for (int h = 0; h < 2 && ok; ++h) {
-            const int colour = reverse ? 1 - h : h;
-            colour_phase(L, L.x, L.b, colour, grid ? grid_team() : block_team());
-            if (grid)
-                ok = grid_sync(H);
-            else
-                __syncthreads();
+// ------------------------------------------------------------------ tiled multigrid
+// A fine level is processed tile by tile in shared memory. The down phase loads
+// x, b and the coefficients of a tile plus a HALO-wide ring, runs the two
+// pre-smoothing sweeps (four red-black half-sweeps) on a region that shrinks by
+// one cell per half-sweep, and forms the restricted residual of the interior;
+// the up phase adds the prolonged coarse correction and runs the two reverse
+// post-smoothing sweeps the same way. Every value in the valid region is the
+// one the whole-grid sweep produces (same inputs, same operations), so the
+// result is identical to sweeping the level with a grid barrier between
+// half-sweeps, with two barriers per level instead of nine.
+__device__ __forceinline__ int wrap_any(int i, int n) {
+    if (i >= 0 && i < n) return i;
+    if (i < 0 && i + n >= 0) return i + n;
+    if (i >= n && i - n < n) return i - n;
+    const int r = i % n;
+    return r < 0 ? r + n : r;
+}
+
+struct TileRefs {
+    double *x, *b, *ku, *kv, *id, *m;
+};
+
+__device__ __forceinline__ TileRefs tile_refs(double* base) {
+    TileRefs t;
+    t.x = base;
+    t.b = base + RN;
+    t.ku = base + 2 * RN;
+    t.kv = base + 3 * RN;
+    t.id = base + 4 * RN;
+    t.m = base + 5 * RN;
+    return t;
+}
+
+// load a tile region of level L whose interior starts at (i0, j0); x from xin
+// (or zero), plus the coarse correction e * mask when C is given
+__device__ void tile_load(const HLevel& L, int i0, int j0, const double* xin, const HLevel* C,
+                          TileRefs t) {
+    for (int r = threadIdx.x; r < RN; r += blockDim.x) {
+        const int rj = r / RW, ri = r - rj * RW;
+        const int gi = wrap_any(i0 - HALO + ri, L.nx), gj = wrap_any(j0 - HALO + rj, L.ny);
+        const int g = gj * L.nx + gi;
+        const double m = L.mask[g];
+        double x = xin ? __ldcg(xin + g) : 0.0;
+        if (C) x = x + __ldcg(C->x + (gj >> 1) * C->nx + (gi >> 1)) * m;
+        t.x[r] = x;
+        t.b[r] = __ldcg(L.b + g);
+        t.ku[r] = L.Ku[g];
+        t.kv[r] = L.Kv[g];
+        t.id[r] = L.inv_diag[g];
+        t.m[r] = m;
+    }
+    __syncthreads();
+}
+
+// one red-black half-sweep of colour `colour` on the region ring >= SHRINK. On
+// even-sized levels the colour of a region cell follows from its region
+// coordinates (a wrap by an even size keeps the parity), so only the cells of
+// that colour are visited; odd-sized levels test each cell.
+template <int SHRINK>
+__device__ void tile_half_sweep_t(const HLevel& L, int i0, int j0, TileRefs t, int colour) {
+    constexpr int ROWS = RW - 2 * SHRINK;
+    constexpr int HALF = (ROWS + 1) / 2;
+    const bool even = ((L.nx | L.ny) & 1) == 0;
+    if (even) {
+        for (int q = threadIdx.x; q < ROWS * HALF; q += blockDim.x) {
+            const int rj = SHRINK + q / HALF;
+            const int ri = SHRINK + ((colour - i0 - j0 - rj - SHRINK) & 1) + 2 * (q % HALF);
+            if (ri >= RW - SHRINK) continue;
+            const int r = rj * RW + ri;
+            const double nb = L.cx * (t.ku[r] * t.x[r + 1] + t.ku[r - 1] * t.x[r - 1]) +
+                              L.cy * (t.kv[r] * t.x[r + RW] + t.kv[r - RW] * t.x[r - RW]);
+            t.x[r] = t.id[r] * (t.b[r] + nb) * t.m[r];
         }
+    } else {
+        for (int r = threadIdx.x; r < RN; r += blockDim.x) {
+            const int rj = r / RW, ri = r - rj * RW;
+            if (ri < SHRINK || ri >= RW - SHRINK || rj < SHRINK || rj >= RW - SHRINK) continue;
+            const int gi = wrap_any(i0 - HALO + ri, L.nx), gj = wrap_any(j0 - HALO + rj, L.ny);
+            if (((gi + gj) & 1) != colour) continue;
+            const double nb = L.cx * (t.ku[r] * t.x[r + 1] + t.ku[r - 1] * t.x[r - 1]) +
+                              L.cy * (t.kv[r] * t.x[r + RW] + t.kv[r - RW] * t.x[r - RW]);
+            t.x[r] = t.id[r] * (t.b[r] + nb) * t.m[r];
+        }
+    }
+    __syncthreads();
+}
+
+// four half-sweeps with colours c0, 1 - c0, c0, 1 - c0 on a region shrinking by one ring each
+__device__ __forceinline__ void tile_four_half_sweeps(const HLevel& L, int i0, int j0, TileRefs t, int c0) {
+    tile_half_sweep_t<1>(L, i0, j0, t, c0);
+    tile_half_sweep_t<2>(L, i0, j0, t, 1 - c0);
+    tile_half_sweep_t<3>(L, i0, j0, t, c0);
+    tile_half_sweep_t<4>(L, i0, j0, t, 1 - c0);
+}
+
+// (b - A x) * mask at region cell r (VarOperator.apply, solvers_var.py:47-53)
+__device__ __forceinline__ double tile_residual(const HLevel& L, double coef, TileRefs t, int r) {
+    const double m = t.m[r];
+    const double xm = t.x[r] * m;
+    const double xe = t.x[r + 1] * t.m[r + 1];
+    const double xw = t.x[r - 1] * t.m[r - 1];
+    const double xn = t.x[r + RW] * t.m[r + RW];
+    const double xs = t.x[r - RW] * t.m[r - RW];
+    const double fx = t.ku[r] * (xe - xm);
+    const double fxw = t.ku[r - 1] * (xm - xw);
+    const double fy = t.kv[r] * (xn - xm);
+    const double fys = t.kv[r - RW] * (xm - xs);
+    const double lap = (fx - fxw) / L.dx2 + (fy - fys) / L.dy2;
+    const double ax = (xm - coef * lap) * m + xm * (1.0 - m);
+    return (t.b[r] - ax) * m;
+}
+
+__device__ void tile_store_x(const HLevel& L, int i0, int j0, TileRefs t, double* xout) {
+    for (int r = threadIdx.x; r < TILE * TILE; r += blockDim.x) {
+        const int cj = r / TILE, ci = r - cj * TILE;
+        const int gi = i0 + ci, gj = j0 + cj;
+        if (gi >= L.nx || gj >= L.ny) continue;
+        xout[gj * L.nx + gi] = t.x[(cj + HALO) * RW + ci + HALO];
     }
 }
 
-// post-smoothing of level l after the coarse correction: the first (black)
-// half-sweep reads the prolonged neighbours (solvers_var.py:148-150)
-__device__ void post_smooth(const HelmParams& H, int l, bool grid, bool& ok) {
+// down phase of level l: pre-smoothing, restricted residual into level l+1
+// (solvers_var.py:141-147); x of level l+1 starts at zero implicitly
+__device__ void mg_down(const HelmParams& H, int l, const double* xin, double* xout, double* smem) {
     const HLevel& L = H.lv[l];
     const HLevel& C = H.lv[l + 1];
-    colour_phase_prolonged(L, C, L.x, L.b, 1, grid ? grid_team() : block_team());
-    if (grid)
-        ok = grid_sync(H);
-    else
+    const int tx = (L.nx + TILE - 1) / TILE, ty = (L.ny + TILE - 1) / TILE;
+    TileRefs t = tile_refs(smem);
+    for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
+        const int i0 = (tile % tx) * TILE, j0 = (tile / tx) * TILE;
+        tile_load(L, i0, j0, xin, nullptr, t);
+        tile_four_half_sweeps(L, i0, j0, t, 0);
+        for (int r = threadIdx.x; r < (TILE / 2) * (TILE / 2); r += blockDim.x) {
+            const int cj = r / (TILE / 2), ci = r - cj * (TILE / 2);
+            const int I = i0 / 2 + ci, J = j0 / 2 + cj;
+            if (I >= C.nx || J >= C.ny) continue;
+            const int r00 = (HALO + 2 * cj) * RW + HALO + 2 * ci;
+            const double a = tile_residual(L, H.coef, t, r00);
+            const double b = tile_residual(L, H.coef, t, r00 + 1);
+            const double c = tile_residual(L, H.coef, t, r00 + RW);
+            const double d = tile_residual(L, H.coef, t, r00 + RW + 1);
+            C.b[J * C.nx + I] = 0.25 * (a + b + c + d);
+        }
+        tile_store_x(L, i0, j0, t, xout);
         __syncthreads();
-    if (!ok) return;
-    colour_phase(L, L.x, L.b, 0, grid ? grid_team() : block_team());
-    if (grid)
-        ok = grid_sync(H);
-    else
-        __syncthreads();
-    if (!ok) return;
-    smooth(L, 1, true, grid, H, ok);
+    }
 }
 
-__device__ void vcycle(const HelmParams& H, bool& ok) {
-    const int nl = H.n_levels;
-    const int cf = H.coarse_from;  // levels >= cf run in CTA 0
-    // descend over the grid-wide levels
-    for (int l = 0; l < nl - 1 && l < cf && ok; ++l) {
-        smooth(H.lv[l], 2, false, true, H, ok);
-        if (!ok) return;
-        restrict_phase(H.lv[l], H.lv[l + 1], H.coef, grid_team());
-        ok = grid_sync(H);
+// up phase of level l: x + prolong(x_coarse) * mask, then the two reverse sweeps
+// (solvers_var.py:148-150)
+__device__ void mg_up(const HelmParams& H, int l, const double* xin, const HLevel& C, double* xout,
+                      double* smem) {
+    const HLevel& L = H.lv[l];
+    const int tx = (L.nx + TILE - 1) / TILE, ty = (L.ny + TILE - 1) / TILE;
+    TileRefs t = tile_refs(smem);
+    for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
+        const int i0 = (tile % tx) * TILE, j0 = (tile / tx) * TILE;
+        tile_load(L, i0, j0, xin, &C, t);
+        tile_four_half_sweeps(L, i0, j0, t, 1);
+        tile_store_x(L, i0, j0, t, xout);
+        __syncthreads();
     }
-    if (!ok) return;
-    if (cf < nl) {
-        if (blockIdx.x == 0) {
-            bool bok = true;
-            for (int l = cf; l < nl - 1; ++l) {
-                smooth(H.lv[l], 2, false, false, H, bok);
-                restrict_phase(H.lv[l], H.lv[l + 1], H.coef, block_team());
-                __syncthreads();
-            }
-            smooth(H.lv[nl - 1], 2, false, false, H, bok);
-            smooth(H.lv[nl - 1], 2, true, false, H, bok);
-            for (int l = nl - 2; l >= cf; --l) post_smooth(H, l, false, bok);
+}
+
+// ---- coarse levels: all of them inside CTA 0, in shared memory
+struct CoarseRefs {
+    double *x, *b, *ku, *kv, *id, *m;
+};
+
+__device__ __forceinline__ CoarseRefs coarse_refs(const HelmParams& H, double* base, int l) {
+    int off = 0, tot = 0;
+    for (int q = H.coarse_from; q < H.n_levels; ++q) {
+        if (q < l) off += H.lv[q].n;
+        tot += H.lv[q].n;
+    }
+    CoarseRefs c;
+    c.x = base + off;
+    c.b = base + tot + off;
+    c.ku = base + 2 * tot + off;
+    c.kv = base + 3 * tot + off;
+    c.id = base + 4 * tot + off;
+    c.m = base + 5 * tot + off;
+    return c;
+}
+
+__device__ void coarse_half_sweep(const HLevel& L, CoarseRefs s, int colour, const CoarseRefs* C,
+                                  const HLevel* LC) {
+    for (int e = threadIdx.x; e < L.n; e += blockDim.x) {
+        const int j = e / L.nx, i = e - j * L.nx;
+        if (((i + j) & 1) != colour) continue;
+        const int ie = j * L.nx + (i + 1 == L.nx ? 0 : i + 1), iw = j * L.nx + (i == 0 ? L.nx - 1 : i - 1);
+        const int jn = (j + 1 == L.ny ? 0 : j + 1) * L.nx + i, js = (j == 0 ? L.ny - 1 : j - 1) * L.nx + i;
+        double xe = s.x[ie], xw = s.x[iw], xn = s.x[jn], xs = s.x[js];
+        if (C) {  // neighbours after the coarse correction x + prolong(e) * mask
+            auto corr = [&](int q) {
+                const int qj = q / L.nx, qi = q - qj * L.nx;
+                return C->x[(qj >> 1) * LC->nx + (qi >> 1)] * s.m[q];
+            };
+            xe = xe + corr(ie);
+            xw = xw + corr(iw);
+            xn = xn + corr(jn);
+            xs = xs + corr(js);
         }
-        ok = grid_sync(H);
-        if (!ok) return;
-    } else {
-        // coarsest level on the whole grid
-        smooth(H.lv[nl - 1], 2, false, true, H, ok);
-        if (!ok) return;
-        smooth(H.lv[nl - 1], 2, true, true, H, ok);
-        if (!ok) return;
+        const double nb = L.cx * (s.ku[e] * xe + s.ku[iw] * xw) + L.cy * (s.kv[e] * xn + s.kv[js] * xs);
+        s.x[e] = s.id[e] * (s.b[e] + nb) * s.m[e];
     }
-    for (int l = (cf < nl - 1 ? cf : nl - 1) - 1; l >= 0 && ok; --l) post_smooth(H, l, true, ok);
+    __syncthreads();
+}
+
+__device__ double coarse_residual(const HLevel& L, double coef, CoarseRefs s, int e) {
+    const int j = e / L.nx, i = e - j * L.nx;
+    const int ie = j * L.nx + (i + 1 == L.nx ? 0 : i + 1), iw = j * L.nx + (i == 0 ? L.nx - 1 : i - 1);
+    const int jn = (j + 1 == L.ny ? 0 : j + 1) * L.nx + i, js = (j == 0 ? L.ny - 1 : j - 1) * L.nx + i;
+    const double m = s.m[e];
+    const double xm = s.x[e] * m, xe = s.x[ie] * s.m[ie], xw = s.x[iw] * s.m[iw];
+    const double xn = s.x[jn] * s.m[jn], xs = s.x[js] * s.m[js];
+    const double fx = s.ku[e] * (xe - xm), fxw = s.ku[iw] * (xm - xw);
+    const double fy = s.kv[e] * (xn - xm), fys = s.kv[js] * (xm - xs);
+    const double lap = (fx - fxw) / L.dx2 + (fy - fys) / L.dy2;
+    const double ax = (xm - coef * lap) * m + xm * (1.0 - m);
+    return (s.b[e] - ax) * m;
+}
+
+// the V-cycle below and including level cf, by CTA 0 alone; reads level cf's b
+// (and x when cf is the finest level) from global memory, writes level cf's x
+__device__ void mg_coarse(const HelmParams& H, double* smem, const double* xin_cf, double* xout_cf) {
+    const int cf = H.coarse_from, nl = H.n_levels;
+    for (int l = cf; l < nl; ++l) {
+        const HLevel& L = H.lv[l];
+        CoarseRefs s = coarse_refs(H, smem, l);
+        for (int e = threadIdx.x; e < L.n; e += blockDim.x) {
+            s.ku[e] = L.Ku[e];
+            s.kv[e] = L.Kv[e];
+            s.id[e] = L.inv_diag[e];
+            s.m[e] = L.mask[e];
+            if (l == cf) {
+                s.b[e] = __ldcg(L.b + e);
+                s.x[e] = xin_cf ? __ldcg(xin_cf + e) : 0.0;
+            }
+        }
+    }
+    __syncthreads();
+    for (int l = cf; l < nl; ++l) {
+        const HLevel& L = H.lv[l];
+        CoarseRefs s = coarse_refs(H, smem, l);
+        for (int h = 0; h < 4; ++h) coarse_half_sweep(L, s, h & 1, nullptr, nullptr);
+        if (l + 1 < nl) {
+            const HLevel& C = H.lv[l + 1];
+            CoarseRefs c = coarse_refs(H, smem, l + 1);
+            for (int e = threadIdx.x; e < C.n; e += blockDim.x) {
+                const int J = e / C.nx, I = e - J * C.nx;
+                const int f00 = (2 * J) * L.nx + 2 * I;
+                const double a = coarse_residual(L, H.coef, s, f00);
+                const double b = coarse_residual(L, H.coef, s, f00 + 1);
+                const double cc = coarse_residual(L, H.coef, s, f00 + L.nx);
+                const double d = coarse_residual(L, H.coef, s, f00 + L.nx + 1);
+                c.b[e] = 0.25 * (a + b + cc + d);
+                c.x[e] = 0.0;
+            }
+            __syncthreads();
+        }
+    }
+    {  // the coarsest level: its reverse sweeps follow the forward ones directly
+        const HLevel& L = H.lv[nl - 1];
+        CoarseRefs s = coarse_refs(H, smem, nl - 1);
+        for (int h = 0; h < 4; ++h) coarse_half_sweep(L, s, 1 - (h & 1), nullptr, nullptr);
+    }
+    for (int l = nl - 2; l >= cf; --l) {
+        const HLevel& L = H.lv[l];
+        CoarseRefs s = coarse_refs(H, smem, l);
+        CoarseRefs c = coarse_refs(H, smem, l + 1);
+        coarse_half_sweep(L, s, 1, &c, &H.lv[l + 1]);
+        coarse_half_sweep(L, s, 0, nullptr, nullptr);
+        coarse_half_sweep(L, s, 1, nullptr, nullptr);
+        coarse_half_sweep(L, s, 0, nullptr, nullptr);
+    }
+    const HLevel& L = H.lv[cf];
+    CoarseRefs s = coarse_refs(H, smem, cf);
+    for (int e = threadIdx.x; e < L.n; e += blockDim.x) xout_cf[e] = s.x[e];
+    __syncthreads();
+}
+
+// smoothing only (the coarsest level when it is too large for CTA 0): two
+// forward or two reverse sweeps
+__device__ void mg_smooth(const HelmParams& H, int l, const double* xin, double* xout, bool reverse,
+                          double* smem) {
+    const HLevel& L = H.lv[l];
+    const int tx = (L.nx + TILE - 1) / TILE, ty = (L.ny + TILE - 1) / TILE;
+    TileRefs t = tile_refs(smem);
+    for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
+        const int i0 = (tile % tx) * TILE, j0 = (tile / tx) * TILE;
+        tile_load(L, i0, j0, xin, nullptr, t);
+        tile_four_half_sweeps(L, i0, j0, t, reverse ? 1 : 0);
+        tile_store_x(L, i0, j0, t, xout);
+        __syncthreads();
+    }
+}
+
+// one V(2,2) cycle on x0 (level 0's current x); returns the buffer holding the
+// new x (x0 or level 0's second buffer). Levels below coarse_from have a grid
+// down and up phase; the rest run in CTA 0, or, when every level is too large
+// for it, the coarsest level is smoothed on the grid.
+__device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, bool& ok) {
+    const int cf = H.coarse_from, nl = H.n_levels;
+    double* x0b = (x0 == H.lv[0].x) ? H.lv[0].x2 : H.lv[0].x;
+    if (cf == 0) {
+        if (blockIdx.x == 0) mg_coarse(H, smem, x0, x0b);
+        ok = grid_sync(H);
+        return x0b;
+    }
+    const int ndown = cf < nl ? cf : nl - 1;
+    for (int l = 0; l < ndown && ok; ++l) {
+        mg_down(H, l, l == 0 ? x0 : nullptr, l == 0 ? x0b : H.lv[l].x, smem);
+        ok = grid_sync(H);
+    }
+    if (!ok) return x0;
+    if (cf < nl) {
+        if (blockIdx.x == 0) mg_coarse(H, smem, nullptr, H.lv[cf].x2);
+        ok = grid_sync(H);
+    } else {
+        const int l = nl - 1;
+        double* xa = (l == 0) ? x0b : H.lv[l].x;
+        double* xb = (l == 0) ? x0 : H.lv[l].x2;
+        mg_smooth(H, l, l == 0 ? x0 : nullptr, xa, false, smem);
+        ok = grid_sync(H);
+        if (!ok) return x0;
+        mg_smooth(H, l, xa, xb, true, smem);
+        ok = grid_sync(H);
+        if (l == 0) return x0;
+    }
+    // ascend: level l reads its down-phase result and level l+1's final x (in x2)
+    for (int l = ndown - 1; l >= 0 && ok; --l) {
+        const double* xin = (l == 0) ? x0b : H.lv[l].x;
+        double* xout = (l == 0) ? x0 : H.lv[l].x2;
+        HLevel C = H.lv[l + 1];
+        C.x = H.lv[l + 1].x2;
+        mg_up(H, l, xin, C, xout, smem);
+        ok = grid_sync(H);
+    }
+    return x0;
 }
 
 // ------------------------------------------------------------------ the solve kernel
@@ -337,9 +578,10 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
         if (H.kind == HK_RBGS || H.kind == HK_MULTIGRID) {
             // stationary iteration with the true residual (solvers_var.py:170-179)
             conv = 0;
+            double* xc = x;  // the level-0 buffer holding the current iterate
             for (int it = 1; it <= H.max_iter && ok; ++it) {
                 if (H.kind == HK_MULTIGRID) {
-                    vcycle(H, ok);
+                    xc = vcycle_tiled(H, xc, sm + H.n_leaves, ok);
                 } else {
                     colour_phase(L0, x, b0, 0, grid_team());
                     ok = grid_sync(H);
@@ -348,9 +590,10 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                     ok = grid_sync(H);
                 }
                 if (!ok) break;
+                const double* xr = xc;
                 leaf_phase(H,
                            [&](int e) {
-                               const double d = __ldcg(b0 + e) - apply_at(L0, H.coef, x, cell_of(L0, e));
+                               const double d = __ldcg(b0 + e) - apply_at(L0, H.coef, xr, cell_of(L0, e));
                                return make_double2(d * d, 0.0);
                            },
                            H.leafA, nullptr);
@@ -362,6 +605,9 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                     conv = 1;
                     break;
                 }
+            }
+            if (ok && xc != x) {
+                for (int e = grid_team().first; e < L0.n; e += grid_team().stride) x[e] = __ldcg(xc + e);
             }
         } else {
             // preconditioned CG (solvers_var.py:181-197)
@@ -587,6 +833,7 @@ int HelmSolver::init(int nx, int ny, double lx, double ly, double coef, int kind
         L.mask = m;
         L.inv_diag = (double*)dalloc(sizeof(double) * L.n);
         L.b = (double*)dalloc(sizeof(double) * L.n);
+        L.x2 = (double*)dalloc(sizeof(double) * L.n);
         if (l == 0) {
             L.Ku = Ku;
             L.Kv = Kv;
@@ -596,11 +843,11 @@ int HelmSolver::init(int nx, int ny, double lx, double ly, double coef, int kind
             L.Kv = (double*)dalloc(sizeof(double) * L.n);
             L.x = (double*)dalloc(sizeof(double) * L.n);
         }
-        if (!L.inv_diag || !L.b || (l > 0 && (!L.Ku || !L.Kv || !L.x))) {
+        if (!L.inv_diag || !L.b || !L.x2 || (l > 0 && (!L.Ku || !L.Kv || !L.x))) {
             err = "cudaMalloc failed (Helmholtz levels)";
             return OC_ERR_CUDA;
         }
-        if (l > 0 && L.n <= kCoarseCells && H.coarse_from == H.n_levels) H.coarse_from = l;
+        if (L.n <= kCoarseCells && H.coarse_from == H.n_levels) H.coarse_from = l;
     }
     const size_t n = (size_t)nx * ny;
     H.r = (double*)dalloc(sizeof(double) * n);
@@ -652,7 +899,10 @@ int HelmSolver::init(int nx, int ny, double lx, double ly, double coef, int kind
         err = "device does not support cooperative launches";
         return OC_ERR_UNSUPPORTED;
     }
-    smem_ = sizeof(double) * (size_t)H.n_leaves;
+    size_t coarse_cells = 0;
+    for (int l = H.coarse_from; l < H.n_levels; ++l) coarse_cells += (size_t)H.lv[l].n;
+    const size_t mg_work = (kind == HK_MULTIGRID) ? std::max<size_t>(6 * RN, 6 * coarse_cells) : 0;
+    smem_ = sizeof(double) * ((size_t)H.n_leaves + mg_work);
     if (smem_ > 200 * 1024) {
         err = "Helmholtz grid too large for the single-pass reduction tree";
         return OC_ERR_UNSUPPORTED;

@@ -17,7 +17,8 @@ struct HLevel {
     double* Ku;
     double* Kv;
     double* inv_diag;
-    double* x;
+    double* x;   // current solution of the level (level 0: the caller's output)
+    double* x2;  // second buffer: the smoothing phases read one and write the other
     double* b;
 };
 

@@ -61,24 +61,89 @@ struct KP {
     const double* tau_u;   // surface stress / rho0 at u faces, masked
     const double* tau_v;
     const double* ustar2;  // closure surface u*^2
+    const int2* kinfo;     // per column: (levels of exact thickness dzr, wet levels)
+    const double2* dzx;    // per column: thickness of wet levels kfull and kfull + 1
+    const int2* kface;     // per column: wet levels of its east (x) and north (y) face
     int face_rule;         // 0 min, 1 mean, 2 harmonic
 };
 
 __device__ __forceinline__ int wrapi(int i, int n) {
-    i %= n;
-    return i < 0 ? i + n : i;
+    if (i < 0) i += n;
+    if (i >= n) i -= n;
+    if (i < 0 || i >= n) {  // only for grids narrower than the offset
+        i %= n;
+        if (i < 0) i += n;
+    }
+    return i;
 }
 
 __device__ __forceinline__ double inv_pos(double a) { return a > 0.0 ? 1.0 / a : 0.0; }
 
-// z-level partial-cell thickness of level k in a column of depth Hc and mask
-// mc; writes the wet mask (reference domain.py:113-129, dz3_ref = dz3 * m3).
-__device__ __forceinline__ double cell_dz(const KP& P, double Hc, double mc, int k, double& m3) {
-    double rem = Hc - P.edge[k];
-    double dz = fmin(fmax(rem, 0.0), P.dzr[k]);
-    if (dz > 0.0 && dz < P.thin[k]) dz = 0.0;
-    m3 = (dz > 0.0 ? 1.0 : 0.0) * mc;
-    return dz * m3;
+// z-level partial-cell thickness of level k of column c and its wet mask
+// (reference domain.py:113-129: dz3_ref = clip(H - edge, 0, dzr) with thin
+// cells removed, times the wet mask). The host stores each column in compact
+// form -- kinfo = (kfull, kb): levels below kfull are full (thickness dzr[k]
+// exactly), levels kfull..kb-1 are wet with the explicit thicknesses dzx, levels
+// from kb on are dry -- after checking that it reproduces the formula bit for
+// bit, so no 3D geometry array is ever read.
+__device__ __forceinline__ double col_dz(const KP& P, int c, int k, double& m3) {
+    const int2 ki = P.kinfo[c];
+    if (k >= ki.y) {
+        m3 = 0.0;
+        return 0.0;
+    }
+    m3 = 1.0;
+    if (k < ki.x) return P.dzr[k];
+    const double2 dx = P.dzx[c];
+    return k == ki.x ? dx.x : dx.y;
+}
+
+// the compact geometry of one column held in registers; dz() equals col_dz()
+struct ColGeo {
+    int kf, kb;
+    double d0, d1;
+    __device__ __forceinline__ static ColGeo load(const KP& P, int c) {
+        const int2 ki = P.kinfo[c];
+        const double2 dx = P.dzx[c];
+        return ColGeo{ki.x, ki.y, dx.x, dx.y};
+    }
+    __device__ __forceinline__ double dz(const KP& P, int k, double& m3) const {
+        if (k >= kb) {
+            m3 = 0.0;
+            return 0.0;
+        }
+        m3 = 1.0;
+        if (k < kf) return P.dzr[k];
+        return k == kf ? d0 : d1;
+    }
+};
+
+__device__ __forceinline__ double col_m3(const KP& P, int c, int k) { return k < P.kinfo[c].y ? 1.0 : 0.0; }
+
+// 3D face masks m3 * m3(neighbour) * mask_face (domain.py:93-96): the wet levels
+// of a face are the top min(kb, kb of the neighbour) levels when the 2D face
+// is open, so one integer per face and column (checked on the host) gives them
+__device__ __forceinline__ double col_m3u(const KP& P, int c, int k) { return k < P.kface[c].x ? 1.0 : 0.0; }
+__device__ __forceinline__ double col_m3v(const KP& P, int c, int k) { return k < P.kface[c].y ? 1.0 : 0.0; }
+
+// depth of the top of level k (the sequential sum of dz3 above it) and of the
+// level centre (reference domain.py:148-154)
+__device__ __forceinline__ double col_above(const KP& P, int c, int k) {
+    const int2 ki = P.kinfo[c];
+    const int m = k < ki.x ? k : ki.x;
+    double above = P.edge[m];
+    if (k > ki.x && ki.x < ki.y) {
+        const double2 dx = P.dzx[c];
+        above = (m == 0) ? dx.x : above + dx.x;
+        if (k > ki.x + 1 && ki.x + 1 < ki.y) above = above + dx.y;
+    }
+    return above;
+}
+
+__device__ __forceinline__ double col_zc(const KP& P, int c, int k) {
+    double m3;
+    const double dz = col_dz(P, c, k, m3);
+    return col_above(P, c, k) + 0.5 * dz;
 }
 
 __device__ __forceinline__ double face_combine(const KP& P, double a, double b) {
@@ -95,7 +160,7 @@ struct CellGeo {
 
 __device__ __forceinline__ CellGeo cell_geo(const KP& P, int c2, int k) {
     CellGeo g;
-    g.dz = cell_dz(P, P.H[c2], P.mask[c2], k, g.m3);
+    g.dz = col_dz(P, c2, k, g.m3);
     return g;
 }
 
@@ -114,47 +179,50 @@ __device__ __forceinline__ double superbee(double r) {
 
 // Upwind-biased value on the face between c0 and c1 (c_m = left of c0,
 // c_p = right of c1), advecting velocity vel, far-cell wet flags wm (left of
-// c0) and wp (right of c1). Reference advection_v06.py:21-47.
+// c0) and wp (right of c1). Reference advection_v06.py:21-47. The reference
+// forms both one-sided values and selects by the sign of vel. Here the inputs
+// are selected first and one value is formed: for vel <= 0 the reference's
+// c1 - t equals c1 + (-t) exactly, so the bits are the same, with one division
+// instead of two and no divergent branch.
 __device__ __forceinline__ double kappa_face(const KP& P, double cm, double c0, double c1, double cp,
                                              double vel, double wm, double wp, bool limited) {
-    double fp, fn;
+    const bool pos = vel > 0.0;
+    const double base = pos ? c0 : c1;
+    const double far = pos ? (c0 - cm) : (cp - c1);
+    const double d = c1 - c0;
+    double t;
     if (limited) {
-        double d = c1 - c0;
-        double eps = d == 0.0 ? 1.0 : d;
-        double rp = d == 0.0 ? 0.0 : (c0 - cm) / eps;
-        double rn = d == 0.0 ? 0.0 : (cp - c1) / eps;
-        fp = c0 + 0.5 * superbee(rp) * d;
-        fn = c1 - 0.5 * superbee(rn) * d;
+        const double eps = d == 0.0 ? 1.0 : d;
+        const double r = d == 0.0 ? 0.0 : far / eps;
+        t = 0.5 * superbee(r) * d;
     } else {
-        fp = c0 + 0.25 * (P.one_m_kappa3 * (c0 - cm) + P.one_p_kappa3 * (c1 - c0));
-        fn = c1 - 0.25 * (P.one_m_kappa3 * (cp - c1) + P.one_p_kappa3 * (c1 - c0));
+        t = 0.25 * (P.one_m_kappa3 * far + P.one_p_kappa3 * d);
     }
-    if (!(wm > 0.0)) fp = c0;
-    if (!(wp > 0.0)) fn = c1;
-    return vel > 0.0 ? fp : fn;
+    const double f = base + (pos ? t : -t);
+    return ((pos ? wm : wp) > 0.0) ? f : base;
 }
 
 // Interior vertical face value at an interface with `above` (layer k-1),
 // `below` (layer k), far_up (k-2, 0 when absent), far_dn (k+1, 0 when absent)
-// and wet flags of the far cells; w positive upward. advection_v06.py:50-74.
+// and wet flags of the far cells; w positive upward. advection_v06.py:50-74,
+// selected before forming as in kappa_face.
 __device__ __forceinline__ double kappa_face_z(const KP& P, double far_up, double above, double below,
                                                double far_dn, double w, bool has_up, bool has_dn,
                                                bool limited) {
-    double d = above - below;
-    double fu, fd;
+    const bool up = w > 0.0;
+    const double base = up ? below : above;
+    const double far = up ? (below - far_dn) : (far_up - above);
+    const double d = above - below;
+    double t;
     if (limited) {
-        double eps = d == 0.0 ? 1.0 : d;
-        double ru = d == 0.0 ? 0.0 : (below - far_dn) / eps;
-        double rd = d == 0.0 ? 0.0 : (far_up - above) / eps;
-        fu = below + 0.5 * superbee(ru) * d;
-        fd = above - 0.5 * superbee(rd) * d;
+        const double eps = d == 0.0 ? 1.0 : d;
+        const double r = d == 0.0 ? 0.0 : far / eps;
+        t = 0.5 * superbee(r) * d;
     } else {
-        fu = below + 0.25 * (P.one_m_kappa3 * (below - far_dn) + P.one_p_kappa3 * (above - below));
-        fd = above - 0.25 * (P.one_m_kappa3 * (far_up - above) + P.one_p_kappa3 * (above - below));
+        t = 0.25 * (P.one_m_kappa3 * far + P.one_p_kappa3 * d);
     }
-    if (!has_dn) fu = below;
-    if (!has_up) fd = above;
-    return w > 0.0 ? fu : fd;
+    const double f = base + (up ? t : -t);
+    return (up ? has_dn : has_up) ? f : base;
 }
 
 // ---------------------------------------------------------------- EOS

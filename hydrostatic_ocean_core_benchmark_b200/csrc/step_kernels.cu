@@ -53,12 +53,25 @@ __device__ __forceinline__ void implicit_row(const KP& P, int k, double dzk, dou
     }
 }
 
+// neighbour offsets of one column, wrapped once (periodic index layout, up to
+// three cells away)
 struct Nbr {
     int i, j, c;
     int nx, ny;
-    __device__ __forceinline__ int at(int dj, int di) const {
-        return wrapi(j + dj, ny) * nx + wrapi(i + di, nx);
+    int ix[7], jy[7];  // i-3..i+3 and (j-3..j+3) * nx, wrapped
+    __device__ __forceinline__ void init(int i_, int j_, int nx_, int ny_) {
+        i = i_;
+        j = j_;
+        nx = nx_;
+        ny = ny_;
+        c = j * nx + i;
+#pragma unroll
+        for (int d = -3; d <= 3; ++d) {
+            ix[d + 3] = wrapi(i + d, nx);
+            jy[d + 3] = wrapi(j + d, ny) * nx;
+        }
     }
+    __device__ __forceinline__ int at(int dj, int di) const { return jy[dj + 3] + ix[di + 3]; }
 };
 
 __device__ __forceinline__ CellGeo geo_off(const KP& P, const Nbr& n, int dj, int di, int k) {
@@ -80,15 +93,11 @@ __device__ __forceinline__ void vfacek(const KP& P, const Nbr& n, int dj, int di
 }
 
 __device__ __forceinline__ double m3u_at(const KP& P, const Nbr& n, int dj, int di, int k) {
-    double m, d;
-    ufacek(P, n, dj, di, k, m, d);
-    return m;
+    return col_m3u(P, n.at(dj, di), k);
 }
 
 __device__ __forceinline__ double m3v_at(const KP& P, const Nbr& n, int dj, int di, int k) {
-    double m, d;
-    vfacek(P, n, dj, di, k, m, d);
-    return m;
+    return col_m3v(P, n.at(dj, di), k);
 }
 
 __device__ __forceinline__ double m3_at(const KP& P, const Nbr& n, int dj, int di, int k) {
@@ -100,74 +109,83 @@ __device__ __forceinline__ double m3_at(const KP& P, const Nbr& n, int dj, int d
     const int j = blockIdx.y * blockDim.y + threadIdx.y; \
     if (i >= P.nx || j >= P.ny) return;                  \
     Nbr nb;                                              \
-    nb.i = i;                                            \
-    nb.j = j;                                            \
-    nb.nx = P.nx;                                        \
-    nb.ny = P.ny;                                        \
-    nb.c = j * P.nx + i;                                 \
+    nb.init(i, j, P.nx, P.ny);                           \
     const size_t n2 = (size_t)P.n2;                      \
     (void)n2;
 
 // ------------------------------------------------------------------ q = A^-1 1 on a column
-// Momentum tridiagonal with a unit right-hand side for the column's interface
-// viscosity km[0..nz] (reference model3d_v05.py:147-153).
-__device__ __forceinline__ void column_q(const KP& P, int nz, const double* dz, const double* m3,
-                                         const double* dzi, const double* kmc, double* cs, double* ds,
-                                         double* __restrict__ q_out, size_t c, size_t n2) {
-    for (int k = 0; k < nz; ++k) {
-        double sub, diag, sup;
-        const double m3k1 = (k + 1 < nz) ? m3[k + 1] : 0.0;
-        implicit_row(P, k, dz[k], m3[k], m3k1, dzi[k], dzi[k + 1], kmc[k], kmc[k + 1], P.thv_dt_drag,
-                     sub, diag, sup);
-        if (k == 0) {
-            cs[0] = sup / diag;
-            ds[0] = 1.0 / diag;
-        } else {
-            const double den = diag - sub * cs[k - 1];
-            cs[k] = sup / den;
-            ds[k] = (1.0 - sub * ds[k - 1]) / den;
-        }
-    }
-    double x = ds[nz - 1];
-    q_out[(size_t)(nz - 1) * n2 + c] = x;
-    for (int k = nz - 2; k >= 0; --k) {
-        x = ds[k] - cs[k] * x;
-        q_out[(size_t)k * n2 + c] = x;
-    }
+// interface spacing of the column (closure.py:43-62): dz[0] at the surface,
+// dz[nz-1] at the bottom, the mean of the two levels elsewhere
+__device__ __forceinline__ double col_dzi(const KP& P, const ColGeo& g, int k) {
+    double m;
+    if (k == 0) return g.dz(P, 0, m);
+    if (k == P.nz) return g.dz(P, P.nz - 1, m);
+    const double a = g.dz(P, k - 1, m);
+    return 0.5 * (a + g.dz(P, k, m));
 }
 
-// column geometry: thickness, wet mask and interface spacing (closure.py:43-62)
-template <int NZM>
-__device__ __forceinline__ void column_geometry(const KP& P, size_t c, double* dz, double* m3,
-                                                double* dzi, double& depth) {
+// Momentum tridiagonal with a unit right-hand side for the column's interface
+// viscosity Km(k), k = 0..nz (reference model3d_v05.py:147-153). The forward
+// elimination keeps its coefficients in cs and its right-hand sides in q, which
+// the back substitution then overwrites with the solution.
+template <class KM>
+__device__ __forceinline__ void column_q(const KP& P, const ColGeo& g, KM Km, double* cs,
+                                         double* __restrict__ q, int c, size_t n2) {
     const int nz = P.nz;
-    const double Hc = P.H[c], mc = P.mask[c];
-    depth = 0.0;
+    double m3_k, dz_k = g.dz(P, 0, m3_k);
+    double dzi_k = dz_k;
+    double km_k = Km(0);
+    double ds = 0.0, cp = 0.0;
+#pragma unroll 2
     for (int k = 0; k < nz; ++k) {
-        dz[k] = cell_dz(P, Hc, mc, k, m3[k]);
-        depth = (k == 0) ? dz[0] : depth + dz[k];
+        double m3_k1 = 0.0, dz_k1 = 0.0;
+        if (k + 1 < nz) dz_k1 = g.dz(P, k + 1, m3_k1);
+        const double dzi_k1 = (k + 1 < nz) ? 0.5 * (dz_k + dz_k1) : dz_k;
+        const double km_k1 = Km(k + 1);
+        double sub, diag, sup;
+        implicit_row(P, k, dz_k, m3_k, m3_k1, dzi_k, dzi_k1, km_k, km_k1, P.thv_dt_drag, sub, diag, sup);
+        if (k == 0) {
+            cp = sup / diag;
+            ds = 1.0 / diag;
+        } else {
+            const double den = diag - sub * cp;
+            cp = sup / den;
+            ds = (1.0 - sub * ds) / den;
+        }
+        cs[k] = cp;
+        if (k + 1 < nz) q[(size_t)k * n2 + c] = ds;
+        km_k = km_k1;
+        dz_k = dz_k1;
+        m3_k = m3_k1;
+        dzi_k = dzi_k1;
     }
-    dzi[0] = dz[0];
-    for (int k = 1; k < nz; ++k) dzi[k] = 0.5 * (dz[k - 1] + dz[k]);
-    dzi[nz] = dz[nz - 1];
+    double x = ds;
+    q[(size_t)(nz - 1) * n2 + c] = x;
+#pragma unroll 4
+    for (int k = nz - 2; k >= 0; --k) {
+        const size_t o = (size_t)k * n2 + c;
+        x = q[o] - cs[k] * x;
+        q[o] = x;
+    }
 }
 
 template <int NZM>
 __global__ void __launch_bounds__(128) k_qsolve(KP P, const double* __restrict__ km,
                                                 double* __restrict__ q) {
     COLUMN_PROLOGUE
-    const int nz = P.nz;
-    const size_t c = nb.c;
-    double dz[NZM], m3[NZM], dzi[NZM + 1], kmc[NZM + 1], cs[NZM], ds[NZM];
-    double depth;
-    column_geometry<NZM>(P, c, dz, m3, dzi, depth);
-    for (int k = 0; k <= nz; ++k) kmc[k] = km[(size_t)k * n2 + c];
-    column_q(P, nz, dz, m3, dzi, kmc, cs, ds, q, c, n2);
+    const int c = nb.c;
+    const ColGeo g = ColGeo::load(P, c);
+    double cs[NZM];
+    column_q(P, g, [&](int k) { return km[(size_t)k * n2 + c]; }, cs, q, c, n2);
 }
 
 // ------------------------------------------------------------------ TKE closure
-// One thread per column: shear and N^2 on interfaces, the mixing lengths, the
-// implicit TKE tridiagonal (nz+1 rows), K_m/K_h, then q for the new K_m.
+// One thread per column (closure.py:141-205): shear and N^2 on interfaces, the
+// mixing lengths, the implicit TKE tridiagonal (nz+1 rows), K_m/K_h, then q for
+// the new K_m. Only N^2, shear^2, the new K_m and the elimination coefficients
+// are kept per thread; the elimination right-hand sides go to e (whose old value
+// at a level is read just before) and q. With the Gaspar lengths, the lengths
+// of interface k are formed inside the forward sweep.
 template <int NZM>
 __global__ void __launch_bounds__(128) k_closure(KP P, const double* __restrict__ u,
                                                  const double* __restrict__ v,
@@ -176,49 +194,92 @@ __global__ void __launch_bounds__(128) k_closure(KP P, const double* __restrict_
                                                  double* __restrict__ kh, double* __restrict__ q) {
     COLUMN_PROLOGUE
     const int nz = P.nz;
-    const size_t c = nb.c;
+    const int c = nb.c;
     const size_t cw = nb.at(0, -1), cs_ = nb.at(-1, 0);
-    double dz[NZM], m3[NZM], dzi[NZM + 1], nn2[NZM + 1], sh2[NZM + 1], lk[NZM + 1], le[NZM + 1];
-    double cst[NZM + 1], dst[NZM + 1];
-    double depth;
-    column_geometry<NZM>(P, c, dz, m3, dzi, depth);
-    // shear^2 and N^2 on interfaces (closure.py:150-161)
-    double uc_prev = 0.0, vc_prev = 0.0, b_prev = 0.0;
+    const ColGeo g = ColGeo::load(P, c);
+    double nn2[NZM + 1], sh2[NZM + 1], lk[NZM + 1], le[NZM + 1], cst[NZM + 1];
+    double depth = 0.0;
     for (int k = 0; k < nz; ++k) {
-        const size_t o = (size_t)k * n2;
-        const double uc = 0.5 * (u[o + c] + u[o + cw]);
-        const double vc = 0.5 * (v[o + c] + v[o + cs_]);
-        const double bk = b[o + c];
-        if (k >= 1) {
-            const double wk = m3[k - 1] * m3[k];
-            const double idz = inv_pos(dzi[k]);
-            const double du = (uc_prev - uc) * idz;
-            const double dv = (vc_prev - vc) * idz;
-            const double db = (b_prev - bk) * idz;
-            sh2[k] = (du * du + dv * dv) * wk;
-            nn2[k] = db * wk;
+        double m;
+        const double dz = g.dz(P, k, m);
+        depth = (k == 0) ? dz : depth + dz;
+    }
+    // shear^2 and N^2 on interfaces (closure.py:150-161)
+    {
+        double uc_prev = 0.0, vc_prev = 0.0, b_prev = 0.0, dz_prev = 0.0, m3_prev = 0.0;
+#pragma unroll 2
+        for (int k = 0; k < nz; ++k) {
+            const size_t o = (size_t)k * n2;
+            const double uc = 0.5 * (u[o + c] + u[o + cw]);
+            const double vc = 0.5 * (v[o + c] + v[o + cs_]);
+            const double bk = b[o + c];
+            double m3k;
+            const double dzk = g.dz(P, k, m3k);
+            if (k >= 1) {
+                const double wk = m3_prev * m3k;
+                const double idz = inv_pos(0.5 * (dz_prev + dzk));
+                const double du = (uc_prev - uc) * idz;
+                const double dv = (vc_prev - vc) * idz;
+                const double db = (b_prev - bk) * idz;
+                sh2[k] = (du * du + dv * dv) * wk;
+                nn2[k] = db * wk;
+            }
+            uc_prev = uc;
+            vc_prev = vc;
+            b_prev = bk;
+            dz_prev = dzk;
+            m3_prev = m3k;
         }
-        uc_prev = uc;
-        vc_prev = vc;
-        b_prev = bk;
     }
     sh2[0] = 0.0;
     nn2[0] = 0.0;
     sh2[nz] = 0.0;
     nn2[nz] = 0.0;
-    // mixing lengths (closure.py:65-129)
-    double zi = 0.0;
+    // recursive lengths (closure.py:106-129) need whole-column sweeps first
+    if (P.mxl_recursive) {
+        double zi = 0.0;
+        for (int k = 0; k <= nz; ++k) {
+            double m;
+            if (k >= 1) zi = (k == 1) ? g.dz(P, 0, m) : zi + g.dz(P, k - 1, m);
+            const double zb = fmax(depth - zi, 0.0);
+            const double ek = fmax(e[(size_t)k * n2 + c], P.e_min);
+            const double n2c = fmax(nn2[k], P.n2_min);
+            const double ell = sqrt(2.0 * ek / n2c);
+            le[k] = fmin(ell, fmin(zi + P.z_0, zb + P.z_0));
+        }
+        for (int k = 1; k <= nz; ++k) le[k] = fmin(le[k], le[k - 1] + col_dzi(P, g, k));
+        for (int k = nz - 1; k >= 0; --k) le[k] = fmin(le[k], le[k + 1] + col_dzi(P, g, k + 1));
+        for (int k = 0; k <= nz; ++k) {
+            double m0, m1;
+            g.dz(P, k >= 1 ? k - 1 : 0, m0);
+            g.dz(P, k, m1);
+            const double wk = (k >= 1 && k <= nz - 1) ? m0 * m1 : 0.0;
+            const double ell = le[k] * wk;
+            lk[k] = fmax(P.l_min, sqrt(ell * ell));
+            le[k] = fmax(P.l_min, fmin(ell, ell));
+        }
+    }
+    // implicit TKE rows and forward sweep (closure.py:171-198)
+    double rhs0 = 0.0, ds = 0.0, cp = 0.0, zi = 0.0;
+    double km_prev = 0.0, km_cur = km[c];
+    double m3_km1 = 0.0, dz_km1 = 0.0;  // level k-1
+    double m3_k, dz_k = g.dz(P, 0, m3_k);
     for (int k = 0; k <= nz; ++k) {
-        if (k >= 1) zi = (k == 1) ? dz[0] : zi + dz[k - 1];
-        const double wk = (k >= 1 && k <= nz - 1) ? m3[k - 1] * m3[k] : 0.0;
-        const double zb = fmax(depth - zi, 0.0);
-        const double ek = fmax(e[(size_t)k * n2 + c], P.e_min);
+        const size_t o = (size_t)k * n2 + c;
+        const double km_next = (k < nz) ? km[o + n2] : 0.0;
+        const double wk = (k >= 1 && k <= nz - 1) ? m3_km1 * m3_k : 0.0;
+        const double e_old = e[o];
+        double le_k;
         if (!P.mxl_recursive) {
-            // march away from interface k until the energy budget is spent; once
-            // the budget is zero the reference's remaining steps add exactly 0
+            // Gaspar lengths (closure.py:65-104): march away from interface k
+            // until the energy budget is spent; once the budget is zero the
+            // reference's remaining steps add exactly 0
+            if (k >= 1) zi = (k == 1) ? dz_km1 : zi + dz_km1;
+            const double zb = fmax(depth - zi, 0.0);
+            const double ek = fmax(e_old, P.e_min);
             double lu = 0.0, bud = ek;
             for (int kk = k - 1; kk >= 0 && bud > 0.0; --kk) {
-                const double n2j = fmax(nn2[kk], 0.0), dzj = dzi[kk];
+                const double n2j = fmax(nn2[kk], 0.0), dzj = col_dzi(P, g, kk);
                 const double cost = n2j * dzj * (lu + 0.5 * dzj);
                 const bool full = cost <= bud;
                 double step = dzj;
@@ -232,7 +293,7 @@ __global__ void __launch_bounds__(128) k_closure(KP P, const double* __restrict_
             double ld = 0.0;
             bud = ek;
             for (int kk = k + 1; kk <= nz && bud > 0.0; ++kk) {
-                const double n2j = fmax(nn2[kk], 0.0), dzj = dzi[kk];
+                const double n2j = fmax(nn2[kk], 0.0), dzj = col_dzi(P, g, kk);
                 const double cost = n2j * dzj * (ld + 0.5 * dzj);
                 const bool full = cost <= bud;
                 double step = dzj;
@@ -246,38 +307,17 @@ __global__ void __launch_bounds__(128) k_closure(KP P, const double* __restrict_
             lu = fmin(lu, zi + P.z_0) * wk;
             ld = fmin(ld, zb + P.z_0) * wk;
             lk[k] = fmax(P.l_min, sqrt(lu * ld));
-            le[k] = fmax(P.l_min, fmin(lu, ld));
+            le_k = fmax(P.l_min, fmin(lu, ld));
         } else {
-            const double n2c = fmax(nn2[k], P.n2_min);
-            const double ell = sqrt(2.0 * ek / n2c);
-            le[k] = fmin(ell, fmin(zi + P.z_0, zb + P.z_0));
+            le_k = le[k];
         }
-    }
-    if (P.mxl_recursive) {
-        for (int k = 1; k <= nz; ++k) le[k] = fmin(le[k], le[k - 1] + dzi[k]);
-        for (int k = nz - 1; k >= 0; --k) le[k] = fmin(le[k], le[k + 1] + dzi[k + 1]);
-        for (int k = 0; k <= nz; ++k) {
-            const double wk = (k >= 1 && k <= nz - 1) ? m3[k - 1] * m3[k] : 0.0;
-            const double ell = le[k] * wk;
-            lk[k] = fmax(P.l_min, sqrt(ell * ell));
-            le[k] = fmax(P.l_min, fmin(ell, ell));
-        }
-    }
-    // implicit TKE rows and forward sweep (closure.py:171-198)
-    double rhs0 = 0.0;
-    double km_prev = 0.0, km_cur = km[c];
-    for (int k = 0; k <= nz; ++k) {
-        const size_t o = (size_t)k * n2 + c;
-        const double km_next = (k < nz) ? km[o + n2] : 0.0;
-        const double wk = (k >= 1 && k <= nz - 1) ? m3[k - 1] * m3[k] : 0.0;
-        const double e_old = e[o];
         const double prod = (km_cur - P.nu) * sh2[k] - (kh[o] - P.kappa) * nn2[k];
-        const double diss = P.c_eps * sqrt(fmax(e_old, P.e_min)) / le[k];
+        const double diss = P.c_eps * sqrt(fmax(e_old, P.e_min)) / le_k;
         double a_up = 0.0, a_dn = 0.0;
         if (k >= 1 && k <= nz - 1) {
-            const double idzi = inv_pos(dzi[k]);
-            a_up = P.dt * (0.5 * (km_prev + km_cur)) * inv_pos(dz[k - 1]) * idzi;
-            a_dn = P.dt * (0.5 * (km_cur + km_next)) * inv_pos(dz[k]) * idzi;
+            const double idzi = inv_pos(0.5 * (dz_km1 + dz_k));
+            a_up = P.dt * (0.5 * (km_prev + km_cur)) * inv_pos(dz_km1) * idzi;
+            a_dn = P.dt * (0.5 * (km_cur + km_next)) * inv_pos(dz_k) * idzi;
         }
         double sub = -a_up, sup = -a_dn;
         double diag = 1.0 + a_up + a_dn + P.dt * diss;
@@ -289,35 +329,48 @@ __global__ void __launch_bounds__(128) k_closure(KP P, const double* __restrict_
             rhs = P.e_min;
         }
         if (k == 0) {
-            rhs = (m3[0] > 0.0) ? P.e_bb * P.ustar2[c] : P.e_min;
+            rhs = (g.kb > 0) ? P.e_bb * P.ustar2[c] : P.e_min;
             rhs0 = rhs;
-            cst[0] = sup / diag;
-            dst[0] = rhs / diag;
+            cp = sup / diag;
+            ds = rhs / diag;
         } else {
-            const double den = diag - sub * cst[k - 1];
-            cst[k] = sup / den;
-            dst[k] = (rhs - sub * dst[k - 1]) / den;
+            const double den = diag - sub * cp;
+            cp = sup / den;
+            ds = (rhs - sub * ds) / den;
         }
+        cst[k] = cp;
+        e[o] = ds;
         km_prev = km_cur;
         km_cur = km_next;
+        m3_km1 = m3_k;
+        dz_km1 = dz_k;
+        if (k + 1 < nz) {
+            dz_k = g.dz(P, k + 1, m3_k);
+        } else {
+            dz_k = 0.0;
+            m3_k = 0.0;
+        }
     }
     // back substitution, e/K update (closure.py:198-205)
     double x = 0.0;
     for (int k = nz; k >= 0; --k) {
-        x = (k == nz) ? dst[nz] : dst[k] - cst[k] * x;
-        const double wk = (k >= 1 && k <= nz - 1) ? m3[k - 1] * m3[k] : 0.0;
+        const size_t o = (size_t)k * n2 + c;
+        x = (k == nz) ? ds : e[o] - cst[k] * x;
+        double m0, m1;
+        g.dz(P, k >= 1 ? k - 1 : 0, m0);
+        g.dz(P, k < nz ? k : 0, m1);
+        const double wk = (k >= 1 && k <= nz - 1) ? m0 * m1 : 0.0;
         double en = fmax(x, P.e_min);
         en = (wk > 0.0) ? en : P.e_min;
         if (k == 0) en = rhs0;
         const double kmn = P.c_k * lk[k] * sqrt(en) * wk + P.nu;
         const double khn = (kmn - P.nu) / P.pr_t + P.kappa;
-        const size_t o = (size_t)k * n2 + c;
         e[o] = en;
         km[o] = kmn;
         kh[o] = khn;
         lk[k] = kmn;
     }
-    column_q(P, nz, dz, m3, dzi, lk, cst, dst, q, c, n2);
+    column_q(P, g, [&](int k) { return lk[k]; }, cst, q, c, n2);
 }
 
 // ------------------------------------------------------------------ Ku, Kv
@@ -374,12 +427,11 @@ __global__ void k_phi(KP P, const double* __restrict__ b, double* __restrict__ p
     COLUMN_PROLOGUE
     const int nz = P.nz;
     const size_t c = nb.c;
-    const double Hc = P.H[c], mc = P.mask[c];
     double above = 0.0, total = 0.0;
     for (int k = 0; k < nz; ++k) {
         const size_t o = (size_t)k * n2 + c;
         double m3;
-        const double dz = cell_dz(P, Hc, mc, k, m3);
+        const double dz = col_dz(P, (int)c, k, m3);
         const double bk = b[o];
         phi[o] = 0.5 * dz * bk + above;
         const double t = dz * bk;
@@ -390,7 +442,7 @@ __global__ void k_phi(KP P, const double* __restrict__ b, double* __restrict__ p
         double s = 0.0;
         for (int k = 0; k < nz; ++k) {
             double m3;
-            const double dz = cell_dz(P, Hc, mc, k, m3);
+            const double dz = col_dz(P, (int)c, k, m3);
             const double t = dz * phi[(size_t)k * n2 + c];
             s = (k == 0) ? t : s + t;
         }
@@ -623,196 +675,210 @@ __device__ __forceinline__ double explicit_dz(const KP& P, int k, double fkm1, d
 }
 
 // ------------------------------------------------------------------ explicit momentum terms
-// Everything of the predictor that depends on the old state only: the
-// common-depth pressure gradient, the old-state Coriolis average, the explicit
-// vertical diffusion and the stress + advection/viscosity increment.
-__global__ void __launch_bounds__(128) k_mom_explicit(
+// One thread per cell: everything of the predictor that depends on the old
+// state only -- the common-depth pressure gradient, the old-state Coriolis
+// average, the explicit vertical diffusion and the stress + advection/viscosity
+// increment (model3d_v05.py:352-370).
+__global__ void __launch_bounds__(256) k_mom_cell(
     KP P, const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ b,
     const double* __restrict__ phi, const double* __restrict__ w, const double* __restrict__ km,
     double* __restrict__ pgx, double* __restrict__ pgy, double* __restrict__ avpv,
     double* __restrict__ avpu, double* __restrict__ dzu, double* __restrict__ dzv,
     double* __restrict__ stu, double* __restrict__ stv) {
-    COLUMN_PROLOGUE
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= P.nx || j >= P.ny) return;
+    Nbr nb;
+    nb.init(i, j, P.nx, P.ny);
+    const size_t n2 = (size_t)P.n2;
     const int nz = P.nz;
-    const size_t c = nb.c, ce = nb.at(0, 1), cn = nb.at(1, 0);
-    const double Hc = P.H[c], mc = P.mask[c];
-    const double He = P.H[ce], me = P.mask[ce];
-    const double Hn = P.H[cn], mn = P.mask[cn];
-    double above_c = 0.0, above_e = 0.0, above_n = 0.0;
-    // face-thickness and bottom flags of the previous / current / next level
-    double dzu_m1 = 0.0, dzv_m1 = 0.0;
+    const int c = nb.c, ce = nb.at(0, 1), cn = nb.at(1, 0);
+    const size_t o = (size_t)k * n2;
+    // geometry of this level, the faces above and below, the bottom flags
+    double m3c, m3e, m3n;
+    const double dz_c = col_dz(P, c, k, m3c), dz_e = col_dz(P, ce, k, m3e), dz_n = col_dz(P, cn, k, m3n);
+    const double m3u_k = m3c * m3e * P.mask_u[c];
+    const double m3v_k = m3c * m3n * P.mask_v[c];
+    const double dzu_k = m3u_k * face_combine(P, dz_c, dz_e);
+    const double dzv_k = m3v_k * face_combine(P, dz_c, dz_n);
+    double m, dzu_p1 = 0.0, dzv_p1 = 0.0, dzu_m1 = 0.0, dzv_m1 = 0.0;
+    const double m3_cn = (k + 1 < nz) ? col_m3(P, c, k + 1) : 0.0;
+    if (k + 1 < nz) {
+        ufacek(P, nb, 0, 0, k + 1, m, dzu_p1);
+        vfacek(P, nb, 0, 0, k + 1, m, dzv_p1);
+    }
     double bottom_m1 = 0.0;
-    double m3_cur, m3_e, m3_n;
-    double dz_c = cell_dz(P, Hc, mc, 0, m3_cur);
-    double dz_e = cell_dz(P, He, me, 0, m3_e);
-    double dz_n = cell_dz(P, Hn, mn, 0, m3_n);
-    for (int k = 0; k < nz; ++k) {
-        const size_t o = (size_t)k * n2;
-        // next level's geometry (for bottom flags and face spacing)
-        double m3_cn = 0.0, m3_en = 0.0, m3_nn = 0.0, dz_cn = 0.0, dz_en = 0.0, dz_nn = 0.0;
-        if (k + 1 < nz) {
-            dz_cn = cell_dz(P, Hc, mc, k + 1, m3_cn);
-            dz_en = cell_dz(P, He, me, k + 1, m3_en);
-            dz_nn = cell_dz(P, Hn, mn, k + 1, m3_nn);
-        }
-        const double m3u_k = m3_cur * m3_e * P.mask_u[c];
-        const double m3v_k = m3_cur * m3_n * P.mask_v[c];
-        const double dzu_k = m3u_k * face_combine(P, dz_c, dz_e);
-        const double dzv_k = m3v_k * face_combine(P, dz_c, dz_n);
-        const double m3u_k1 = m3_cn * m3_en * P.mask_u[c];
-        const double m3v_k1 = m3_cn * m3_nn * P.mask_v[c];
-        const double dzu_p1 = m3u_k1 * face_combine(P, dz_cn, dz_en);
-        const double dzv_p1 = m3v_k1 * face_combine(P, dz_cn, dz_nn);
-        const double bottom_k = (m3_cur > 0.0 && m3_cn == 0.0) ? 1.0 : 0.0;
-        // ---- pressure gradient at a common depth (model3d_v05.py:211-230)
-        const double zc_c = above_c + 0.5 * dz_c;
-        const double zc_e = above_e + 0.5 * dz_e;
-        const double zc_n = above_n + 0.5 * dz_n;
-        const double phc = phi[o + c], phe = phi[o + ce], phn = phi[o + cn];
-        const double bc = b[o + c], be = b[o + ce], bn = b[o + cn];
-        double px, py;
-        if (P.pgf_correction) {
-            const double zfx = 0.5 * (zc_c + zc_e);
-            px = m3u_k * ((phe + be * (zfx - zc_e)) - (phc + bc * (zfx - zc_c))) / P.dx;
-            const double zfy = 0.5 * (zc_c + zc_n);
-            py = m3v_k * ((phn + bn * (zfy - zc_n)) - (phc + bc * (zfy - zc_c))) / P.dy;
-        } else {
-            px = m3u_k * (phe - phc) / P.dx * m3u_k;
-            py = m3v_k * (phn - phc) / P.dy * m3v_k;
-        }
-        pgx[o + c] = px;
-        pgy[o + c] = py;
-        // ---- Coriolis averages of the old state
-        avpv[o + c] = v_on_u(P, nb, v, o, k);
-        avpu[o + c] = u_on_v(P, nb, u, o, k);
-        // ---- explicit vertical diffusion (viscosity of the cell column)
-        const double K_k = km[o + c], K_k1 = km[o + n2 + c];
-        const double uk = u[o + c], vk = v[o + c];
-        const double ukm = (k > 0) ? u[o - n2 + c] : 0.0, vkm = (k > 0) ? v[o - n2 + c] : 0.0;
-        const double ukp = (k + 1 < nz) ? u[o + n2 + c] : 0.0;
-        const double vkp = (k + 1 < nz) ? v[o + n2 + c] : 0.0;
-        dzu[o + c] = explicit_dz(P, k, ukm, uk, ukp, K_k, K_k1, dzu_m1, dzu_k, dzu_p1, bottom_m1,
-                                 bottom_k, m3_cur, P.tau_u[c], P.bottom_drag);
-        dzv[o + c] = explicit_dz(P, k, vkm, vk, vkp, K_k, K_k1, dzv_m1, dzv_k, dzv_p1, bottom_m1,
-                                 bottom_k, m3_cur, P.tau_v[c], P.bottom_drag);
-        // ---- advection and horizontal viscosity, then the stress increment
-        double exu = 0.0, exv = 0.0;
-        if (P.advection != 0) {
-            exu = exu - mom_adv_u(P, nb, u, v, w, k) * m3u_k;
-            exv = exv - mom_adv_v(P, nb, u, v, w, k) * m3v_k;
-        }
-        if (P.a_h > 0.0) {
-            exu = exu + P.a_h * hlap(P, nb, u, k, 0);
-            exv = exv + P.a_h * hlap(P, nb, v, k, 1);
-        }
-        if (k == 0) {
-            stu[o + c] = P.thv_dt * P.tau_u[c] * inv_pos(dzu_k) + P.dt * exu;
-            stv[o + c] = P.thv_dt * P.tau_v[c] * inv_pos(dzv_k) + P.dt * exv;
-        } else {
-            stu[o + c] = 0.0 + P.dt * exu;
-            stv[o + c] = 0.0 + P.dt * exv;
-        }
-        // advance the column prefix sums and the level window
-        above_c = (k == 0) ? dz_c : above_c + dz_c;
-        above_e = (k == 0) ? dz_e : above_e + dz_e;
-        above_n = (k == 0) ? dz_n : above_n + dz_n;
-        dzu_m1 = dzu_k;
-        dzv_m1 = dzv_k;
-        bottom_m1 = bottom_k;
-        dz_c = dz_cn;
-        dz_e = dz_en;
-        dz_n = dz_nn;
-        m3_cur = m3_cn;
-        m3_e = m3_en;
-        m3_n = m3_nn;
+    if (k > 0) {
+        ufacek(P, nb, 0, 0, k - 1, m, dzu_m1);
+        vfacek(P, nb, 0, 0, k - 1, m, dzv_m1);
+        bottom_m1 = (col_m3(P, c, k - 1) > 0.0 && m3c == 0.0) ? 1.0 : 0.0;
+    }
+    const double bottom_k = (m3c > 0.0 && m3_cn == 0.0) ? 1.0 : 0.0;
+    // ---- pressure gradient at a common depth (model3d_v05.py:211-230)
+    const double phc = phi[o + c], phe = phi[o + ce], phn = phi[o + cn];
+    const double bc = b[o + c], be = b[o + ce], bn = b[o + cn];
+    double px, py;
+    if (P.pgf_correction) {
+        const double zc_c = col_above(P, c, k) + 0.5 * dz_c;
+        const double zc_e = col_above(P, ce, k) + 0.5 * dz_e;
+        const double zc_n = col_above(P, cn, k) + 0.5 * dz_n;
+        const double zfx = 0.5 * (zc_c + zc_e);
+        px = m3u_k * ((phe + be * (zfx - zc_e)) - (phc + bc * (zfx - zc_c))) / P.dx;
+        const double zfy = 0.5 * (zc_c + zc_n);
+        py = m3v_k * ((phn + bn * (zfy - zc_n)) - (phc + bc * (zfy - zc_c))) / P.dy;
+    } else {
+        px = m3u_k * (phe - phc) / P.dx * m3u_k;
+        py = m3v_k * (phn - phc) / P.dy * m3v_k;
+    }
+    pgx[o + c] = px;
+    pgy[o + c] = py;
+    // ---- Coriolis averages of the old state
+    avpv[o + c] = v_on_u(P, nb, v, o, k);
+    avpu[o + c] = u_on_v(P, nb, u, o, k);
+    // ---- explicit vertical diffusion (viscosity of the cell column)
+    const double K_k = km[o + c], K_k1 = km[o + n2 + c];
+    const double uk = u[o + c], vk = v[o + c];
+    const double ukm = (k > 0) ? u[o - n2 + c] : 0.0, vkm = (k > 0) ? v[o - n2 + c] : 0.0;
+    const double ukp = (k + 1 < nz) ? u[o + n2 + c] : 0.0;
+    const double vkp = (k + 1 < nz) ? v[o + n2 + c] : 0.0;
+    dzu[o + c] = explicit_dz(P, k, ukm, uk, ukp, K_k, K_k1, dzu_m1, dzu_k, dzu_p1, bottom_m1, bottom_k,
+                             m3c, P.tau_u[c], P.bottom_drag);
+    dzv[o + c] = explicit_dz(P, k, vkm, vk, vkp, K_k, K_k1, dzv_m1, dzv_k, dzv_p1, bottom_m1, bottom_k,
+                             m3c, P.tau_v[c], P.bottom_drag);
+    // ---- advection and horizontal viscosity, then the stress increment
+    double exu = 0.0, exv = 0.0;
+    if (P.advection != 0) {
+        exu = exu - mom_adv_u(P, nb, u, v, w, k) * m3u_k;
+        exv = exv - mom_adv_v(P, nb, u, v, w, k) * m3v_k;
+    }
+    if (P.a_h > 0.0) {
+        exu = exu + P.a_h * hlap(P, nb, u, k, 0);
+        exv = exv + P.a_h * hlap(P, nb, v, k, 1);
+    }
+    if (k == 0) {
+        stu[o + c] = P.thv_dt * P.tau_u[c] * inv_pos(dzu_k) + P.dt * exu;
+        stv[o + c] = P.thv_dt * P.tau_v[c] * inv_pos(dzv_k) + P.dt * exv;
+    } else {
+        stu[o + c] = 0.0 + P.dt * exu;
+        stv[o + c] = 0.0 + P.dt * exv;
     }
 }
 
 // ------------------------------------------------------------------ predictor + column solves
-// For one Picard iteration: the explicit predictors Gu, Gv with the iterate's
-// Coriolis, both tridiagonal solves with the cell column's momentum rows, the
-// cell-mask multiply and the depth-integrated transports of the result.
-template <int NZM>
-__global__ void __launch_bounds__(128) k_predictor(
+// Per cell, for one Picard iteration: the explicit predictors with the iterate's
+// Coriolis average plus the stress/advection increment -- the right-hand sides
+// of the two momentum tridiagonals (model3d_v05.py:387-393).
+__global__ void __launch_bounds__(256) k_predictor_rhs(
     KP P, const double* __restrict__ u, const double* __restrict__ v,
     const double* __restrict__ u_it, const double* __restrict__ v_it,
     const double* __restrict__ pgx, const double* __restrict__ pgy,
     const double* __restrict__ avpv, const double* __restrict__ avpu,
     const double* __restrict__ dzu, const double* __restrict__ dzv,
     const double* __restrict__ stu, const double* __restrict__ stv,
-    const double* __restrict__ gx2, const double* __restrict__ gy2, const double* __restrict__ km,
-    double* __restrict__ ghu, double* __restrict__ ghv, double* __restrict__ Ug,
-    double* __restrict__ Vg) {
+    const double* __restrict__ gx2, const double* __restrict__ gy2, double* __restrict__ ru,
+    double* __restrict__ rv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= P.nx || j >= P.ny) return;
+    Nbr nb;
+    nb.init(i, j, P.nx, P.ny);
+    const int c = nb.c;
+    const size_t o = (size_t)k * P.n2;
+    const double vcor = P.one_m_tc * avpv[o + c] + P.theta_cor * v_on_u(P, nb, v_it, o, k);
+    const double ucor = P.one_m_tc * avpu[o + c] + P.theta_cor * u_on_v(P, nb, u_it, o, k);
+    double gu, gv;
+    if (P.scheme != 2) {
+        const double m3u_k = col_m3u(P, c, k), m3v_k = col_m3v(P, c, k);
+        gu = u[o + c] + P.dt * (P.f0 * vcor + pgx[o + c]) - P.c1 * (gx2[c] * m3u_k) + P.c3 * dzu[o + c];
+        gv = v[o + c] + P.dt * (P.neg_f0 * ucor + pgy[o + c]) - P.c1 * (gy2[c] * m3v_k) + P.c3 * dzv[o + c];
+    } else {
+        gu = u[o + c] + P.dt * (P.f0 * vcor + pgx[o + c]) + P.c3 * dzu[o + c];
+        gv = v[o + c] + P.dt * (P.neg_f0 * ucor + pgy[o + c]) + P.c3 * dzv[o + c];
+    }
+    ru[o + c] = gu + stu[o + c];
+    rv[o + c] = gv + stv[o + c];
+}
+
+// Per column: both momentum tridiagonals with the cell column's rows
+// (vertical.py:17-44 on vertical_var.py:35-77 coefficients), the cell-mask
+// multiply and the depth-integrated transports (model3d_v05.py:426-433). The
+// right-hand sides arrive in gh_u/gh_v; the forward elimination overwrites them
+// with its intermediate values, the back substitution with the solution, and
+// the transports are summed in a last, downward pass to keep the reference's
+// order. Only the elimination coefficients stay in the thread.
+template <int NZM>
+__global__ void __launch_bounds__(128) k_momentum_solve(KP P, const double* __restrict__ km,
+                                                        double* __restrict__ ghu,
+                                                        double* __restrict__ ghv,
+                                                        double* __restrict__ Ug,
+                                                        double* __restrict__ Vg) {
     COLUMN_PROLOGUE
     const int nz = P.nz;
-    const size_t c = nb.c, ce = nb.at(0, 1), cn = nb.at(1, 0);
-    double dz[NZM], m3[NZM], dzi[NZM + 1], cs[NZM], dsu[NZM], dsv[NZM];
-    double depth;
-    column_geometry<NZM>(P, c, dz, m3, dzi, depth);
-    const double He = P.H[ce], me = P.mask[ce], Hn = P.H[cn], mn = P.mask[cn];
-    const bool split = P.scheme == 2;
-    const double gxe = split ? 0.0 : gx2[c], gye = split ? 0.0 : gy2[c];
+    const int c = nb.c;
+    const ColGeo g = ColGeo::load(P, c);
+    double cs[NZM];
+    double m3_k, dz_k = g.dz(P, 0, m3_k);
+    double dzi_k = dz_k;
     double km_k = km[c];
+    double du = 0.0, dv = 0.0, cp = 0.0;
+#pragma unroll 4
     for (int k = 0; k < nz; ++k) {
-        const size_t o = (size_t)k * n2;
-        const double km_k1 = km[o + n2 + c];
-        double m3e, m3n;
-        cell_dz(P, He, me, k, m3e);
-        cell_dz(P, Hn, mn, k, m3n);
-        const double m3u_k = m3[k] * m3e * P.mask_u[c];
-        const double m3v_k = m3[k] * m3n * P.mask_v[c];
-        const double vcor = P.one_m_tc * avpv[o + c] + P.theta_cor * v_on_u(P, nb, v_it, o, k);
-        const double ucor = P.one_m_tc * avpu[o + c] + P.theta_cor * u_on_v(P, nb, u_it, o, k);
-        double gu, gv;
-        if (!split) {
-            gu = u[o + c] + P.dt * (P.f0 * vcor + pgx[o + c]) - P.c1 * (gxe * m3u_k) + P.c3 * dzu[o + c];
-            gv = v[o + c] + P.dt * (P.neg_f0 * ucor + pgy[o + c]) - P.c1 * (gye * m3v_k) +
-                 P.c3 * dzv[o + c];
-        } else {
-            gu = u[o + c] + P.dt * (P.f0 * vcor + pgx[o + c]) + P.c3 * dzu[o + c];
-            gv = v[o + c] + P.dt * (P.neg_f0 * ucor + pgy[o + c]) + P.c3 * dzv[o + c];
-        }
-        const double ru = gu + stu[o + c];
-        const double rv = gv + stv[o + c];
+        const size_t o = (size_t)k * n2 + c;
+        const double km_k1 = km[o + n2];
+        const double ru = ghu[o], rv = ghv[o];
+        double m3_k1 = 0.0, dz_k1 = 0.0;
+        if (k + 1 < nz) dz_k1 = g.dz(P, k + 1, m3_k1);
+        const double dzi_k1 = (k + 1 < nz) ? 0.5 * (dz_k + dz_k1) : dz_k;
         double sub, diag, sup;
-        const double m3k1 = (k + 1 < nz) ? m3[k + 1] : 0.0;
-        implicit_row(P, k, dz[k], m3[k], m3k1, dzi[k], dzi[k + 1], km_k, km_k1, P.thv_dt_drag, sub,
-                     diag, sup);
+        implicit_row(P, k, dz_k, m3_k, m3_k1, dzi_k, dzi_k1, km_k, km_k1, P.thv_dt_drag, sub, diag, sup);
         if (k == 0) {
-            cs[0] = sup / diag;
-            dsu[0] = ru / diag;
-            dsv[0] = rv / diag;
+            cp = sup / diag;
+            du = ru / diag;
+            dv = rv / diag;
         } else {
-            const double den = diag - sub * cs[k - 1];
-            cs[k] = sup / den;
-            dsu[k] = (ru - sub * dsu[k - 1]) / den;
-            dsv[k] = (rv - sub * dsv[k - 1]) / den;
+            const double den = diag - sub * cp;
+            cp = sup / den;
+            du = (ru - sub * du) / den;
+            dv = (rv - sub * dv) / den;
         }
+        cs[k] = cp;
+        ghu[o] = du;
+        ghv[o] = dv;
         km_k = km_k1;
+        dz_k = dz_k1;
+        m3_k = m3_k1;
+        dzi_k = dzi_k1;
     }
-    double xu = dsu[nz - 1], xv = dsv[nz - 1];
-    dsu[nz - 1] = xu;
-    dsv[nz - 1] = xv;
+    double xu = du, xv = dv;
+    {
+        const size_t o = (size_t)(nz - 1) * n2 + c;
+        const double m = (nz - 1 < g.kb) ? 1.0 : 0.0;
+        ghu[o] = xu * m;
+        ghv[o] = xv * m;
+    }
+#pragma unroll 4
     for (int k = nz - 2; k >= 0; --k) {
-        xu = dsu[k] - cs[k] * xu;
-        xv = dsv[k] - cs[k] * xv;
-        dsu[k] = xu;
-        dsv[k] = xv;
+        const size_t o = (size_t)k * n2 + c;
+        const double m = (k < g.kb) ? 1.0 : 0.0;
+        xu = ghu[o] - cs[k] * xu;
+        xv = ghv[o] - cs[k] * xv;
+        ghu[o] = xu * m;
+        ghv[o] = xv * m;
     }
+    const ColGeo ge = ColGeo::load(P, nb.at(0, 1)), gn = ColGeo::load(P, nb.at(1, 0));
+    const int2 kfc = P.kface[c];
     double su = 0.0, sv = 0.0;
+#pragma unroll 4
     for (int k = 0; k < nz; ++k) {
-        const size_t o = (size_t)k * n2;
-        const double hu = dsu[k] * m3[k];
-        const double hv = dsv[k] * m3[k];
-        ghu[o + c] = hu;
-        ghv[o + c] = hv;
-        double m3e, m3n;
-        const double dze = cell_dz(P, He, me, k, m3e);
-        const double dzn = cell_dz(P, Hn, mn, k, m3n);
-        const double m3u_k = m3[k] * m3e * P.mask_u[c];
-        const double m3v_k = m3[k] * m3n * P.mask_v[c];
-        const double tu = m3u_k * face_combine(P, dz[k], dze) * hu;
-        const double tv = m3v_k * face_combine(P, dz[k], dzn) * hv;
+        const size_t o = (size_t)k * n2 + c;
+        double m3c, m3e, m3n;
+        const double dzc = g.dz(P, k, m3c);
+        const double dze = ge.dz(P, k, m3e);
+        const double dzn = gn.dz(P, k, m3n);
+        const double tu = (k < kfc.x ? 1.0 : 0.0) * face_combine(P, dzc, dze) * ghu[o];
+        const double tv = (k < kfc.y ? 1.0 : 0.0) * face_combine(P, dzc, dzn) * ghv[o];
         su = (k == 0) ? tu : su + tu;
         sv = (k == 0) ? tv : sv + tv;
     }
@@ -829,14 +895,9 @@ __global__ void k_backsub(KP P, const double* __restrict__ ghu, const double* __
     const size_t c = nb.c, ce = nb.at(0, 1), cn = nb.at(1, 0);
     const double gx = P.mask_u[c] * (eta_new[ce] - eta_new[c]) / P.dx;
     const double gy = P.mask_v[c] * (eta_new[cn] - eta_new[c]) / P.dy;
-    const double Hc = P.H[c], mc = P.mask[c], He = P.H[ce], me = P.mask[ce];
-    const double Hn = P.H[cn], mn = P.mask[cn];
     for (int k = 0; k < P.nz; ++k) {
         const size_t o = (size_t)k * n2 + c;
-        double m3, m3e, m3n;
-        cell_dz(P, Hc, mc, k, m3);
-        cell_dz(P, He, me, k, m3e);
-        cell_dz(P, Hn, mn, k, m3n);
+        const double m3 = col_m3(P, (int)c, k), m3e = col_m3(P, (int)ce, k), m3n = col_m3(P, (int)cn, k);
         const double m3u_k = m3 * m3e * P.mask_u[c];
         const double m3v_k = m3 * m3n * P.mask_v[c];
         const double qk = q[o];
@@ -938,81 +999,115 @@ __device__ __forceinline__ double tracer_rhs(const KP& P, const Nbr& nb, const d
     return rhs;
 }
 
+// One thread per cell: the right-hand sides of the implicit tracer solves.
+__global__ void __launch_bounds__(256) k_tracer_rhs(KP P, const double* __restrict__ T,
+                                                    const double* __restrict__ S,
+                                                    const double* __restrict__ bold,
+                                                    const double* __restrict__ u,
+                                                    const double* __restrict__ v,
+                                                    const double* __restrict__ w,
+                                                    const double* __restrict__ kh,
+                                                    double* __restrict__ rT, double* __restrict__ rS) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= P.nx || j >= P.ny) return;
+    Nbr nb;
+    nb.init(i, j, P.nx, P.ny);
+    const int nz = P.nz;
+    const size_t n2 = (size_t)P.n2;
+    const size_t o = (size_t)k * n2 + nb.c;
+    double m3k, m3_m1 = 0.0, m3_p1 = 0.0;
+    const double dzk = col_dz(P, nb.c, k, m3k);
+    const double dz_m1 = (k > 0) ? col_dz(P, nb.c, k - 1, m3_m1) : 0.0;
+    const double dz_p1 = (k + 1 < nz) ? col_dz(P, nb.c, k + 1, m3_p1) : 0.0;
+    if (P.tracers_ts) {
+        rT[o] = tracer_rhs(P, nb, T, u, v, w, kh, k, dzk, m3k, dz_m1, dz_p1, m3_m1, m3_p1, P.flux_t, 0.0);
+        rS[o] = tracer_rhs(P, nb, S, u, v, w, kh, k, dzk, m3k, dz_m1, dz_p1, m3_m1, m3_p1, P.flux_s, 0.0);
+    } else {
+        const double src = P.neg_n2 * (0.5 * (w[o] + w[o + n2]));
+        rT[o] = tracer_rhs(P, nb, bold, u, v, w, kh, k, dzk, m3k, dz_m1, dz_p1, m3_m1, m3_p1, 0.0, src);
+    }
+}
+
+// One thread per column: the implicit solves with the diffusivity rows
+// (shared by T and S), the cell mask, and the EOS of the new T/S
+// (model3d_v05.py:514-533). The forward elimination stores its right-hand sides
+// in the outputs; the back substitution finishes each level there, EOS
+// included, with the level-centre depth in closed form (col_above is the
+// sequential sum of the thicknesses above, bit for bit).
 template <int NZM>
-__global__ void __launch_bounds__(128) k_tracers(KP P, const double* __restrict__ T,
-                                                 const double* __restrict__ S,
-                                                 const double* __restrict__ bold,
-                                                 const double* __restrict__ u,
-                                                 const double* __restrict__ v,
-                                                 const double* __restrict__ w,
-                                                 const double* __restrict__ kh,
-                                                 double* __restrict__ T_out,
-                                                 double* __restrict__ S_out,
-                                                 double* __restrict__ b_out) {
+__global__ void __launch_bounds__(128) k_tracer_solve(KP P, const double* __restrict__ rT,
+                                                      const double* __restrict__ rS,
+                                                      const double* __restrict__ kh,
+                                                      double* __restrict__ T_out,
+                                                      double* __restrict__ S_out,
+                                                      double* __restrict__ b_out) {
     COLUMN_PROLOGUE
     const int nz = P.nz;
-    const size_t c = nb.c;
-    double dz[NZM], m3[NZM], dzi[NZM + 1], cs[NZM], d1[NZM], d2[NZM];
-    double depth;
-    column_geometry<NZM>(P, c, dz, m3, dzi, depth);
+    const int c = nb.c;
+    const ColGeo g = ColGeo::load(P, c);
+    double cs[NZM];
     const bool ts = P.tracers_ts;
+    double* __restrict__ o1 = ts ? T_out : b_out;
+    double m3_k, dz_k = g.dz(P, 0, m3_k);
+    double dzi_k = dz_k;
     double kh_k = kh[c];
+    double d1 = 0.0, d2 = 0.0, cp = 0.0;
+#pragma unroll 4
     for (int k = 0; k < nz; ++k) {
         const size_t o = (size_t)k * n2 + c;
         const double kh_k1 = kh[o + n2];
-        const double dz_m1 = (k > 0) ? dz[k - 1] : 0.0, m3_m1 = (k > 0) ? m3[k - 1] : 0.0;
-        const double dz_p1 = (k + 1 < nz) ? dz[k + 1] : 0.0, m3_p1 = (k + 1 < nz) ? m3[k + 1] : 0.0;
-        double r1, r2 = 0.0;
-        if (ts) {
-            r1 = tracer_rhs(P, nb, T, u, v, w, kh, k, dz[k], m3[k], dz_m1, dz_p1, m3_m1, m3_p1,
-                            P.flux_t, 0.0);
-            r2 = tracer_rhs(P, nb, S, u, v, w, kh, k, dz[k], m3[k], dz_m1, dz_p1, m3_m1, m3_p1,
-                            P.flux_s, 0.0);
-        } else {
-            const double src = P.neg_n2 * (0.5 * (w[o] + w[o + n2]));
-            r1 = tracer_rhs(P, nb, bold, u, v, w, kh, k, dz[k], m3[k], dz_m1, dz_p1, m3_m1, m3_p1,
-                            0.0, src);
-        }
+        double m3_k1 = 0.0, dz_k1 = 0.0;
+        if (k + 1 < nz) dz_k1 = g.dz(P, k + 1, m3_k1);
+        const double dzi_k1 = (k + 1 < nz) ? 0.5 * (dz_k + dz_k1) : dz_k;
+        const double r1 = rT[o];
+        const double r2 = ts ? rS[o] : 0.0;
         double sub, diag, sup;
-        implicit_row(P, k, dz[k], m3[k], m3_p1, dzi[k], dzi[k + 1], kh_k, kh_k1, P.thv_dt_zero, sub,
-                     diag, sup);
+        implicit_row(P, k, dz_k, m3_k, m3_k1, dzi_k, dzi_k1, kh_k, kh_k1, P.thv_dt_zero, sub, diag, sup);
         if (k == 0) {
-            cs[0] = sup / diag;
-            d1[0] = r1 / diag;
-            d2[0] = r2 / diag;
+            cp = sup / diag;
+            d1 = r1 / diag;
+            d2 = r2 / diag;
         } else {
-            const double den = diag - sub * cs[k - 1];
-            cs[k] = sup / den;
-            d1[k] = (r1 - sub * d1[k - 1]) / den;
-            d2[k] = (r2 - sub * d2[k - 1]) / den;
+            const double den = diag - sub * cp;
+            cp = sup / den;
+            d1 = (r1 - sub * d1) / den;
+            d2 = (r2 - sub * d2) / den;
+        }
+        cs[k] = cp;
+        if (k + 1 < nz) {
+            o1[o] = d1;
+            if (ts) S_out[o] = d2;
         }
         kh_k = kh_k1;
+        dz_k = dz_k1;
+        m3_k = m3_k1;
+        dzi_k = dzi_k1;
     }
-    double x1 = d1[nz - 1], x2 = d2[nz - 1];
+    double x1 = d1, x2 = d2;
+#pragma unroll 4
     for (int k = nz - 1; k >= 0; --k) {
-        if (k < nz - 1) {
-            x1 = d1[k] - cs[k] * x1;
-            x2 = d2[k] - cs[k] * x2;
-        }
-        d1[k] = x1;
-        d2[k] = x2;
-    }
-    double above = 0.0;
-    for (int k = 0; k < nz; ++k) {
         const size_t o = (size_t)k * n2 + c;
-        const double zc = above + 0.5 * dz[k];
-        above = (k == 0) ? dz[0] : above + dz[k];
+        if (k < nz - 1) {
+            x1 = o1[o] - cs[k] * x1;
+            if (ts) x2 = S_out[o] - cs[k] * x2;
+        }
+        double m3;
+        const double dz = g.dz(P, k, m3);
         if (ts) {
-            const double Tn = d1[k] * m3[k];
-            const double Sn = d2[k] * m3[k];
+            const double Tn = x1 * m3;
+            const double Sn = x2 * m3;
+            const double zc = col_above(P, c, k) + 0.5 * dz;
             T_out[o] = Tn;
             S_out[o] = Sn;
-            b_out[o] = buoyancy_of(P, Tn, Sn, zc) * m3[k];
+            b_out[o] = buoyancy_of(P, Tn, Sn, zc) * m3;
         } else {
-            b_out[o] = d1[k] * m3[k];
+            b_out[o] = x1 * m3;
         }
     }
 }
+
 
 // ------------------------------------------------------------------ EOS on a flat buffer
 __global__ void k_buoyancy(KP P, const double* __restrict__ T, const double* __restrict__ S,
@@ -1026,12 +1121,11 @@ __global__ void k_diag_buoyancy(KP P, const double* __restrict__ T, const double
                                 double* __restrict__ b) {
     COLUMN_PROLOGUE
     const size_t c = nb.c;
-    const double Hc = P.H[c], mc = P.mask[c];
     double above = 0.0;
     for (int k = 0; k < P.nz; ++k) {
         const size_t o = (size_t)k * n2 + c;
         double m3;
-        const double dz = cell_dz(P, Hc, mc, k, m3);
+        const double dz = col_dz(P, (int)c, k, m3);
         const double zc = above + 0.5 * dz;
         above = (k == 0) ? dz : above + dz;
         b[o] = buoyancy_of(P, T[o], S[o], zc) * m3;
@@ -1279,22 +1373,29 @@ void launch_phi(const KP& P, const double* b, double* phi, cudaStream_t s) {
     k_phi<<<col_grid(P), col_block(), 0, s>>>(P, b, phi);
 }
 
+static dim3 cell_block() { return dim3(32, 8, 1); }
+static dim3 cell_grid(const KP& P) { return dim3((P.nx + 31) / 32, (P.ny + 7) / 8, P.nz); }
+
 void launch_mom_explicit(const KP& P, const double* u, const double* v, const double* b,
                          const double* phi, const double* w, const double* km, double* pgx,
                          double* pgy, double* avpv, double* avpu, double* dzu, double* dzv,
                          double* stu, double* stv, cudaStream_t s) {
-    k_mom_explicit<<<col_grid(P), col_block(), 0, s>>>(P, u, v, b, phi, w, km, pgx, pgy, avpv, avpu,
-                                                      dzu, dzv, stu, stv);
+    k_mom_cell<<<cell_grid(P), cell_block(), 0, s>>>(P, u, v, b, phi, w, km, pgx, pgy, avpv, avpu, dzu,
+                                                    dzv, stu, stv);
 }
 
-void launch_predictor(const KP& P, const double* u, const double* v, const double* u_it,
-                      const double* v_it, const double* pgx, const double* pgy, const double* avpv,
-                      const double* avpu, const double* dzu, const double* dzv, const double* stu,
-                      const double* stv, const double* gx2, const double* gy2, const double* km,
-                      double* ghu, double* ghv, double* Ug, double* Vg, cudaStream_t s) {
-    NZ_DISPATCH(P.nz, (k_predictor<NZM><<<col_grid(P), col_block(), 0, s>>>(
-                          P, u, v, u_it, v_it, pgx, pgy, avpv, avpu, dzu, dzv, stu, stv, gx2, gy2,
-                          km, ghu, ghv, Ug, Vg)));
+void launch_predictor_rhs(const KP& P, const double* u, const double* v, const double* u_it,
+                          const double* v_it, const double* pgx, const double* pgy, const double* avpv,
+                          const double* avpu, const double* dzu, const double* dzv, const double* stu,
+                          const double* stv, const double* gx2, const double* gy2, double* ru, double* rv,
+                          cudaStream_t s) {
+    k_predictor_rhs<<<cell_grid(P), cell_block(), 0, s>>>(P, u, v, u_it, v_it, pgx, pgy, avpv, avpu, dzu,
+                                                          dzv, stu, stv, gx2, gy2, ru, rv);
+}
+
+void launch_momentum_solve(const KP& P, const double* km, double* ghu, double* ghv, double* Ug, double* Vg,
+                           cudaStream_t s) {
+    NZ_DISPATCH(P.nz, (k_momentum_solve<NZM><<<col_grid(P), col_block(), 0, s>>>(P, km, ghu, ghv, Ug, Vg)));
 }
 
 void launch_backsub(const KP& P, const double* ghu, const double* ghv, const double* q,
@@ -1302,11 +1403,16 @@ void launch_backsub(const KP& P, const double* ghu, const double* ghv, const dou
     k_backsub<<<col_grid(P), col_block(), 0, s>>>(P, ghu, ghv, q, eta_new, u_out, v_out);
 }
 
-void launch_tracers(const KP& P, const double* T, const double* S, const double* bold,
-                    const double* u, const double* v, const double* w, const double* kh,
-                    double* T_out, double* S_out, double* b_out, cudaStream_t s) {
-    NZ_DISPATCH(P.nz, (k_tracers<NZM><<<col_grid(P), col_block(), 0, s>>>(
-                          P, T, S, bold, u, v, w, kh, T_out, S_out, b_out)));
+void launch_tracer_rhs(const KP& P, const double* T, const double* S, const double* bold,
+                       const double* u, const double* v, const double* w, const double* kh, double* rT,
+                       double* rS, cudaStream_t s) {
+    k_tracer_rhs<<<cell_grid(P), cell_block(), 0, s>>>(P, T, S, bold, u, v, w, kh, rT, rS);
+}
+
+void launch_tracer_solve(const KP& P, const double* rT, const double* rS, const double* kh,
+                         double* T_out, double* S_out, double* b_out, cudaStream_t s) {
+    NZ_DISPATCH(P.nz, (k_tracer_solve<NZM><<<col_grid(P), col_block(), 0, s>>>(P, rT, rS, kh, T_out,
+                                                                             S_out, b_out)));
 }
 
 void launch_buoyancy_flat(const KP& P, const double* T, const double* S, const double* z, double* b,

@@ -15,16 +15,22 @@ void launch_mom_explicit(const KP& P, const double* u, const double* v, const do
                          const double* phi, const double* w, const double* km, double* pgx,
                          double* pgy, double* avpv, double* avpu, double* dzu, double* dzv,
                          double* stu, double* stv, cudaStream_t s);
-void launch_predictor(const KP& P, const double* u, const double* v, const double* u_it,
-                      const double* v_it, const double* pgx, const double* pgy, const double* avpv,
-                      const double* avpu, const double* dzu, const double* dzv, const double* stu,
-                      const double* stv, const double* gx2, const double* gy2, const double* km,
-                      double* ghu, double* ghv, double* Ug, double* Vg, cudaStream_t s);
+// right-hand sides of the two momentum tridiagonals for one Picard pass (per cell)
+void launch_predictor_rhs(const KP& P, const double* u, const double* v, const double* u_it,
+                          const double* v_it, const double* pgx, const double* pgy, const double* avpv,
+                          const double* avpu, const double* dzu, const double* dzv, const double* stu,
+                          const double* stv, const double* gx2, const double* gy2, double* ru, double* rv,
+                          cudaStream_t s);
+// both column solves in place on gh_u/gh_v, then the transports
+void launch_momentum_solve(const KP& P, const double* km, double* ghu, double* ghv, double* Ug, double* Vg,
+                           cudaStream_t s);
 void launch_backsub(const KP& P, const double* ghu, const double* ghv, const double* q,
                     const double* eta_new, double* u_out, double* v_out, cudaStream_t s);
-void launch_tracers(const KP& P, const double* T, const double* S, const double* bold,
-                    const double* u, const double* v, const double* w, const double* kh,
-                    double* T_out, double* S_out, double* b_out, cudaStream_t s);
+void launch_tracer_rhs(const KP& P, const double* T, const double* S, const double* bold,
+                       const double* u, const double* v, const double* w, const double* kh, double* rT,
+                       double* rS, cudaStream_t s);
+void launch_tracer_solve(const KP& P, const double* rT, const double* rS, const double* kh,
+                         double* T_out, double* S_out, double* b_out, cudaStream_t s);
 void launch_buoyancy_flat(const KP& P, const double* T, const double* S, const double* z, double* b,
                           int64_t n, cudaStream_t s);
 void launch_diag_buoyancy(const KP& P, const double* T, const double* S, double* b, cudaStream_t s);

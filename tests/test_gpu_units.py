@@ -108,3 +108,24 @@ def test_binary_refuses_open_boundaries(tmp_path):
     proc = subprocess.run([str(exe), str(nml)], capture_output=True, text=True, timeout=60)
     assert proc.returncode != 0
     assert "FATAL" in proc.stderr
+
+
+@pytest.mark.parametrize("nx,ny", [(66, 66), (50, 50), (96, 80), (256, 256), (40, 24)])
+def test_multigrid_paths_match_oracle(nx, ny):
+    """Every V-cycle layout: all levels on the grid (66: the coarsening stops at an odd
+    33x33), partial tiles (50, 96x80), grid levels above CTA-0 levels (256), all in CTA 0 (40x24)."""
+    from hydrostatic_ocean_core_benchmark_b200 import cases
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    s = cases.seamount_basin(nx=nx, ny=ny, nz=8, seed=nx * 1000 + ny, solver_kind="multigrid")
+    p = s.params
+    st = OceanStepper(p, s.H, s.mask, dzr=s.dzr)
+    ref = orc.OracleStepper(p, s.H, s.mask, dzr=s.dzr)
+    assert np.array_equal(st.field("ku"), ref.Ku)
+    rng = np.random.default_rng(nx + ny)
+    for _ in range(2):
+        rhs = rng.standard_normal((ny, nx))
+        x, its = st.helmholtz_solve(rhs)
+        xr, itr, ok = ref.solver.solve(rhs)
+        assert its == itr
+        assert np.array_equal(x, xr)
+    st.close()
