@@ -104,6 +104,12 @@ __device__ __forceinline__ double m3_at(const KP& P, const Nbr& n, int dj, int d
     return geo_off(P, n, dj, di, k).m3;
 }
 
+// face thickness at level k of a face whose wet levels are the top kf ones,
+// between cells of thickness dza and dzb (equals face_geo's dzf)
+__device__ __forceinline__ double face_dz(const KP& P, int kf, int k, double dza, double dzb) {
+    return (k < kf ? 1.0 : 0.0) * face_combine(P, dza, dzb);
+}
+
 #define COLUMN_PROLOGUE                                  \
     const int i = blockIdx.x * blockDim.x + threadIdx.x; \
     const int j = blockIdx.y * blockDim.y + threadIdx.y; \
@@ -380,14 +386,17 @@ __global__ void k_kukv(KP P, const double* __restrict__ q, double* __restrict__ 
     COLUMN_PROLOGUE
     const size_t c = nb.c;
     const size_t ce = nb.at(0, 1), cn = nb.at(1, 0);
+    const ColGeo gc = ColGeo::load(P, (int)c), ge = ColGeo::load(P, (int)ce), gn = ColGeo::load(P, (int)cn);
+    const int2 kf = P.kface[c];
     double su = 0.0, sv = 0.0;
+#pragma unroll 4
     for (int k = 0; k < P.nz; ++k) {
         const size_t o = (size_t)k * n2;
-        double m3f, dzf;
-        ufacek(P, nb, 0, 0, k, m3f, dzf);
-        const double tu = dzf * fmin(q[o + c], q[o + ce]);
-        vfacek(P, nb, 0, 0, k, m3f, dzf);
-        const double tv = dzf * fmin(q[o + c], q[o + cn]);
+        double m;
+        const double dzc = gc.dz(P, k, m), dze = ge.dz(P, k, m), dzn = gn.dz(P, k, m);
+        const double qc = q[o + c];
+        const double tu = face_dz(P, kf.x, k, dzc, dze) * fmin(qc, q[o + ce]);
+        const double tv = face_dz(P, kf.y, k, dzc, dzn) * fmin(qc, q[o + cn]);
         su = (k == 0) ? tu : su + tu;
         sv = (k == 0) ? tv : sv + tv;
     }
@@ -403,16 +412,21 @@ __global__ void k_wcol(KP P, const double* __restrict__ u, const double* __restr
     COLUMN_PROLOGUE
     const int nz = P.nz;
     const size_t c = nb.c, cw = nb.at(0, -1), cs_ = nb.at(-1, 0);
+    const ColGeo gc = ColGeo::load(P, (int)c), ge = ColGeo::load(P, nb.at(0, 1)),
+                 gw = ColGeo::load(P, (int)cw), gn = ColGeo::load(P, nb.at(1, 0)), gs = ColGeo::load(P, (int)cs_);
+    const int2 kf = P.kface[c];
+    const int kuw = P.kface[cw].x, kvs = P.kface[cs_].y;
     double acc = 0.0;
     w[(size_t)nz * n2 + c] = 0.0;
+#pragma unroll 4
     for (int k = nz - 1; k >= 0; --k) {
         const size_t o = (size_t)k * n2;
-        double m3f, dzu_c, dzu_w, dzv_c, dzv_s;
-        ufacek(P, nb, 0, 0, k, m3f, dzu_c);
-        ufacek(P, nb, 0, -1, k, m3f, dzu_w);
-        vfacek(P, nb, 0, 0, k, m3f, dzv_c);
-        vfacek(P, nb, -1, 0, k, m3f, dzv_s);
-        const double m3 = m3_at(P, nb, 0, 0, k);
+        double m3, m;
+        const double dzc = gc.dz(P, k, m3);
+        const double dzu_c = face_dz(P, kf.x, k, dzc, ge.dz(P, k, m));
+        const double dzu_w = face_dz(P, kuw, k, gw.dz(P, k, m), dzc);
+        const double dzv_c = face_dz(P, kf.y, k, dzc, gn.dz(P, k, m));
+        const double dzv_s = face_dz(P, kvs, k, gs.dz(P, k, m), dzc);
         const double td = m3 * ((dzu_c * u[o + c] - dzu_w * u[o + cw]) / P.dx +
                                 (dzv_c * v[o + c] - dzv_s * v[o + cs_]) / P.dy);
         acc = (k == nz - 1) ? td : acc + td;
@@ -427,11 +441,13 @@ __global__ void k_phi(KP P, const double* __restrict__ b, double* __restrict__ p
     COLUMN_PROLOGUE
     const int nz = P.nz;
     const size_t c = nb.c;
+    const ColGeo g = ColGeo::load(P, (int)c);
     double above = 0.0, total = 0.0;
+#pragma unroll 4
     for (int k = 0; k < nz; ++k) {
         const size_t o = (size_t)k * n2 + c;
         double m3;
-        const double dz = col_dz(P, (int)c, k, m3);
+        const double dz = g.dz(P, k, m3);
         const double bk = b[o];
         phi[o] = 0.5 * dz * bk + above;
         const double t = dz * bk;
@@ -442,7 +458,7 @@ __global__ void k_phi(KP P, const double* __restrict__ b, double* __restrict__ p
         double s = 0.0;
         for (int k = 0; k < nz; ++k) {
             double m3;
-            const double dz = col_dz(P, (int)c, k, m3);
+            const double dz = g.dz(P, k, m3);
             const double t = dz * phi[(size_t)k * n2 + c];
             s = (k == 0) ? t : s + t;
         }
@@ -679,7 +695,7 @@ __device__ __forceinline__ double explicit_dz(const KP& P, int k, double fkm1, d
 // state only -- the common-depth pressure gradient, the old-state Coriolis
 // average, the explicit vertical diffusion and the stress + advection/viscosity
 // increment (model3d_v05.py:352-370).
-__global__ void __launch_bounds__(256) k_mom_cell(
+__global__ void __launch_bounds__(256, 4) k_mom_cell(
     KP P, const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ b,
     const double* __restrict__ phi, const double* __restrict__ w, const double* __restrict__ km,
     double* __restrict__ pgx, double* __restrict__ pgy, double* __restrict__ avpv,
@@ -895,11 +911,14 @@ __global__ void k_backsub(KP P, const double* __restrict__ ghu, const double* __
     const size_t c = nb.c, ce = nb.at(0, 1), cn = nb.at(1, 0);
     const double gx = P.mask_u[c] * (eta_new[ce] - eta_new[c]) / P.dx;
     const double gy = P.mask_v[c] * (eta_new[cn] - eta_new[c]) / P.dy;
+    const int kb = P.kinfo[c].y;
+    const int2 kf = P.kface[c];
+#pragma unroll 4
     for (int k = 0; k < P.nz; ++k) {
         const size_t o = (size_t)k * n2 + c;
-        const double m3 = col_m3(P, (int)c, k), m3e = col_m3(P, (int)ce, k), m3n = col_m3(P, (int)cn, k);
-        const double m3u_k = m3 * m3e * P.mask_u[c];
-        const double m3v_k = m3 * m3n * P.mask_v[c];
+        const double m3 = k < kb ? 1.0 : 0.0;
+        const double m3u_k = k < kf.x ? 1.0 : 0.0;
+        const double m3v_k = k < kf.y ? 1.0 : 0.0;
         const double qk = q[o];
         u_out[o] = (ghu[o] - P.c2 * qk * gx * m3u_k) * m3;
         v_out[o] = (ghv[o] - P.c2 * qk * gy * m3v_k) * m3;
@@ -1000,7 +1019,7 @@ __device__ __forceinline__ double tracer_rhs(const KP& P, const Nbr& nb, const d
 }
 
 // One thread per cell: the right-hand sides of the implicit tracer solves.
-__global__ void __launch_bounds__(256) k_tracer_rhs(KP P, const double* __restrict__ T,
+__global__ void __launch_bounds__(256, 4) k_tracer_rhs(KP P, const double* __restrict__ T,
                                                     const double* __restrict__ S,
                                                     const double* __restrict__ bold,
                                                     const double* __restrict__ u,
@@ -1138,14 +1157,16 @@ __global__ void k_transport(KP P, const double* __restrict__ u, const double* __
                             double* __restrict__ U, double* __restrict__ V) {
     COLUMN_PROLOGUE
     const size_t c = nb.c;
+    const ColGeo gc = ColGeo::load(P, (int)c), ge = ColGeo::load(P, nb.at(0, 1)), gn = ColGeo::load(P, nb.at(1, 0));
+    const int2 kf = P.kface[c];
     double su = 0.0, sv = 0.0;
+#pragma unroll 4
     for (int k = 0; k < P.nz; ++k) {
         const size_t o = (size_t)k * n2 + c;
-        double m, dzf;
-        ufacek(P, nb, 0, 0, k, m, dzf);
-        const double tu = dzf * u[o];
-        vfacek(P, nb, 0, 0, k, m, dzf);
-        const double tv = dzf * v[o];
+        double m;
+        const double dzc = gc.dz(P, k, m);
+        const double tu = face_dz(P, kf.x, k, dzc, ge.dz(P, k, m)) * u[o];
+        const double tv = face_dz(P, kf.y, k, dzc, gn.dz(P, k, m)) * v[o];
         su = (k == 0) ? tu : su + tu;
         sv = (k == 0) ? tv : sv + tv;
     }
@@ -1290,18 +1311,21 @@ __global__ void k_split_correct(KP P, const double* __restrict__ ghu, const doub
                                 double* __restrict__ u_out, double* __restrict__ v_out) {
     COLUMN_PROLOGUE
     const size_t c = nb.c;
+    const ColGeo gc = ColGeo::load(P, (int)c), ge = ColGeo::load(P, nb.at(0, 1)), gn = ColGeo::load(P, nb.at(1, 0));
+    const int2 kf = P.kface[c];
     double Hu = 0.0, Hv = 0.0;
     for (int k = 0; k < P.nz; ++k) {
-        double m, du, dv;
-        ufacek(P, nb, 0, 0, k, m, du);
-        vfacek(P, nb, 0, 0, k, m, dv);
+        double m;
+        const double dzc = gc.dz(P, k, m);
+        const double du = face_dz(P, kf.x, k, dzc, ge.dz(P, k, m));
+        const double dv = face_dz(P, kf.y, k, dzc, gn.dz(P, k, m));
         Hu = (k == 0) ? du : Hu + du;
         Hv = (k == 0) ? dv : Hv + dv;
     }
     const double ihu = inv_pos(Hu), ihv = inv_pos(Hv);
     for (int k = 0; k < P.nz; ++k) {
         const size_t o = (size_t)k * n2 + c;
-        const double m3u_k = m3u_at(P, nb, 0, 0, k), m3v_k = m3v_at(P, nb, 0, 0, k);
+        const double m3u_k = k < kf.x ? 1.0 : 0.0, m3v_k = k < kf.y ? 1.0 : 0.0;
         u_out[o] = (ghu[o] - Ug[c] * ihu + U[c] * ihu) * m3u_k;
         v_out[o] = (ghv[o] - Vg[c] * ihv + V[c] * ihv) * m3v_k;
     }
