@@ -145,30 +145,47 @@ __device__ void colour_phase(const HLevel& L, double* x, const double* b, int co
 // ------------------------------------------------------------------ pairwise sums
 // Calls f(e) exactly once per element of level 0, grouped by NumPy's leaves;
 // f returns the two values to accumulate. Writes the per-leaf sums.
+//
+// One warp per leaf (a leaf has at most 128 elements), consecutive leaves on
+// different CTAs. Lane l evaluates f for leaf elements l, l+32, l+64, l+96 with
+// independent loads. The eight interleaved accumulators of NumPy's unrolled
+// loop are then formed in their sequential order by lanes j = 0..7 (element
+// 8t + j sits on lane (8t + j) mod 32 in register t / 32 -- the same register on
+// every lane for a given t), folded as ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)), and
+// the len mod 8 remaining elements are added one by one.
 template <class F>
 __device__ void leaf_phase(const HelmParams& H, F f, double* outA, double* outB) {
     const int lane = threadIdx.x & 31;
     const int lane8 = lane & 7;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int base = warp * 4; base < H.n_leaves; base += nwarps * 4) {
-        const int L = base + (lane >> 3);
-        const bool act = L < H.n_leaves;
-        int s = 0, len = 0;
-        if (act) {
-            s = H.leaf_start[L];
-            len = H.leaf_start[L + 1] - s;
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    const int my = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // leaf L runs on CTA L mod grid
+    for (int L = my; L < H.n_leaves; L += nwarps) {
+        const int s = H.leaf_start[L];
+        const int len = H.leaf_start[L + 1] - s;
+        double va[4], vb[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = lane + 32 * q;
+            double2 v = make_double2(0.0, 0.0);
+            if (e < len) v = f(s + e);
+            va[q] = v.x;
+            vb[q] = v.y;
         }
+        // element e of the leaf on every lane; e must be the same on all lanes or
+        // share e / 32 (the source register is chosen by the caller's e)
+        auto pick = [&](const double* r, int e) {
+            const int q = e >> 5;
+            const double x = q == 0 ? r[0] : (q == 1 ? r[1] : (q == 2 ? r[2] : r[3]));
+            return __shfl_sync(0xffffffffu, x, e & 31);
+        };
         const int m = len >= 8 ? len - (len % 8) : 0;
         double ra = 0.0, rb = 0.0;
-        if (act && len >= 8) {
-            double2 v = f(s + lane8);
-            ra = v.x;
-            rb = v.y;
-            for (int t = 8 + lane8; t < m; t += 8) {
-                v = f(s + t);
-                ra = ra + v.x;
-                rb = rb + v.y;
+        if (len >= 8) {
+            ra = pick(va, lane8);
+            rb = pick(vb, lane8);
+            for (int t = 8; t < m; t += 8) {
+                ra = ra + pick(va, t + lane8);
+                rb = rb + pick(vb, t + lane8);
             }
         }
         ra = ra + __shfl_xor_sync(0xffffffffu, ra, 1);
@@ -177,14 +194,13 @@ __device__ void leaf_phase(const HelmParams& H, F f, double* outA, double* outB)
         rb = rb + __shfl_xor_sync(0xffffffffu, rb, 2);
         ra = ra + __shfl_xor_sync(0xffffffffu, ra, 4);
         rb = rb + __shfl_xor_sync(0xffffffffu, rb, 4);
-        if (act && lane8 == 0) {
-            double a = len >= 8 ? ra : 0.0;
-            double bsum = len >= 8 ? rb : 0.0;
-            for (int t = m; t < len; ++t) {
-                const double2 v = f(s + t);
-                a = a + v.x;
-                bsum = bsum + v.y;
-            }
+        double a = len >= 8 ? ra : 0.0;
+        double bsum = len >= 8 ? rb : 0.0;
+        for (int t = m; t < len; ++t) {
+            a = a + pick(va, t);
+            bsum = bsum + pick(vb, t);
+        }
+        if (lane == 0) {
             outA[L] = a;
             if (outB) outB[L] = bsum;
         }
