@@ -261,6 +261,7 @@ __device__ __forceinline__ TileRefs tile_refs(double* base) {
 // (or zero), plus the coarse correction e * mask when C is given
 __device__ void tile_load(const HLevel& L, int i0, int j0, const double* xin, const HLevel* C,
                           TileRefs t) {
+#pragma unroll 4
     for (int r = threadIdx.x; r < RN; r += blockDim.x) {
         const int rj = r / RW, ri = r - rj * RW;
         const int gi = wrap_any(i0 - HALO + ri, L.nx), gj = wrap_any(j0 - HALO + rj, L.ny);
