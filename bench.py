@@ -306,33 +306,92 @@ def run_ours(args, rank, world, local_rank):
         raise RuntimeError(f"the timed run failed: {stats}")
     value = world * n3 * args.steps / (ms_max / 1e3)
 
-    # end to end through the C ABI with pinned host buffers, every step
+    # end to end through the C ABI with pinned host buffers, every step. Each of
+    # `members` independent model states (an ensemble; member 0 is the timed
+    # state) round-trips through its own pinned host buffers every step: upload
+    # (oc_set_state_async) on one stream, the step on the compute stream, download
+    # (oc_get_state_async) on a third, ordered per member with events, so one
+    # member's copies overlap another's step. All steps share one compute stream,
+    # so the multigrid solves never run concurrently.
     e2e = None
     if args.e2e_steps > 0:
+        fields = ("eta", "u", "v", "b", "T", "S", "e")
         host = st.get_state()
-        pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
-                  for k, v in host.items() if k in ("eta", "u", "v", "b", "T", "S", "e")}
-        outs = {k: torch.empty_like(v).pin_memory() for k, v in pinned.items()}
-        h2d = sum(v.numel() * 8 for v in pinned.values())
-        d2h = sum(v.numel() * 8 for v in outs.values())
+        members = max(1, args.e2e_members)
+        steppers = [st] + [OceanStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c,
+                                        device=local_rank) for _ in range(members - 1)]
+        bufs = [{k: torch.from_numpy(np.ascontiguousarray(host[k])).pin_memory() for k in fields}
+                for _ in range(members)]
+        for m in range(1, members):
+            steppers[m].set_state(**{k: host[k] for k in fields})
+        h2d = sum(v.numel() * 8 for v in bufs[0].values())
+        d2h = h2d
+        s_in = torch.cuda.Stream(device=local_rank)
+        s_cmp = torch.cuda.Stream(device=local_rank)
+        s_out = torch.cuda.Stream(device=local_rank)
+        ev_out = [None] * members
+
+        def round_trip(n):
+            m = n % members
+            if ev_out[m] is not None:
+                s_in.wait_event(ev_out[m])
+            steppers[m].set_state_async(s_in, **bufs[m])
+            e_in = torch.cuda.Event()
+            e_in.record(s_in)
+            s_cmp.wait_event(e_in)
+            steppers[m].step(1, stream=s_cmp)
+            e_c = torch.cuda.Event()
+            e_c.record(s_cmp)
+            s_out.wait_event(e_c)
+            steppers[m].get_state_async(s_out, bufs[m])
+            ev_out[m] = torch.cuda.Event()
+            ev_out[m].record(s_out)
+
+        for n in range(members):  # warm-up round
+            round_trip(n)
         torch.cuda.synchronize()
         barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(torch.cuda.default_stream())
-        for _ in range(args.e2e_steps):
-            st.set_state(**pinned)
-            st.step(1)
-            st.get_state(out=outs)
-            pinned, outs = outs, pinned
-        e1.record(torch.cuda.default_stream())
+        e0.record(s_in)
+        for n in range(args.e2e_steps):
+            round_trip(n)
+        for ev in ev_out:
+            s_in.wait_event(ev)
+        e1.record(s_in)
         e1.synchronize()
+        torch.cuda.synchronize()
         barrier()
         e_ms = max_over_ranks(e0.elapsed_time(e1))
+        for m in range(members):
+            stm = steppers[m].stats()
+            if stm["solver_failures"] or stm["diverged"]:
+                raise RuntimeError(f"end-to-end member {m} failed: {stm}")
+        # the same protocol with one state, every step waiting for the previous one
+        seq_steps = max(1, args.e2e_steps // members)
+        pinned = bufs[0]
+        torch.cuda.synchronize()
+        q0 = torch.cuda.Event(enable_timing=True)
+        q1 = torch.cuda.Event(enable_timing=True)
+        q0.record(torch.cuda.default_stream())
+        for _ in range(seq_steps):
+            st.set_state(**pinned)
+            st.step(1)
+            st.get_state(out=pinned)
+        q1.record(torch.cuda.default_stream())
+        q1.synchronize()
+        q_ms = max_over_ranks(q0.elapsed_time(q1))
+        for m in range(1, members):
+            steppers[m].close()
         e2e = {"value": world * n3 * args.e2e_steps / (e_ms / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "steps": args.e2e_steps, "ms_per_step": e_ms / args.e2e_steps,
-               "path": "OceanStepper.set_state/step/get_state (oc_set_state, oc_step, oc_get_state)"}
+               "steps": args.e2e_steps, "ms_per_step": e_ms / args.e2e_steps, "members": members,
+               "path": "OceanStepper.set_state_async/step/get_state_async (oc_set_state_async, "
+                       "oc_step, oc_get_state_async), pinned host buffers, one round trip of the "
+                       "full state per step",
+               "sequential": {"value": world * n3 * seq_steps / (q_ms / 1e3), "unit": UNIT,
+                              "steps": seq_steps, "ms_per_step": q_ms / seq_steps,
+                              "path": "OceanStepper.set_state/step/get_state (synchronous, one state)"}}
 
     # roofline of the dominant kernel
     peak, peak_kind = measured_hbm_peak()
@@ -402,7 +461,9 @@ def main():
     ap.add_argument("--ny", type=int, default=512)
     ap.add_argument("--nz", type=int, default=50)
     ap.add_argument("--seed", type=int, default=20261203)
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=12)
+    ap.add_argument("--e2e-members", type=int, default=3,
+                    help="independent states round-tripped through the host in turn (overlap)")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-nx", type=int, default=128)
     ap.add_argument("--no-cpu", action="store_true")

@@ -706,7 +706,8 @@ static int copy_in(double* dst, const double* src, size_t n, int on_device, cuda
                : 1;
 }
 
-int oc_set_state(oc_handle* h, const oc_state_view* s, int32_t on_device) {
+// enqueue the copies (and the derived fields) of a state on stream st
+static int set_state_on(oc_handle* h, const oc_state_view* s, int32_t on_device, cudaStream_t st) {
     if (!h || !s) return OC_ERR_ARG;
     if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain before the state");
     if (!s->eta || !s->u || !s->v) return fail(h, OC_ERR_ARG, "eta, u and v are required");
@@ -714,7 +715,6 @@ int oc_set_state(oc_handle* h, const oc_state_view* s, int32_t on_device) {
     if (ts && (!s->T || !s->S)) return fail(h, OC_ERR_ARG, "T and S are required with TS tracers");
     if (!ts && !s->b) return fail(h, OC_ERR_ARG, "b is required with buoyancy tracers");
     cudaSetDevice(h->cfg.device);
-    cudaStream_t st = 0;
     const int c = h->cur;
     int bad = 0;
     bad |= copy_in(h->ETA[c], s->eta, h->n2, on_device, st);
@@ -741,10 +741,20 @@ int oc_set_state(oc_handle* h, const oc_state_view* s, int32_t on_device) {
         launch_kukv(h->P, h->q, h->Ku, h->Kv, st);
         if (h->solver) h->solver->rebuild(st);
     }
-    const cudaError_t e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_fail(h, e, "oc_set_state");
     h->has_state = true;
     return OC_OK;
+}
+
+int oc_set_state(oc_handle* h, const oc_state_view* s, int32_t on_device) {
+    const int rc = set_state_on(h, s, on_device, 0);
+    if (rc) return rc;
+    const cudaError_t e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) return cuda_fail(h, e, "oc_set_state");
+    return OC_OK;
+}
+
+int oc_set_state_async(oc_handle* h, const oc_state_view* s, int32_t on_device, void* stream) {
+    return set_state_on(h, s, on_device, (cudaStream_t)stream);
 }
 
 int oc_reset_mixing(oc_handle* h) {
@@ -766,14 +776,8 @@ static int device_status(oc_handle* h) {
     return st;
 }
 
-int oc_get_state(oc_handle* h, const oc_state_view* s, int32_t on_device) {
-    if (!h || !s) return OC_ERR_ARG;
-    if (!h->has_state) return fail(h, OC_ERR_STATE, "no state has been set");
-    cudaSetDevice(h->cfg.device);
-    cudaError_t e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) return cuda_fail(h, e, "oc_get_state");
-    const int dst = device_status(h);
-    if (dst) return fail(h, dst, "a device-side wait ran out its bound");
+// enqueue the copies of the current state on stream st
+static int get_state_on(oc_handle* h, const oc_state_view* s, int32_t on_device, cudaStream_t st) {
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     const int c = h->cur;
     const bool ts = h->cfg.tracers == OC_TRACERS_TS;
@@ -787,10 +791,31 @@ int oc_get_state(oc_handle* h, const oc_state_view* s, int32_t on_device) {
                  {s->km, h->km, h->n3i},     {s->kh, h->kh, h->n3i}};
     for (auto& it : items) {
         if (!it.dst || !it.src) continue;
-        e = cudaMemcpy(it.dst, it.src, it.n * sizeof(double), kind);
+        const cudaError_t e = cudaMemcpyAsync(it.dst, it.src, it.n * sizeof(double), kind, st);
         if (e != cudaSuccess) return cuda_fail(h, e, "oc_get_state copy");
     }
     return OC_OK;
+}
+
+int oc_get_state(oc_handle* h, const oc_state_view* s, int32_t on_device) {
+    if (!h || !s) return OC_ERR_ARG;
+    if (!h->has_state) return fail(h, OC_ERR_STATE, "no state has been set");
+    cudaSetDevice(h->cfg.device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(h, e, "oc_get_state");
+    const int dst = device_status(h);
+    if (dst) return fail(h, dst, "a device-side wait ran out its bound");
+    const int rc = get_state_on(h, s, on_device, 0);
+    if (rc) return rc;
+    e = cudaStreamSynchronize(0);
+    return e == cudaSuccess ? OC_OK : cuda_fail(h, e, "oc_get_state");
+}
+
+int oc_get_state_async(oc_handle* h, const oc_state_view* s, int32_t on_device, void* stream) {
+    if (!h || !s) return OC_ERR_ARG;
+    if (!h->has_state) return fail(h, OC_ERR_STATE, "no state has been set");
+    cudaSetDevice(h->cfg.device);
+    return get_state_on(h, s, on_device, (cudaStream_t)stream);
 }
 
 int oc_step(oc_handle* h, int32_t n_steps, void* stream) {

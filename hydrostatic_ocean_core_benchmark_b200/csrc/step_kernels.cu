@@ -926,126 +926,179 @@ __global__ void k_backsub(KP P, const double* __restrict__ ghu, const double* __
 }
 
 // ------------------------------------------------------------------ tracers + EOS
-// Flux-form advection with the face masks and real face thickness
-// (model3d_v05.py:482-512) of tracer C at level k
-__device__ double tracer_adv(const KP& P, const Nbr& nb, const double* __restrict__ C,
-                             const double* __restrict__ u, const double* __restrict__ v,
-                             const double* __restrict__ w, int k, double dzc, double m3c) {
-    const size_t n2 = P.n2;
-    const size_t o = (size_t)k * n2;
+// Tiled right-hand sides of the implicit tracer solves (model3d_v05.py:466-512).
+// A CTA owns a TRX x TRY tile of columns and TR_KL levels and marches down the
+// levels. At each level the horizontal face fluxes of the tile -- TRX + 1 east
+// faces per row, TRY + 1 north faces per column -- are formed once into shared
+// memory (double-buffered, one barrier per level); a per-cell form would form
+// every face twice, once from each side. The vertical face at the bottom of a
+// cell is carried to the next level as the face at its top, and the column's
+// tracer values, w and K_h roll in registers. Every face and cell value is
+// formed by the reference's operations in the reference's order.
+constexpr int TRX = 32, TRY = 8, TR_KL = 10;
+
+struct Stencil4 {
+    int cm, c0, c1, cp;  // far upstream, the two cells of the face, far downstream (flat 2D)
+};
+
+// the east face of column i in row j (cells i-1, i, i+1, i+2), periodic index layout
+__device__ __forceinline__ Stencil4 xstencil(int j, int i, int nx, int ny) {
+    const int r = wrapi(j, ny) * nx;
+    return Stencil4{r + wrapi(i - 1, nx), r + wrapi(i, nx), r + wrapi(i + 1, nx), r + wrapi(i + 2, nx)};
+}
+
+// the north face of row j in column i (rows j-1, j, j+1, j+2)
+__device__ __forceinline__ Stencil4 ystencil(int j, int i, int nx, int ny) {
+    const int ii = wrapi(i, nx);
+    return Stencil4{wrapi(j - 1, ny) * nx + ii, wrapi(j, ny) * nx + ii, wrapi(j + 1, ny) * nx + ii,
+                    wrapi(j + 2, ny) * nx + ii};
+}
+
+// tracer value on a horizontal face: centred, kappa/TVD with the dry far-cell
+// fallback, or first-order upwind (model3d_v05.py:482-497)
+__device__ __forceinline__ double tracer_face(const KP& P, const double* __restrict__ C, size_t o,
+                                              const Stencil4& s, double vel, int k) {
+    const double a = C[o + s.c0], b = C[o + s.c1];
+    if (P.advection == 1) return 0.5 * (a + b);
+    if (P.advection >= 3)
+        return kappa_face(P, C[o + s.cm], a, b, C[o + s.cp], vel, col_m3(P, s.cm, k), col_m3(P, s.cp, k),
+                          P.advection == 4);
+    return vel > 0.0 ? a : b;
+}
+
+// flux through an east (ax = 0) or north (ax = 1) face: face thickness x
+// normal velocity x face value (model3d_v05.py:498-501)
+__device__ __forceinline__ double tracer_flux(const KP& P, const double* __restrict__ C,
+                                              const double* __restrict__ vel_f, size_t o,
+                                              const Stencil4& s, int k, int ax) {
+    const double vel = vel_f[o + s.c0];
+    const int2 kf = P.kface[s.c0];
+    double m;
+    const double dzf = face_dz(P, ax == 0 ? kf.x : kf.y, k, col_dz(P, s.c0, k, m), col_dz(P, s.c1, k, m));
+    return dzf * vel * tracer_face(P, C, o, s, vel, k);
+}
+
+// tracer value on interface kk of a column (0 = surface) from the column values
+// at kk-2, kk-1, kk, kk+1 and w there (model3d_v05.py:502-510)
+__device__ __forceinline__ double tracer_vface(const KP& P, const ColGeo& g, int kk, double f_m2, double f_m1,
+                                               double f_0, double f_p1, double wv) {
     const int nz = P.nz;
-    auto F = [&](int dj, int di) { return C[o + nb.at(dj, di)]; };
-    auto Fk = [&](int kk) { return C[(size_t)kk * n2 + nb.c]; };
-    const int adv = P.advection;
-    const bool lim = adv == 4;
-    const double u0 = u[o + nb.c], uw = u[o + nb.at(0, -1)];
-    const double v0 = v[o + nb.c], vs = v[o + nb.at(-1, 0)];
-    double cx0, cxw, cy0, cys;
-    if (adv == 1) {
-        cx0 = 0.5 * (F(0, 0) + F(0, 1));
-        cxw = 0.5 * (F(0, -1) + F(0, 0));
-        cy0 = 0.5 * (F(0, 0) + F(1, 0));
-        cys = 0.5 * (F(-1, 0) + F(0, 0));
-    } else if (adv >= 3) {
-        cx0 = kappa_face(P, F(0, -1), F(0, 0), F(0, 1), F(0, 2), u0, m3_at(P, nb, 0, -1, k),
-                         m3_at(P, nb, 0, 2, k), lim);
-        cxw = kappa_face(P, F(0, -2), F(0, -1), F(0, 0), F(0, 1), uw, m3_at(P, nb, 0, -2, k),
-                         m3_at(P, nb, 0, 1, k), lim);
-        cy0 = kappa_face(P, F(-1, 0), F(0, 0), F(1, 0), F(2, 0), v0, m3_at(P, nb, -1, 0, k),
-                         m3_at(P, nb, 2, 0, k), lim);
-        cys = kappa_face(P, F(-2, 0), F(-1, 0), F(0, 0), F(1, 0), vs, m3_at(P, nb, -2, 0, k),
-                         m3_at(P, nb, 1, 0, k), lim);
-    } else {
-        cx0 = u0 > 0.0 ? F(0, 0) : F(0, 1);
-        cxw = uw > 0.0 ? F(0, -1) : F(0, 0);
-        cy0 = v0 > 0.0 ? F(0, 0) : F(1, 0);
-        cys = vs > 0.0 ? F(-1, 0) : F(0, 0);
+    if (kk == 0) return f_0;
+    if (kk == nz) return 0.0;
+    if (P.advection >= 3) {
+        const double fu = (kk >= 2) ? f_m2 : 0.0;
+        const double fd = (kk + 1 <= nz - 1) ? f_p1 : 0.0;
+        const bool hu = (kk >= 2) && kk - 2 < g.kb;
+        const bool hd = (kk + 1 <= nz - 1) && kk + 1 < g.kb;
+        return kappa_face_z(P, fu, f_m1, f_0, fd, wv, hu, hd, P.advection == 4);
     }
-    double m, dzu0, dzuw, dzv0, dzvs;
-    ufacek(P, nb, 0, 0, k, m, dzu0);
-    ufacek(P, nb, 0, -1, k, m, dzuw);
-    vfacek(P, nb, 0, 0, k, m, dzv0);
-    vfacek(P, nb, -1, 0, k, m, dzvs);
-    const double fx0 = dzu0 * u0 * cx0, fxw = dzuw * uw * cxw;
-    const double fy0 = dzv0 * v0 * cy0, fys = dzvs * vs * cys;
-    const double inv = inv_pos(dzc);
-    const double hdiv = ((fx0 - fxw) / P.dx + (fy0 - fys) / P.dy) * inv;
-    double cf[2];
-    for (int t = 0; t < 2; ++t) {
-        const int kk = k + t;
-        if (kk == 0) {
-            cf[t] = Fk(0);
-        } else if (kk == nz) {
-            cf[t] = 0.0;
-        } else if (adv >= 3) {
-            const double fu = (kk >= 2) ? Fk(kk - 2) : 0.0;
-            const double fd = (kk + 1 <= nz - 1) ? Fk(kk + 1) : 0.0;
-            const bool hu = (kk >= 2) && m3_at(P, nb, 0, 0, kk - 2) > 0.0;
-            const bool hd = (kk + 1 <= nz - 1) && m3_at(P, nb, 0, 0, kk + 1) > 0.0;
-            cf[t] = kappa_face_z(P, fu, Fk(kk - 1), Fk(kk), fd, w[(size_t)kk * n2 + nb.c], hu, hd, lim);
-        } else {
-            cf[t] = 0.5 * (Fk(kk - 1) + Fk(kk));
+    return 0.5 * (f_m1 + f_0);
+}
+
+__global__ void __launch_bounds__(TRX * TRY, 4) k_tracer_rhs(KP P, const double* __restrict__ T,
+                                                             const double* __restrict__ S,
+                                                             const double* __restrict__ bold,
+                                                             const double* __restrict__ u,
+                                                             const double* __restrict__ v,
+                                                             const double* __restrict__ w,
+                                                             const double* __restrict__ kh,
+                                                             double* __restrict__ rT,
+                                                             double* __restrict__ rS) {
+    __shared__ double sfx[2][2][TRY][TRX + 1];  // [buffer][field][row][west face of column]
+    __shared__ double sfy[2][2][TRY + 1][TRX];  // [buffer][field][south face of row][column]
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i0 = blockIdx.x * TRX, j0 = blockIdx.y * TRY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const size_t n2 = P.n2;
+    const bool live = i < nx && j < ny;
+    const bool ts = P.tracers_ts;
+    const int nf = ts ? 2 : 1;
+    const bool adv = P.advection != 0;
+    const int kbeg = blockIdx.z * TR_KL;
+    const int kend = kbeg + TR_KL < nz ? kbeg + TR_KL : nz;
+    // faces this thread forms: the west and south faces of its cell, and for two
+    // warps the east faces of the tile's last column / north faces of its last row
+    const bool xextra = ty == TRY - 2 && tx < TRY, yextra = ty == TRY - 1;
+    const int c = wrapi(j, ny) * nx + wrapi(i, nx);
+    const ColGeo g = ColGeo::load(P, c);
+    const double* __restrict__ C0 = ts ? T : bold;
+    double* __restrict__ R0 = rT;
+    // rolling column values of each field at k-1, k, k+1 and the face at the top of level k
+    double fm1[2] = {0.0, 0.0}, f0[2] = {0.0, 0.0}, fp1[2] = {0.0, 0.0}, ftop[2] = {0.0, 0.0};
+    double w_k = 0.0, kh_k = 0.0;
+    if (live) {
+#pragma unroll
+        for (int f = 0; f < 2; ++f) {
+            if (f >= nf) break;
+            const double* __restrict__ C = f == 0 ? C0 : S;
+            const double fm2 = kbeg >= 2 ? C[(size_t)(kbeg - 2) * n2 + c] : 0.0;
+            fm1[f] = kbeg >= 1 ? C[(size_t)(kbeg - 1) * n2 + c] : 0.0;
+            f0[f] = C[(size_t)kbeg * n2 + c];
+            fp1[f] = kbeg + 1 < nz ? C[(size_t)(kbeg + 1) * n2 + c] : 0.0;
+            if (adv) ftop[f] = tracer_vface(P, g, kbeg, fm2, fm1[f], f0[f], fp1[f], w[(size_t)kbeg * n2 + c]);
         }
+        w_k = w[(size_t)kbeg * n2 + c];
+        kh_k = kh[(size_t)kbeg * n2 + c];
     }
-    const double vdiv = (w[o + nb.c] * cf[0] - w[o + n2 + nb.c] * cf[1]) * inv;
-    return (hdiv + vdiv) * m3c;
-}
-
-// right-hand side of the implicit tracer solve at level k (model3d_v05.py:466-479)
-__device__ __forceinline__ double tracer_rhs(const KP& P, const Nbr& nb, const double* __restrict__ C,
-                                             const double* __restrict__ u,
-                                             const double* __restrict__ v,
-                                             const double* __restrict__ w,
-                                             const double* __restrict__ kh, int k, double dzk,
-                                             double m3k, double dz_m1, double dz_p1, double m3_m1,
-                                             double m3_p1, double surf, double source) {
-    const size_t n2 = P.n2;
-    const size_t o = (size_t)k * n2 + nb.c;
-    const int nz = P.nz;
-    double tend = source;
-    if (P.advection != 0) tend = tend - tracer_adv(P, nb, C, u, v, w, k, dzk, m3k);
-    if (P.k_h > 0.0) tend = tend + P.k_h * hlap(P, nb, C, k, 2);
-    // explicit vertical diffusion with zero drag (vertical_var.py:80-106)
-    const double ck = C[o];
-    const double ckm = (k > 0) ? C[o - n2] : 0.0;
-    const double ckp = (k + 1 < nz) ? C[o + n2] : 0.0;
-    const double bottom_m1 = (k > 0 && m3_m1 > 0.0 && m3k == 0.0) ? 1.0 : 0.0;
-    const double bottom_k = (m3k > 0.0 && m3_p1 == 0.0) ? 1.0 : 0.0;
-    const double diff = explicit_dz(P, k, ckm, ck, ckp, kh[o], kh[o + n2], dz_m1, dzk, dz_p1,
-                                    bottom_m1, bottom_k, m3k, surf, 0.0);
-    double rhs = ck + P.dt * tend + P.c3 * diff;
-    if (k == 0) rhs = rhs + P.thv_dt * surf * inv_pos(dzk);
-    return rhs;
-}
-
-// One thread per cell: the right-hand sides of the implicit tracer solves.
-__global__ void __launch_bounds__(256, 4) k_tracer_rhs(KP P, const double* __restrict__ T,
-                                                    const double* __restrict__ S,
-                                                    const double* __restrict__ bold,
-                                                    const double* __restrict__ u,
-                                                    const double* __restrict__ v,
-                                                    const double* __restrict__ w,
-                                                    const double* __restrict__ kh,
-                                                    double* __restrict__ rT, double* __restrict__ rS) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
-    if (i >= P.nx || j >= P.ny) return;
-    Nbr nb;
-    nb.init(i, j, P.nx, P.ny);
-    const int nz = P.nz;
-    const size_t n2 = (size_t)P.n2;
-    const size_t o = (size_t)k * n2 + nb.c;
-    double m3k, m3_m1 = 0.0, m3_p1 = 0.0;
-    const double dzk = col_dz(P, nb.c, k, m3k);
-    const double dz_m1 = (k > 0) ? col_dz(P, nb.c, k - 1, m3_m1) : 0.0;
-    const double dz_p1 = (k + 1 < nz) ? col_dz(P, nb.c, k + 1, m3_p1) : 0.0;
-    if (P.tracers_ts) {
-        rT[o] = tracer_rhs(P, nb, T, u, v, w, kh, k, dzk, m3k, dz_m1, dz_p1, m3_m1, m3_p1, P.flux_t, 0.0);
-        rS[o] = tracer_rhs(P, nb, S, u, v, w, kh, k, dzk, m3k, dz_m1, dz_p1, m3_m1, m3_p1, P.flux_s, 0.0);
-    } else {
-        const double src = P.neg_n2 * (0.5 * (w[o] + w[o + n2]));
-        rT[o] = tracer_rhs(P, nb, bold, u, v, w, kh, k, dzk, m3k, dz_m1, dz_p1, m3_m1, m3_p1, 0.0, src);
+    for (int k = kbeg; k < kend; ++k) {
+        const int buf = (k - kbeg) & 1;
+        const size_t o = (size_t)k * n2;
+        if (adv) {
+#pragma unroll 1
+            for (int f = 0; f < nf; ++f) {
+                const double* __restrict__ C = f == 0 ? C0 : S;
+                sfx[buf][f][ty][tx] = tracer_flux(P, C, u, o, xstencil(j, i - 1, nx, ny), k, 0);
+                sfy[buf][f][ty][tx] = tracer_flux(P, C, v, o, ystencil(j - 1, i, nx, ny), k, 1);
+                if (xextra) sfx[buf][f][tx][TRX] = tracer_flux(P, C, u, o, xstencil(j0 + tx, i0 + TRX - 1, nx, ny), k, 0);
+                if (yextra) sfy[buf][f][TRY][tx] = tracer_flux(P, C, v, o, ystencil(j0 + TRY - 1, i, nx, ny), k, 1);
+            }
+            __syncthreads();
+        }
+        if (!live) continue;
+        double m3k, m3_m1 = 0.0, m3_p1 = 0.0;
+        const double dzk = g.dz(P, k, m3k);
+        const double dz_m1 = (k > 0) ? g.dz(P, k - 1, m3_m1) : 0.0;
+        const double dz_p1 = (k + 1 < nz) ? g.dz(P, k + 1, m3_p1) : 0.0;
+        const double bottom_m1 = (k > 0 && m3_m1 > 0.0 && m3k == 0.0) ? 1.0 : 0.0;
+        const double bottom_k = (m3k > 0.0 && m3_p1 == 0.0) ? 1.0 : 0.0;
+        const double w_k1 = w[o + n2 + c];
+        const double kh_k1 = kh[o + n2 + c];
+        const double inv = inv_pos(dzk);
+#pragma unroll
+        for (int f = 0; f < 2; ++f) {
+            if (f >= nf) break;
+            const double* __restrict__ C = f == 0 ? C0 : S;
+            const double fp2 = (k + 2 < nz) ? C[o + 2 * n2 + c] : 0.0;
+            const double surf = ts ? (f == 0 ? P.flux_t : P.flux_s) : 0.0;
+            double tend = ts ? 0.0 : P.neg_n2 * (0.5 * (w_k + w_k1));
+            double fbot = 0.0;
+            if (adv) {
+                fbot = tracer_vface(P, g, k + 1, fm1[f], f0[f], fp1[f], fp2, w_k1);
+                const double hdiv = ((sfx[buf][f][ty][tx + 1] - sfx[buf][f][ty][tx]) / P.dx +
+                                     (sfy[buf][f][ty + 1][tx] - sfy[buf][f][ty][tx]) / P.dy) *
+                                    inv;
+                const double vdiv = (w_k * ftop[f] - w_k1 * fbot) * inv;
+                tend = tend - (hdiv + vdiv) * m3k;
+            }
+            if (P.k_h > 0.0) {
+                Nbr nb;
+                nb.init(wrapi(i, nx), wrapi(j, ny), nx, ny);
+                tend = tend + P.k_h * hlap(P, nb, C, k, 2);
+            }
+            // explicit vertical diffusion with zero drag (vertical_var.py:80-106)
+            const double diff = explicit_dz(P, k, k > 0 ? fm1[f] : 0.0, f0[f], k + 1 < nz ? fp1[f] : 0.0, kh_k,
+                                            kh_k1, dz_m1, dzk, dz_p1, bottom_m1, bottom_k, m3k, surf, 0.0);
+            double rhs = f0[f] + P.dt * tend + P.c3 * diff;
+            if (k == 0) rhs = rhs + P.thv_dt * surf * inv_pos(dzk);
+            (f == 0 ? R0 : rS)[o + c] = rhs;
+            ftop[f] = fbot;
+            fm1[f] = f0[f];
+            f0[f] = fp1[f];
+            fp1[f] = fp2;
+        }
+        w_k = w_k1;
+        kh_k = kh_k1;
     }
 }
 
@@ -1430,7 +1483,8 @@ void launch_backsub(const KP& P, const double* ghu, const double* ghv, const dou
 void launch_tracer_rhs(const KP& P, const double* T, const double* S, const double* bold,
                        const double* u, const double* v, const double* w, const double* kh, double* rT,
                        double* rS, cudaStream_t s) {
-    k_tracer_rhs<<<cell_grid(P), cell_block(), 0, s>>>(P, T, S, bold, u, v, w, kh, rT, rS);
+    const dim3 grid((P.nx + TRX - 1) / TRX, (P.ny + TRY - 1) / TRY, (P.nz + TR_KL - 1) / TR_KL);
+    k_tracer_rhs<<<grid, dim3(TRX, TRY), 0, s>>>(P, T, S, bold, u, v, w, kh, rT, rS);
 }
 
 void launch_tracer_solve(const KP& P, const double* rT, const double* rS, const double* kh,

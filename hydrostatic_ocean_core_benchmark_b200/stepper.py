@@ -124,6 +124,26 @@ class OceanStepper:
                                      self._shapes(), writable=False)
         self._call("oc_set_state", self.lib.oc_set_state, self.h, C.byref(view), dev)
 
+    def set_state_async(self, stream, eta, u, v, b=None, T=None, S=None, e=None, km=None, kh=None):
+        """Enqueue the state copies on `stream` without waiting (oc_set_state_async).
+        Inputs must be contiguous float64 tensors (pinned host or CUDA) or C-contiguous
+        float64 arrays that stay alive and unchanged until the stream passes the copies."""
+        arrays = dict(eta=eta, u=u, v=v, b=b, T=T, S=S, e=e, km=km, kh=kh)
+        for name, a in arrays.items():
+            if a is not None and not _is_tensor(a) and not (
+                    isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+                raise ValueError(f"{name}: asynchronous inputs must be contiguous float64")
+        view, dev, keep = self._view(arrays, self._shapes(), writable=False)
+        sp = getattr(stream, "cuda_stream", stream)
+        self._call("oc_set_state_async", self.lib.oc_set_state_async, self.h, C.byref(view), dev, sp)
+
+    def get_state_async(self, stream, out: dict):
+        """Enqueue the copies of the current state into ``out`` on `stream` without
+        waiting (oc_get_state_async); ``out`` is complete once the stream passes them."""
+        view, dev, keep = self._view(out, self._shapes(), writable=True)
+        sp = getattr(stream, "cuda_stream", stream)
+        self._call("oc_get_state_async", self.lib.oc_get_state_async, self.h, C.byref(view), dev, sp)
+
     def reset_mixing(self):
         self._call("oc_reset_mixing", self.lib.oc_reset_mixing, self.h)
 

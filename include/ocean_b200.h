@@ -135,12 +135,25 @@ int oc_set_forcing(oc_handle* h, const double* taux_c, const double* tauy_c);
 /* Copy a state in (on_device = 0: host pointers, 1: device pointers). */
 int oc_set_state(oc_handle* h, const oc_state_view* s, int32_t on_device);
 
+/* The same, enqueued on `stream` (cudaStream_t; NULL = legacy default stream)
+ * without waiting: the source buffers must stay unchanged until the stream has
+ * passed the copies, and host buffers must be pinned for the copies to overlap
+ * other work. A following oc_step on the same stream sees the state. No
+ * reference counterpart: the reference steps host arrays synchronously. */
+int oc_set_state_async(oc_handle* h, const oc_state_view* s, int32_t on_device, void* stream);
+
 /* Restore the constant viscosity nu and diffusivity kappa of the
  * configuration (the stepper's state at construction). */
 int oc_reset_mixing(oc_handle* h);
 
 /* Copy the current state out (host or device pointers). Synchronises the stream. */
 int oc_get_state(oc_handle* h, const oc_state_view* s, int32_t on_device);
+
+/* The same, enqueued on `stream` after the work already on it, without
+ * waiting; the destination is complete once the stream has passed the copies.
+ * A device-side error of the steps before it is reported by the next
+ * synchronous call (oc_get_state, oc_get_stats). No reference counterpart. */
+int oc_get_state_async(oc_handle* h, const oc_state_view* s, int32_t on_device, void* stream);
 
 /* Advance n_steps on `stream` (a cudaStream_t, or NULL for the legacy default stream).
  * Asynchronous: returns once the work is enqueued. */

@@ -129,3 +129,52 @@ def test_multigrid_paths_match_oracle(nx, ny):
         assert its == itr
         assert np.array_equal(x, xr)
     st.close()
+
+
+def test_async_state_round_trip_matches_synchronous():
+    """oc_set_state_async / oc_step / oc_get_state_async on user streams (pinned host
+    buffers, two handles alternating as in the end-to-end bench) give the bits of the
+    synchronous set_state / step / get_state path."""
+    import torch
+    from hydrostatic_ocean_core_benchmark_b200 import cases
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    s = cases.seamount_basin(nx=48, ny=40, nz=10, seed=7)
+    p = s.params
+    fields = ("eta", "u", "v", "b", "T", "S", "e")
+    ref = OceanStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    ref.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
+    start = ref.get_state()
+    cur = {k: start[k] for k in fields}
+    for _ in range(3):
+        ref.set_state(**cur)
+        ref.step(1)
+        cur = {k: v for k, v in ref.get_state().items() if k in fields}
+    members = [OceanStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c) for _ in range(2)]
+    for m in members:
+        m.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
+    bufs = [{k: torch.from_numpy(np.ascontiguousarray(start[k])).pin_memory() for k in fields}
+            for _ in range(2)]
+    s_in, s_cmp, s_out = (torch.cuda.Stream() for _ in range(3))
+    ev_out = [None, None]
+    for n in range(6):  # each member does three round trips, interleaved
+        m = n % 2
+        if ev_out[m] is not None:
+            s_in.wait_event(ev_out[m])
+        members[m].set_state_async(s_in, **bufs[m])
+        e = torch.cuda.Event()
+        e.record(s_in)
+        s_cmp.wait_event(e)
+        members[m].step(1, stream=s_cmp)
+        e = torch.cuda.Event()
+        e.record(s_cmp)
+        s_out.wait_event(e)
+        members[m].get_state_async(s_out, bufs[m])
+        ev_out[m] = torch.cuda.Event()
+        ev_out[m].record(s_out)
+    torch.cuda.synchronize()
+    for m in range(2):
+        for k in fields:
+            assert np.array_equal(bufs[m][k].numpy().reshape(cur[k].shape), cur[k]), (m, k)
+        assert members[m].stats()["solver_failures"] == 0
+    for st in [ref, *members]:
+        st.close()
