@@ -72,6 +72,12 @@ class OcStats(C.Structure):
     ]
 
 
+class OcHelmConfig(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("dx", C.c_double), ("dy", C.c_double),
+                ("coef", C.c_double), ("solver", C.c_int32), ("rtol", C.c_double),
+                ("max_iter", C.c_int32), ("device", C.c_int32)]
+
+
 class OcKernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("total_ms", C.c_double)]
 
@@ -101,6 +107,14 @@ _SIGNATURES = {
                                     C.c_int32, C.c_int32, C.c_void_p]),
     "oc_buoyancy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                               C.c_int64, C.c_void_p]),
+    "oc_helm_create": (C.c_int, [C.POINTER(OcHelmConfig), C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.POINTER(C.c_void_p)]),
+    "oc_helm_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
+                                C.POINTER(C.c_int32), C.c_void_p]),
+    "oc_helm_last_error": (C.c_char_p, [C.c_void_p]),
+    "oc_helm_destroy": (C.c_int, [C.c_void_p]),
+    "oc_density": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "oc_get_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),
     "oc_run_namelist": (C.c_int, [C.c_char_p]),
     "oc_last_error": (C.c_char_p, [C.c_void_p]),

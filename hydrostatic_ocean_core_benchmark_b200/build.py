@@ -21,7 +21,10 @@ LIB_DIR = PKG / "lib"
 BIN_DIR = PKG / "bin"
 LIB = LIB_DIR / "libocean_b200.so"
 EXE = BIN_DIR / "ocean3d5_b200"
-SOURCES = ["step_kernels.cu", "helmholtz.cu", "capi.cu", "thomas_noalloc.cu", "protocol.cpp"]
+# executables over the C ABI: (main source, binary)
+MAINS = [("ocean3d5_main.cpp", EXE), ("helmholtz_bench_main.cpp", BIN_DIR / "helmholtz_bench_b200"),
+         ("eos_bench_main.cpp", BIN_DIR / "eos_bench_b200")]
+SOURCES = ["step_kernels.cu", "helmholtz.cu", "capi.cu", "thomas_noalloc.cu", "standalone.cu", "protocol.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--extended-lambda",
          "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{ROOT / 'include'}", f"-I{CSRC}"]
@@ -42,9 +45,9 @@ def _stale(target: Path, deps: list[Path]) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
-    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "ocean_b200.h",
-                                                                      CSRC / "ocean3d5_main.cpp"]
-    if not force and not _stale(LIB, deps) and not _stale(EXE, deps):
+    deps = ([CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "ocean_b200.h"]
+            + [CSRC / m for m, _ in MAINS])
+    if not force and not _stale(LIB, deps) and not any(_stale(exe, deps) for _, exe in MAINS):
         return LIB
     LIB_DIR.mkdir(exist_ok=True)
     BIN_DIR.mkdir(exist_ok=True)
@@ -64,9 +67,9 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     tmp = LIB.with_suffix(".so.tmp")
     subprocess.run([cc, *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)
-    subprocess.run([cc, *FLAGS, "-x", "c++", str(CSRC / "ocean3d5_main.cpp"), "-o", str(EXE),
-                    f"-L{LIB_DIR}", "-locean_b200", "-Xlinker", "-rpath,$ORIGIN/../lib", "-lcudart"],
-                   check=True)
+    for main, exe in MAINS:
+        subprocess.run([cc, *FLAGS, "-x", "c++", str(CSRC / main), "-o", str(exe), f"-L{LIB_DIR}",
+                        "-locean_b200", "-Xlinker", "-rpath,$ORIGIN/../lib", "-lcudart"], check=True)
     return LIB
 
 

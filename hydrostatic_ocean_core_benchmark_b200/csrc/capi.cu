@@ -671,7 +671,7 @@ int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const dou
     if (h->cfg.scheme == OC_SCHEME_THETA) {
         h->solver = new HelmSolver();
         const double coef = h->cfg.g * std::pow(h->cfg.theta, 2.0) * std::pow(h->cfg.dt, 2.0);
-        rc = h->solver->init(nx, ny, h->cfg.lx, h->cfg.ly, coef, h->cfg.solver, h->cfg.rtol,
+        rc = h->solver->init(nx, ny, h->cfg.lx / nx, h->cfg.ly / ny, coef, h->cfg.solver, h->cfg.rtol,
                              h->cfg.max_iter, h->mask.data(), h->Ku, h->Kv, 4096, h->d_status, h->err);
         if (rc) return rc;
     }

@@ -797,7 +797,7 @@ HelmSolver::~HelmSolver() {
     for (void* p : allocs_) cudaFree(p);
 }
 
-int HelmSolver::init(int nx, int ny, double lx, double ly, double coef, int kind, double rtol,
+int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int kind, double rtol,
                      int max_iter, const double* mask_host, double* Ku, double* Kv, int log_cap,
                      int* status, std::string& err) {
     HelmParams& H = hp_;
@@ -836,7 +836,9 @@ int HelmSolver::init(int nx, int ny, double lx, double ly, double coef, int kind
         L.nx = dims[l].first;
         L.ny = dims[l].second;
         L.n = L.nx * L.ny;
-        const double dx = lx / L.nx, dy = ly / L.ny;
+        // coarse level l spans the same length with nx / 2^l cells: Lx / (nx / 2^l)
+        // is exactly (Lx / nx) * 2^l, the reference's CGrid spacing of that level
+        const double dx = std::ldexp(dx0, l), dy = std::ldexp(dy0, l);
         L.dx2 = std::pow(dx, 2.0);
         L.dy2 = std::pow(dy, 2.0);
         L.cx = coef * (1.0 / std::pow(dx, 2.0));

@@ -50,8 +50,9 @@ struct HelmParams {
 class HelmSolver {
    public:
     ~HelmSolver();
-    // Ku/Kv/mask are device arrays of the fine level owned by the caller.
-    int init(int nx, int ny, double lx, double ly, double coef, int kind, double rtol, int max_iter,
+    // Ku/Kv are device arrays of the fine level owned by the caller, mask a host
+    // array; dx, dy the fine-level spacing.
+    int init(int nx, int ny, double dx, double dy, double coef, int kind, double rtol, int max_iter,
              const double* mask_host, double* Ku, double* Kv, int log_cap, int* status,
              std::string& err);
     // recompute coarse coefficients and inverse diagonals after Ku/Kv changed

@@ -263,15 +263,22 @@ __device__ __forceinline__ double rho_teos10(double CT, double SA, double z) {
     return ((rz3 * zh + rz2) * zh + rz1) * zh + rz0 + r0;
 }
 
-__device__ __forceinline__ double rho_anomaly(const KP& P, double T, double S, double z) {
-    if (P.eos == 0) return P.rho0 * (-P.alpha_t * (T - P.t0) + P.beta_s * (S - P.s0));
-    if (P.eos == 1) {
+// density anomaly rho' (eos.py:103-127): linear with the given constants, the
+// simplified EOS, or polyTEOS10-bsq about rho0
+__device__ __forceinline__ double rho_anomaly_of(int eos, double rho0, double alpha_t, double beta_s,
+                                                 double t0, double s0, double T, double S, double z) {
+    if (eos == 0) return rho0 * (-alpha_t * (T - t0) + beta_s * (S - s0));
+    if (eos == 1) {
         const double Ta = T - 10.0, Sa = S - 35.0;
         return (-1.6550e-1 * (1.0 + (0.5 * 5.9520e-2) * Ta + 1.4970e-4 * z) * Ta
                 + 7.6554e-1 * (1.0 - (0.5 * 7.4914e-4) * Sa - 1.1090e-5 * z) * Sa
                 - 2.4341e-3 * Ta * Sa);
     }
-    return rho_teos10(T, S, z) - P.rho0;
+    return rho_teos10(T, S, z) - rho0;
+}
+
+__device__ __forceinline__ double rho_anomaly(const KP& P, double T, double S, double z) {
+    return rho_anomaly_of(P.eos, P.rho0, P.alpha_t, P.beta_s, P.t0, P.s0, T, S, z);
 }
 
 __device__ __forceinline__ double buoyancy_of(const KP& P, double T, double S, double z) {

@@ -203,6 +203,42 @@ int oc_thomas_noalloc(const double* sub, const double* diag, const double* sup, 
 int oc_buoyancy(oc_handle* h, const double* T, const double* S, const double* z, double* b,
                 int64_t count, void* stream);
 
+/* ---- Standalone kernels (the reference's standalone benches) --------------
+ *
+ * A Helmholtz solver on given depth-integrated face coefficients, replacing
+ * the solver of the reference's standalone bench (libs/cuda/src/
+ * helmholtz_bench.cu) on the system tools/write_helmholtz_case.py writes:
+ * A = I - coef D[K G .] on an nx x ny periodic-index grid with spacings dx,
+ * dy, solved by HelmholtzVar's four methods (libs/core/solvers_var.py:162-197).
+ * It is the step's own solver, so the iteration counts equal NumPy's. */
+typedef struct oc_helm oc_helm;
+typedef struct oc_helm_config {
+    int32_t nx, ny;
+    double dx, dy;     /* fine-grid spacing [m]; level l uses dx * 2^l */
+    double coef;       /* g theta^2 dt^2 */
+    int32_t solver;    /* OC_SOLVER_* */
+    double rtol;
+    int32_t max_iter;
+    int32_t device;
+} oc_helm_config;
+
+/* ku, kv, mask: host fp64 [ny][nx] (ku.bin, kv.bin, mask.bin of a case). */
+int oc_helm_create(const oc_helm_config* cfg, const double* ku, const double* kv, const double* mask,
+                   oc_helm** out);
+/* x = A^-1 rhs (on_device = 0: host arrays, 1: device arrays), synchronising;
+ * *iterations and *converged as HelmholtzVar's SolveReport. */
+int oc_helm_solve(oc_helm* h, const double* rhs, double* x, int32_t on_device, int32_t* iterations,
+                  int32_t* converged, void* stream);
+const char* oc_helm_last_error(oc_helm* h);
+int oc_helm_destroy(oc_helm* h);
+
+/* The reference EOS bench's per-cell quantity (libs/cuda/src/eos_bench.cu over
+ * libs/core/eos.py:68-127) on device buffers of `count` cells: rho' for
+ * OC_EOS_LINEAR (with rho0, alpha_t, beta_s, t0, s0) and OC_EOS_SEOS, the full
+ * in-situ density rho for OC_EOS_TEOS10. Asynchronous on `stream`. */
+int oc_density(int32_t eos, double rho0, double alpha_t, double beta_s, double t0, double s0,
+               const double* T, const double* S, const double* z, double* rho, int64_t count, void* stream);
+
 /* Copy a static geometry or coefficient field to host memory: names "dz3",
  * "mask3", "mask3u", "mask3v", "dz3u", "dz3v", "zc" ([nz][ny][nx]), "q"
  * ([nz][ny][nx]), "ku", "kv", "mask_u", "mask_v" ([ny][nx]). */
