@@ -3,16 +3,20 @@
 
 Workload: the seeded seamount basin (512 x 512 x 50 cells, 2000 km square,
 closed, stretched levels 10 -> 250 m, double-gyre wind, TKE closure, TVD3
-advection, polyTEOS10 EOS, theta = 0.5 with the multigrid Helmholtz solver,
+advection, polyTEOS10 EOS, theta = 0.6 with the multigrid Helmholtz solver,
 dt = 600 s). A "step" is one model time step over the whole grid.
 
 Prints one JSON line. ``value`` is cell-steps/s of the device-resident state
-(all ranks, max-over-ranks device time); ``e2e`` is the same metric through the
-C-ABI with host buffers (pinned-host -> device state upload, the step, device
--> pinned-host download, every step); ``roofline`` is the dominant kernel's
-algorithmic bandwidth against the measured HBM peak; ``cpu_baseline`` times the
-CPU oracle (a NumPy port, bit-identical to the reference's NumPy stepper) on a
-bounded sample of the same recipe.
+(all ranks, max-over-ranks device time, CUDA events on the launching stream,
+the steps replayed as recorded two-step CUDA graphs). ``kernels`` and
+``roofline`` come from a second timed region of plain launches with CUDA
+events around every launch: the dominant kernel's algorithmic bandwidth
+against the measured HBM peak. ``e2e`` is the same metric through the C ABI
+with pinned host buffers: every step uploads a full state, steps it and
+downloads it, three independent states taking turns so that copies overlap
+steps (``e2e.sequential``: one state, every copy waiting). ``cpu_baseline``
+times the CPU oracle (a NumPy port, bit-identical to the reference's NumPy
+stepper) on a bounded sample of the same recipe.
 
 Multi-GPU: replicas only (the theta step does not shard); each rank advances
 its own replica, ``scaling`` is "weak".
@@ -272,36 +276,52 @@ def run_ours(args, rank, world, local_rank):
                       device=local_rank)
     st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
     stream = torch.cuda.Stream(device=local_rank)
-    # warm-up
-    st.step(args.warmup, stream=stream)
+    graph = not args.no_graph
+    # warm-up; with graphs, two more steps record the graph of the buffer the
+    # timed region starts from, so no recording happens inside it
+    st.step(args.warmup, stream=stream, graph=graph)
+    if graph:
+        st.step(2, stream=stream, graph=True)
     stream.synchronize()
     st.stats()
     log0 = len(st.solve_log())
     launches0 = st.stats()["kernel_launches"]
-    st.kernel_times()
-    # timed region: device-resident state, events on the launching stream
+    # timed region: device-resident state, events on the launching stream; the
+    # steps replay the recorded two-step CUDA graphs (oc_step_graph)
     out_dir = ROOT / "gpurun_out"
     clocks = ClockSampler(local_rank, out_dir / f"clocks_rank{rank}.csv" if out_dir.is_dir() else None)
     clocks.start()
-    st.set_profiling(True)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
     ev0.record(stream)
-    st.step(args.steps, stream=stream)
+    st.step(args.steps, stream=stream, graph=graph)
     ev1.record(stream)
     ev1.synchronize()
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
-    st.set_profiling(False)
     ms = ev0.elapsed_time(ev1)
     ms_max = max_over_ranks(ms)
+    launches = st.stats()["kernel_launches"] - launches0
+    # per-kernel timed region: the same steps launched one by one with CUDA events
+    # around every launch on the launching stream (oc_set_profiling); these give
+    # the kernel shares and the roofline's per-launch durations
+    st.kernel_times()
+    st.set_profiling(True)
+    pv0 = torch.cuda.Event(enable_timing=True)
+    pv1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    pv0.record(stream)
+    st.step(args.profile_steps, stream=stream)
+    pv1.record(stream)
+    pv1.synchronize()
+    st.set_profiling(False)
+    ms_prof = max_over_ranks(pv0.elapsed_time(pv1))
     ktimes = st.kernel_times()
     stats = st.stats()
     log = st.solve_log()[log0:]
-    launches = stats["kernel_launches"] - launches0
     if stats["solver_failures"] or stats["diverged"]:
         raise RuntimeError(f"the timed run failed: {stats}")
     value = world * n3 * args.steps / (ms_max / 1e3)
@@ -408,7 +428,7 @@ def run_ours(args, rank, world, local_rank):
     roofline = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_ms}
-    iters_per_step = sum(log) / args.steps
+    iters_per_step = sum(log) / (args.steps + args.profile_steps)  # both timed regions
     bstep = step_algorithmic_bytes(p, iters_per_step)
     step_gbs = bstep / (ms / args.steps / 1e3) / 1e9
     kernel_share = {k: {"launches": v[0], "ms": v[1], "share": v[1] / max(1e-12, sum(x[1] for x in ktimes.values()))}
@@ -440,8 +460,11 @@ def run_ours(args, rank, world, local_rank):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
+            "launch_mode": "two-step CUDA graphs (oc_step_graph)" if graph else "one launch per kernel",
             "clocks": clk,
             "kernels": kernel_share,
+            "kernels_region": {"steps": args.profile_steps, "ms_per_step": ms_prof / args.profile_steps,
+                               "note": "per-kernel CUDA events around every launch (plain launches)"},
             "solver_iterations_per_solve": iters_per_solve,
         }
         print(json.dumps(line), flush=True)
@@ -462,6 +485,9 @@ def main():
     ap.add_argument("--nz", type=int, default=50)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--e2e-steps", type=int, default=12)
+    ap.add_argument("--profile-steps", type=int, default=20,
+                    help="steps of the per-kernel event region (kernel shares, roofline)")
+    ap.add_argument("--no-graph", action="store_true", help="launch the timed steps one by one")
     ap.add_argument("--e2e-members", type=int, default=3,
                     help="independent states round-tripped through the host in turn (overlap)")
     ap.add_argument("--cpu-steps", type=int, default=2)

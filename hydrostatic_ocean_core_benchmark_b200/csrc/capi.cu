@@ -96,6 +96,14 @@ struct oc_handle {
     std::vector<std::string> prof_names;
     std::vector<long long> prof_launches;
     std::vector<double> prof_ms;
+    // CUDA graphs of two steps (one period of the ping-pong buffers), one per
+    // starting buffer, and the counter increments one launch stands for
+    struct Counters {
+        long long steps, tridiag, rebuilds, substeps, solves, launches;
+    };
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    Counters graph_delta[2] = {};
+    cudaStream_t capture_stream = nullptr;
 };
 
 namespace {
@@ -417,7 +425,7 @@ int step_once(oc_handle* h, cudaStream_t s) {
         h->tridiag += 2;
         if (theta) {
             { Prof pr(h, s, "helm_rhs"); launch_helm_rhs(P, eta, h->div_old, h->Ug, h->Vg, h->rhs2, s); }
-            int rc = ensure_log(h, h->solves + 1, s);
+            int rc = ensure_log(h, h->solves + 1, s);  // graphs reserve the log before recording
             if (rc) return rc;
             {
                 Prof pr(h, s, "helm_solve");
@@ -487,6 +495,53 @@ int step_once(oc_handle* h, cudaStream_t s) {
     h->cur = nxt;
     h->steps += 1;
     return check_launch(h, "step");
+}
+
+void drop_graphs(oc_handle* h) {
+    for (auto& g : h->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// Record two steps from the current buffers into a graph. Nothing runs: the
+// host state the recording advanced (buffer index, counters) is put back and
+// the counters one launch stands for are kept.
+int capture_graph(oc_handle* h) {
+    if (!h->capture_stream && cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(h, OC_ERR_CUDA, "cudaStreamCreate failed");
+    const int cur = h->cur;
+    const oc_handle::Counters before{h->steps, h->tridiag, h->rebuilds, h->substeps, h->solves, h->launches};
+    const bool prof = h->profiling;
+    h->profiling = false;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->capture_stream, cudaStreamCaptureModeThreadLocal);
+    int rc = e == cudaSuccess ? OC_OK : cuda_fail(h, e, "graph capture begin");
+    for (int n = 0; n < 2 && rc == OC_OK; ++n) rc = step_once(h, h->capture_stream);
+    e = cudaStreamEndCapture(h->capture_stream, &g);
+    h->profiling = prof;
+    const oc_handle::Counters after{h->steps, h->tridiag, h->rebuilds, h->substeps, h->solves, h->launches};
+    h->cur = cur;
+    h->steps = before.steps;
+    h->tridiag = before.tridiag;
+    h->rebuilds = before.rebuilds;
+    h->substeps = before.substeps;
+    h->solves = before.solves;
+    h->launches = before.launches;
+    if (rc == OC_OK && e != cudaSuccess) rc = cuda_fail(h, e, "graph capture (a step call cannot be recorded)");
+    if (rc == OC_OK && cudaGraphInstantiate(&h->graph[cur], g, 0) != cudaSuccess)
+        rc = fail(h, OC_ERR_CUDA, "graph instantiation failed");
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    if (rc) {
+        h->graph[cur] = nullptr;
+        return rc;
+    }
+    h->graph_delta[cur] = {after.steps - before.steps, after.tridiag - before.tridiag, after.rebuilds - before.rebuilds,
+                           after.substeps - before.substeps, after.solves - before.solves,
+                           after.launches - before.launches};
+    return OC_OK;
 }
 
 }  // namespace
@@ -685,6 +740,7 @@ int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const dou
 
 int oc_set_forcing(oc_handle* h, const double* taux_c, const double* tauy_c) {
     if (!h) return OC_ERR_ARG;
+    drop_graphs(h);
     if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain before the forcing");
     cudaSetDevice(h->cfg.device);
     if (!taux_c && !tauy_c) {
@@ -826,6 +882,49 @@ int oc_step(oc_handle* h, int32_t n_steps, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     h->last_stream = s;
     for (int n = 0; n < n_steps; ++n) {
+        const int rc = step_once(h, s);
+        if (rc) return rc;
+    }
+    return OC_OK;
+}
+
+int oc_step_graph(oc_handle* h, int32_t n_steps, void* stream) {
+    if (!h) return OC_ERR_ARG;
+    if (!h->has_state) return fail(h, OC_ERR_STATE, "set the state before stepping");
+    if (n_steps < 0) return fail(h, OC_ERR_ARG, "n_steps must be >= 0");
+    cudaSetDevice(h->cfg.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    h->last_stream = s;
+    if (h->profiling) return oc_step(h, n_steps, stream);  // per-kernel events need the launches one by one
+    const int pairs = n_steps / 2;
+    if (pairs > 0) {
+        // the solve log must hold every solve of the launches without moving:
+        // reserve it (and record again if it had to grow)
+        const long long per_pair = h->solver ? 2LL * h->cfg.n_picard : 0;
+        const long long need = h->solves + per_pair * pairs + per_pair;
+        if (h->solver && need > h->solver->log_capacity()) {
+            const int rc = ensure_log(h, 2 * need, s);
+            if (rc) return rc;
+            drop_graphs(h);
+        }
+        if (!h->graph[h->cur]) {
+            const int rc = capture_graph(h);
+            if (rc) return rc;
+        }
+        const int g = h->cur;
+        const oc_handle::Counters& d = h->graph_delta[g];
+        for (int i = 0; i < pairs; ++i) {
+            const cudaError_t e = cudaGraphLaunch(h->graph[g], s);
+            if (e != cudaSuccess) return cuda_fail(h, e, "graph launch");
+            h->steps += d.steps;
+            h->tridiag += d.tridiag;
+            h->rebuilds += d.rebuilds;
+            h->substeps += d.substeps;
+            h->solves += d.solves;
+            h->launches += d.launches;
+        }
+    }
+    if (n_steps % 2) {
         const int rc = step_once(h, s);
         if (rc) return rc;
     }
@@ -1001,6 +1100,8 @@ void oc_destroy(oc_handle* h) {
     if (!h) return;
     cudaSetDevice(h->cfg.device);
     cudaDeviceSynchronize();
+    drop_graphs(h);
+    if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
     delete h->solver;
     for (void* p : h->allocs) cudaFree(p);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);

@@ -979,9 +979,19 @@ int HelmSolver::solve(const double* rhs, double* x, cudaStream_t s, std::string&
     HelmParams H = hp_;
     H.rhs = rhs;
     H.lv[0].x = x;
-    void* args[] = {&H};
-    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_helm_solve, dim3(grid_),
-                                                      dim3(block_), args, smem_, s);
+    // a cooperative launch (every CTA resident, for the grid barriers) through
+    // the extensible launch API, which stream capture records into a graph
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid_);
+    cfg.blockDim = dim3(block_);
+    cfg.dynamicSmemBytes = smem_;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_helm_solve, H);
     if (e != cudaSuccess) {
         err = std::string("Helmholtz solve launch: ") + cudaGetErrorString(e);
         return OC_ERR_CUDA;

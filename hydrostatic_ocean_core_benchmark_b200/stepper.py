@@ -158,12 +158,16 @@ class OceanStepper:
         self._call("oc_get_state", self.lib.oc_get_state, self.h, C.byref(view), dev)
         return out
 
-    def step(self, n_steps: int = 1, stream=None):
-        """Enqueue n_steps on `stream` (torch.cuda.Stream, raw cudaStream_t int, or None)."""
+    def step(self, n_steps: int = 1, stream=None, graph: bool = False):
+        """Enqueue n_steps on `stream` (torch.cuda.Stream, raw cudaStream_t int, or None);
+        graph=True replays recorded two-step CUDA graphs (oc_step_graph)."""
         sp = None
         if stream is not None:
             sp = getattr(stream, "cuda_stream", stream)
-        self._call("oc_step", self.lib.oc_step, self.h, int(n_steps), sp)
+        if graph:
+            self._call("oc_step_graph", self.lib.oc_step_graph, self.h, int(n_steps), sp)
+        else:
+            self._call("oc_step", self.lib.oc_step, self.h, int(n_steps), sp)
 
     def stats(self) -> dict:
         st = _lib.OcStats()

@@ -159,6 +159,16 @@ int oc_get_state_async(oc_handle* h, const oc_state_view* s, int32_t on_device, 
  * Asynchronous: returns once the work is enqueued. */
 int oc_step(oc_handle* h, int32_t n_steps, void* stream);
 
+/* The same through CUDA graphs: two steps (one period of the state's ping-pong
+ * buffers) are recorded once per starting buffer, on first use, and replayed;
+ * an odd last step runs as oc_step. Results and counters are those of
+ * oc_step. The first call for each buffer records (and must not itself be
+ * inside a stream capture); a grown solve log, new forcing or enabled per-kernel
+ * profiling make it record again or fall back to oc_step. This is the
+ * graph-captured step of the reference's proposed oc_graph_capture /
+ * oc_graph_launch pair, folded into one call. */
+int oc_step_graph(oc_handle* h, int32_t n_steps, void* stream);
+
 /* Wait for the handle's work, then fill the counters (synchronises). */
 int oc_get_stats(oc_handle* h, oc_stats* out);
 

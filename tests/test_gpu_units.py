@@ -178,3 +178,33 @@ def test_async_state_round_trip_matches_synchronous():
         assert members[m].stats()["solver_failures"] == 0
     for st in [ref, *members]:
         st.close()
+
+
+@pytest.mark.parametrize("case", ["seamount_basin_ref_mg", "gate_v06_seamount_tke_split",
+                                  "gate_rough_TS_fb_upwind"])
+def test_graph_steps_match_plain_steps(case):
+    """oc_step_graph (two-step CUDA graphs per starting buffer, an odd last step run
+    plainly) gives the bits, counters and solve log of oc_step."""
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    meta, arrays = load_fixture(case)
+    p, H, mask, dzr, tx, ty, s = case_inputs(meta, arrays)
+    runs = []
+    for graph in (False, True):
+        st = OceanStepper(p, H, mask, dzr=dzr, taux_c=tx, tauy_c=ty)
+        st.set_state(eta=s.eta, u=s.u, v=s.v, b=s.b, T=s.T, S=s.S)
+        st.step(5, graph=graph)   # odd: 2 graph launches + 1 plain step
+        st.step(4, graph=graph)   # starts from the other buffer: records its graph
+        st.set_profiling(True)
+        st.step(2, graph=graph)   # profiling falls back to plain launches
+        st.set_profiling(False)
+        st.step(3, graph=graph)
+        stats = st.stats()
+        runs.append((st.get_state(), stats, st.solve_log()))
+        st.close()
+    (a, sa, la), (b, sb, lb) = runs
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    for k in ("steps", "solver_iterations", "solver_failures", "solver_rebuilds", "tridiagonal_solves",
+              "barotropic_substeps", "solves"):
+        assert sa[k] == sb[k], k
+    assert la == lb
