@@ -31,12 +31,16 @@ namespace oc {
 
 static constexpr long long kBarrierCycles = 2000000000LL;
 static constexpr int kCoarseCells = 1024;
-// fine-level tiles: interior TILE x TILE cells plus a halo of HALO cells, enough
+// fine-level tiles: interior TX x TY cells plus a halo of HALO cells, enough
 // for four red-black half-sweeps and one residual on a shrinking region
-static constexpr int TILE = 32;
 static constexpr int HALO = 5;
-static constexpr int RW = TILE + 2 * HALO;
-static constexpr int RN = RW * RW;
+template <int TX_, int TY_>
+struct TileShape {
+    static constexpr int TX = TX_, TY = TY_;
+    static constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
+};
+using Tile32 = TileShape<32, 32>;    // every grid level by default
+using TileWide = TileShape<128, 16>;  // level 0 of large grids: one tile per CTA, one NumPy leaf per row
 
 // ------------------------------------------------------------------ barrier
 __device__ __forceinline__ bool grid_sync(const HelmParams& H) {
@@ -143,20 +147,44 @@ __device__ void colour_phase(const HLevel& L, double* x, const double* b, int co
 }
 
 // ------------------------------------------------------------------ pairwise sums
+// element e of a warp's leaf values held as r[e / 32] on lane e mod 32, on every
+// lane; e / 32 must be the same on all lanes (the source register is the caller's)
+__device__ __forceinline__ double leaf_pick(const double* r, int e) {
+    const int q = e >> 5;
+    const double x = q == 0 ? r[0] : (q == 1 ? r[1] : (q == 2 ? r[2] : r[3]));
+    return __shfl_sync(0xffffffffu, x, e & 31);
+}
+
+// NumPy's pairwise sum of one leaf (len <= 128 values) that a warp holds as
+// va[q] = element lane + 32 q. The eight interleaved accumulators of NumPy's
+// unrolled loop are formed in their sequential order by lanes j = 0..7
+// (element 8t + j sits on lane (8t + j) mod 32 in register t / 32, the same
+// register on every lane for a given t), folded as
+// ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)), and the len mod 8 remaining elements are
+// added one by one. Every lane returns the sum.
+__device__ __forceinline__ double leaf_sum_warp(const double* va, int len) {
+    const int lane8 = threadIdx.x & 7;
+    const int m = len >= 8 ? len - (len % 8) : 0;
+    double ra = 0.0;
+    if (len >= 8) {
+        ra = leaf_pick(va, lane8);
+        for (int t = 8; t < m; t += 8) ra = ra + leaf_pick(va, t + lane8);
+    }
+    ra = ra + __shfl_xor_sync(0xffffffffu, ra, 1);
+    ra = ra + __shfl_xor_sync(0xffffffffu, ra, 2);
+    ra = ra + __shfl_xor_sync(0xffffffffu, ra, 4);
+    double a = len >= 8 ? __shfl_sync(0xffffffffu, ra, 0) : 0.0;
+    for (int t = m; t < len; ++t) a = a + leaf_pick(va, t);
+    return a;
+}
+
 // Calls f(e) exactly once per element of level 0, grouped by NumPy's leaves;
-// f returns the two values to accumulate. Writes the per-leaf sums.
-//
-// One warp per leaf (a leaf has at most 128 elements), consecutive leaves on
-// different CTAs. Lane l evaluates f for leaf elements l, l+32, l+64, l+96 with
-// independent loads. The eight interleaved accumulators of NumPy's unrolled
-// loop are then formed in their sequential order by lanes j = 0..7 (element
-// 8t + j sits on lane (8t + j) mod 32 in register t / 32 -- the same register on
-// every lane for a given t), folded as ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)), and
-// the len mod 8 remaining elements are added one by one.
+// f returns the two values to accumulate. Writes the per-leaf sums. One warp
+// per leaf, consecutive leaves on different CTAs; lane l evaluates f for leaf
+// elements l, l+32, l+64, l+96 with independent loads.
 template <class F>
 __device__ void leaf_phase(const HelmParams& H, F f, double* outA, double* outB) {
     const int lane = threadIdx.x & 31;
-    const int lane8 = lane & 7;
     const int nwarps = gridDim.x * (blockDim.x >> 5);
     const int my = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // leaf L runs on CTA L mod grid
     for (int L = my; L < H.n_leaves; L += nwarps) {
@@ -171,35 +199,8 @@ __device__ void leaf_phase(const HelmParams& H, F f, double* outA, double* outB)
             va[q] = v.x;
             vb[q] = v.y;
         }
-        // element e of the leaf on every lane; e must be the same on all lanes or
-        // share e / 32 (the source register is chosen by the caller's e)
-        auto pick = [&](const double* r, int e) {
-            const int q = e >> 5;
-            const double x = q == 0 ? r[0] : (q == 1 ? r[1] : (q == 2 ? r[2] : r[3]));
-            return __shfl_sync(0xffffffffu, x, e & 31);
-        };
-        const int m = len >= 8 ? len - (len % 8) : 0;
-        double ra = 0.0, rb = 0.0;
-        if (len >= 8) {
-            ra = pick(va, lane8);
-            rb = pick(vb, lane8);
-            for (int t = 8; t < m; t += 8) {
-                ra = ra + pick(va, t + lane8);
-                rb = rb + pick(vb, t + lane8);
-            }
-        }
-        ra = ra + __shfl_xor_sync(0xffffffffu, ra, 1);
-        rb = rb + __shfl_xor_sync(0xffffffffu, rb, 1);
-        ra = ra + __shfl_xor_sync(0xffffffffu, ra, 2);
-        rb = rb + __shfl_xor_sync(0xffffffffu, rb, 2);
-        ra = ra + __shfl_xor_sync(0xffffffffu, ra, 4);
-        rb = rb + __shfl_xor_sync(0xffffffffu, rb, 4);
-        double a = len >= 8 ? ra : 0.0;
-        double bsum = len >= 8 ? rb : 0.0;
-        for (int t = m; t < len; ++t) {
-            a = a + pick(va, t);
-            bsum = bsum + pick(vb, t);
-        }
+        const double a = leaf_sum_warp(va, len);
+        const double bsum = outB ? leaf_sum_warp(vb, len) : 0.0;
         if (lane == 0) {
             outA[L] = a;
             if (outB) outB[L] = bsum;
@@ -246,24 +247,26 @@ struct TileRefs {
     double *x, *b, *ku, *kv, *id, *m;
 };
 
+template <class S>
 __device__ __forceinline__ TileRefs tile_refs(double* base) {
     TileRefs t;
     t.x = base;
-    t.b = base + RN;
-    t.ku = base + 2 * RN;
-    t.kv = base + 3 * RN;
-    t.id = base + 4 * RN;
-    t.m = base + 5 * RN;
+    t.b = base + S::RN;
+    t.ku = base + 2 * S::RN;
+    t.kv = base + 3 * S::RN;
+    t.id = base + 4 * S::RN;
+    t.m = base + 5 * S::RN;
     return t;
 }
 
 // load a tile region of level L whose interior starts at (i0, j0); x from xin
 // (or zero), plus the coarse correction e * mask when C is given
+template <class S>
 __device__ void tile_load(const HLevel& L, int i0, int j0, const double* xin, const HLevel* C,
                           TileRefs t) {
 #pragma unroll 4
-    for (int r = threadIdx.x; r < RN; r += blockDim.x) {
-        const int rj = r / RW, ri = r - rj * RW;
+    for (int r = threadIdx.x; r < S::RN; r += blockDim.x) {
+        const int rj = r / S::RW, ri = r - rj * S::RW;
         const int gi = wrap_any(i0 - HALO + ri, L.nx), gj = wrap_any(j0 - HALO + rj, L.ny);
         const int g = gj * L.nx + gi;
         const double m = L.mask[g];
@@ -283,10 +286,11 @@ __device__ void tile_load(const HLevel& L, int i0, int j0, const double* xin, co
 // even-sized levels the colour of a region cell follows from its region
 // coordinates (a wrap by an even size keeps the parity), so only the cells of
 // that colour are visited; odd-sized levels test each cell.
-template <int SHRINK>
+template <class S, int SHRINK>
 __device__ void tile_half_sweep_t(const HLevel& L, int i0, int j0, TileRefs t, int colour) {
-    constexpr int ROWS = RW - 2 * SHRINK;
-    constexpr int HALF = (ROWS + 1) / 2;
+    constexpr int RW = S::RW, RH = S::RH;
+    constexpr int ROWS = RH - 2 * SHRINK, COLS = RW - 2 * SHRINK;
+    constexpr int HALF = (COLS + 1) / 2;
     const bool even = ((L.nx | L.ny) & 1) == 0;
     if (even) {
         for (int q = threadIdx.x; q < ROWS * HALF; q += blockDim.x) {
@@ -299,9 +303,9 @@ __device__ void tile_half_sweep_t(const HLevel& L, int i0, int j0, TileRefs t, i
             t.x[r] = t.id[r] * (t.b[r] + nb) * t.m[r];
         }
     } else {
-        for (int r = threadIdx.x; r < RN; r += blockDim.x) {
+        for (int r = threadIdx.x; r < S::RN; r += blockDim.x) {
             const int rj = r / RW, ri = r - rj * RW;
-            if (ri < SHRINK || ri >= RW - SHRINK || rj < SHRINK || rj >= RW - SHRINK) continue;
+            if (ri < SHRINK || ri >= RW - SHRINK || rj < SHRINK || rj >= RH - SHRINK) continue;
             const int gi = wrap_any(i0 - HALO + ri, L.nx), gj = wrap_any(j0 - HALO + rj, L.ny);
             if (((gi + gj) & 1) != colour) continue;
             const double nb = L.cx * (t.ku[r] * t.x[r + 1] + t.ku[r - 1] * t.x[r - 1]) +
@@ -313,15 +317,18 @@ __device__ void tile_half_sweep_t(const HLevel& L, int i0, int j0, TileRefs t, i
 }
 
 // four half-sweeps with colours c0, 1 - c0, c0, 1 - c0 on a region shrinking by one ring each
+template <class S>
 __device__ __forceinline__ void tile_four_half_sweeps(const HLevel& L, int i0, int j0, TileRefs t, int c0) {
-    tile_half_sweep_t<1>(L, i0, j0, t, c0);
-    tile_half_sweep_t<2>(L, i0, j0, t, 1 - c0);
-    tile_half_sweep_t<3>(L, i0, j0, t, c0);
-    tile_half_sweep_t<4>(L, i0, j0, t, 1 - c0);
+    tile_half_sweep_t<S, 1>(L, i0, j0, t, c0);
+    tile_half_sweep_t<S, 2>(L, i0, j0, t, 1 - c0);
+    tile_half_sweep_t<S, 3>(L, i0, j0, t, c0);
+    tile_half_sweep_t<S, 4>(L, i0, j0, t, 1 - c0);
 }
 
 // (b - A x) * mask at region cell r (VarOperator.apply, solvers_var.py:47-53)
+template <class S>
 __device__ __forceinline__ double tile_residual(const HLevel& L, double coef, TileRefs t, int r) {
+    constexpr int RW = S::RW;
     const double m = t.m[r];
     const double xm = t.x[r] * m;
     const double xe = t.x[r + 1] * t.m[r + 1];
@@ -337,54 +344,77 @@ __device__ __forceinline__ double tile_residual(const HLevel& L, double coef, Ti
     return (t.b[r] - ax) * m;
 }
 
+template <class S>
 __device__ void tile_store_x(const HLevel& L, int i0, int j0, TileRefs t, double* xout) {
-    for (int r = threadIdx.x; r < TILE * TILE; r += blockDim.x) {
-        const int cj = r / TILE, ci = r - cj * TILE;
+    for (int r = threadIdx.x; r < S::TX * S::TY; r += blockDim.x) {
+        const int cj = r / S::TX, ci = r - cj * S::TX;
         const int gi = i0 + ci, gj = j0 + cj;
         if (gi >= L.nx || gj >= L.ny) continue;
-        xout[gj * L.nx + gi] = t.x[(cj + HALO) * RW + ci + HALO];
+        xout[gj * L.nx + gi] = t.x[(cj + HALO) * S::RW + ci + HALO];
     }
 }
 
 // down phase of level l: pre-smoothing, restricted residual into level l+1
 // (solvers_var.py:141-147); x of level l+1 starts at zero implicitly
+template <class S>
 __device__ void mg_down(const HelmParams& H, int l, const double* xin, double* xout, double* smem) {
     const HLevel& L = H.lv[l];
     const HLevel& C = H.lv[l + 1];
-    const int tx = (L.nx + TILE - 1) / TILE, ty = (L.ny + TILE - 1) / TILE;
-    TileRefs t = tile_refs(smem);
+    const int tx = (L.nx + S::TX - 1) / S::TX, ty = (L.ny + S::TY - 1) / S::TY;
+    TileRefs t = tile_refs<S>(smem);
     for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
-        const int i0 = (tile % tx) * TILE, j0 = (tile / tx) * TILE;
-        tile_load(L, i0, j0, xin, nullptr, t);
-        tile_four_half_sweeps(L, i0, j0, t, 0);
-        for (int r = threadIdx.x; r < (TILE / 2) * (TILE / 2); r += blockDim.x) {
-            const int cj = r / (TILE / 2), ci = r - cj * (TILE / 2);
+        const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
+        tile_load<S>(L, i0, j0, xin, nullptr, t);
+        tile_four_half_sweeps<S>(L, i0, j0, t, 0);
+        for (int r = threadIdx.x; r < (S::TX / 2) * (S::TY / 2); r += blockDim.x) {
+            const int cj = r / (S::TX / 2), ci = r - cj * (S::TX / 2);
             const int I = i0 / 2 + ci, J = j0 / 2 + cj;
             if (I >= C.nx || J >= C.ny) continue;
-            const int r00 = (HALO + 2 * cj) * RW + HALO + 2 * ci;
-            const double a = tile_residual(L, H.coef, t, r00);
-            const double b = tile_residual(L, H.coef, t, r00 + 1);
-            const double c = tile_residual(L, H.coef, t, r00 + RW);
-            const double d = tile_residual(L, H.coef, t, r00 + RW + 1);
+            const int r00 = (HALO + 2 * cj) * S::RW + HALO + 2 * ci;
+            const double a = tile_residual<S>(L, H.coef, t, r00);
+            const double b = tile_residual<S>(L, H.coef, t, r00 + 1);
+            const double c = tile_residual<S>(L, H.coef, t, r00 + S::RW);
+            const double d = tile_residual<S>(L, H.coef, t, r00 + S::RW + 1);
             C.b[J * C.nx + I] = 0.25 * (a + b + c + d);
         }
-        tile_store_x(L, i0, j0, t, xout);
+        tile_store_x<S>(L, i0, j0, t, xout);
         __syncthreads();
     }
 }
 
 // up phase of level l: x + prolong(x_coarse) * mask, then the two reverse sweeps
-// (solvers_var.py:148-150)
+// (solvers_var.py:148-150). With `leaves`, level 0's tiles are one NumPy leaf
+// per interior row (128 cells starting at a multiple of 128): after the sweeps
+// every interior cell and its four neighbours hold the new x, so each warp forms
+// the squared residual (b - A x)^2 of one row and its leaf sum in NumPy's order
+// -- the per-cycle residual norm without another pass over the grid.
+template <class S>
 __device__ void mg_up(const HelmParams& H, int l, const double* xin, const HLevel& C, double* xout,
-                      double* smem) {
+                      double* smem, double* leaves) {
     const HLevel& L = H.lv[l];
-    const int tx = (L.nx + TILE - 1) / TILE, ty = (L.ny + TILE - 1) / TILE;
-    TileRefs t = tile_refs(smem);
+    const int tx = (L.nx + S::TX - 1) / S::TX, ty = (L.ny + S::TY - 1) / S::TY;
+    TileRefs t = tile_refs<S>(smem);
     for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
-        const int i0 = (tile % tx) * TILE, j0 = (tile / tx) * TILE;
-        tile_load(L, i0, j0, xin, &C, t);
-        tile_four_half_sweeps(L, i0, j0, t, 1);
-        tile_store_x(L, i0, j0, t, xout);
+        const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
+        tile_load<S>(L, i0, j0, xin, &C, t);
+        tile_four_half_sweeps<S>(L, i0, j0, t, 1);
+        tile_store_x<S>(L, i0, j0, t, xout);
+        if constexpr (S::TX == 128) {
+            if (leaves) {
+                const int lane = threadIdx.x & 31;
+                for (int cj = threadIdx.x >> 5; cj < S::TY; cj += blockDim.x >> 5) {
+                    if (j0 + cj >= L.ny) continue;  // warp-uniform
+                    double va[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const double d = tile_residual<S>(L, H.coef, t, (cj + HALO) * S::RW + HALO + lane + 32 * q);
+                        va[q] = d * d;
+                    }
+                    const double a = leaf_sum_warp(va, 128);
+                    if (lane == 0) leaves[((j0 + cj) * L.nx + i0) / 128] = a;
+                }
+            }
+        }
         __syncthreads();
     }
 }
@@ -512,13 +542,13 @@ __device__ void mg_coarse(const HelmParams& H, double* smem, const double* xin_c
 __device__ void mg_smooth(const HelmParams& H, int l, const double* xin, double* xout, bool reverse,
                           double* smem) {
     const HLevel& L = H.lv[l];
-    const int tx = (L.nx + TILE - 1) / TILE, ty = (L.ny + TILE - 1) / TILE;
-    TileRefs t = tile_refs(smem);
+    const int tx = (L.nx + Tile32::TX - 1) / Tile32::TX, ty = (L.ny + Tile32::TY - 1) / Tile32::TY;
+    TileRefs t = tile_refs<Tile32>(smem);
     for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
-        const int i0 = (tile % tx) * TILE, j0 = (tile / tx) * TILE;
-        tile_load(L, i0, j0, xin, nullptr, t);
-        tile_four_half_sweeps(L, i0, j0, t, reverse ? 1 : 0);
-        tile_store_x(L, i0, j0, t, xout);
+        const int i0 = (tile % tx) * Tile32::TX, j0 = (tile / tx) * Tile32::TY;
+        tile_load<Tile32>(L, i0, j0, xin, nullptr, t);
+        tile_four_half_sweeps<Tile32>(L, i0, j0, t, reverse ? 1 : 0);
+        tile_store_x<Tile32>(L, i0, j0, t, xout);
         __syncthreads();
     }
 }
@@ -537,7 +567,10 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, b
     }
     const int ndown = cf < nl ? cf : nl - 1;
     for (int l = 0; l < ndown && ok; ++l) {
-        mg_down(H, l, l == 0 ? x0 : nullptr, l == 0 ? x0b : H.lv[l].x, smem);
+        if (l == 0 && H.wide0)
+            mg_down<TileWide>(H, 0, x0, x0b, smem);
+        else
+            mg_down<Tile32>(H, l, l == 0 ? x0 : nullptr, l == 0 ? x0b : H.lv[l].x, smem);
         ok = grid_sync(H);
     }
     if (!ok) return x0;
@@ -561,7 +594,10 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, b
         double* xout = (l == 0) ? x0 : H.lv[l].x2;
         HLevel C = H.lv[l + 1];
         C.x = H.lv[l + 1].x2;
-        mg_up(H, l, xin, C, xout, smem);
+        if (l == 0 && H.wide0)
+            mg_up<TileWide>(H, 0, xin, C, xout, smem, H.fused_res ? H.leafA : nullptr);
+        else
+            mg_up<Tile32>(H, l, xin, C, xout, smem, nullptr);
         ok = grid_sync(H);
     }
     return x0;
@@ -598,7 +634,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
             double* xc = x;  // the level-0 buffer holding the current iterate
             for (int it = 1; it <= H.max_iter && ok; ++it) {
                 if (H.kind == HK_MULTIGRID) {
-                    xc = vcycle_tiled(H, xc, sm + H.n_leaves, ok);
+                    xc = vcycle_tiled(H, xc, sm, ok);
                 } else {
                     colour_phase(L0, x, b0, 0, grid_team());
                     ok = grid_sync(H);
@@ -607,15 +643,19 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                     ok = grid_sync(H);
                 }
                 if (!ok) break;
-                const double* xr = xc;
-                leaf_phase(H,
-                           [&](int e) {
-                               const double d = __ldcg(b0 + e) - apply_at(L0, H.coef, xr, cell_of(L0, e));
-                               return make_double2(d * d, 0.0);
-                           },
-                           H.leafA, nullptr);
-                ok = grid_sync(H);
-                if (!ok) break;
+                // the true residual's leaf sums: formed by the last up phase when
+                // level 0's tiles are NumPy's leaves, else by a pass of their own
+                if (!(H.kind == HK_MULTIGRID && H.fused_res)) {
+                    const double* xr = xc;
+                    leaf_phase(H,
+                               [&](int e) {
+                                   const double d = __ldcg(b0 + e) - apply_at(L0, H.coef, xr, cell_of(L0, e));
+                                   return make_double2(d * d, 0.0);
+                               },
+                               H.leafA, nullptr);
+                    ok = grid_sync(H);
+                    if (!ok) break;
+                }
                 iters = it;
                 const double res = sqrt(tree_fold(H, H.leafA, sm));
                 if (res <= tol) {
@@ -920,8 +960,20 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     }
     size_t coarse_cells = 0;
     for (int l = H.coarse_from; l < H.n_levels; ++l) coarse_cells += (size_t)H.lv[l].n;
-    const size_t mg_work = (kind == HK_MULTIGRID) ? std::max<size_t>(6 * RN, 6 * coarse_cells) : 0;
-    smem_ = sizeof(double) * ((size_t)H.n_leaves + mg_work);
+    // Level 0 of a grid whose 32 x 32 tiles need more than one round over the SMs
+    // runs 128 x 16 tiles instead. When NumPy's leaves are then exactly the tiles'
+    // 128-cell rows, the last up phase forms the residual's leaf sums itself.
+    const bool grid_levels = kind == HK_MULTIGRID && H.n_levels >= 2 && H.coarse_from >= 1;
+    const long long tiles32 = (long long)((nx + 31) / 32) * ((ny + 31) / 32);
+    H.wide0 = (grid_levels && nx % TileWide::TX == 0 && tiles32 > sms) ? 1 : 0;
+    bool aligned = H.n_leaves > 0;
+    for (int q = 0; q < H.n_leaves && aligned; ++q)
+        aligned = leaves[q] == 128 * q && leaves[q + 1] - leaves[q] == 128;
+    H.fused_res = (H.wide0 && aligned) ? 1 : 0;
+    const size_t tile_work = 6 * (size_t)(H.wide0 ? std::max(TileWide::RN, Tile32::RN) : Tile32::RN);
+    const size_t mg_work = (kind == HK_MULTIGRID) ? std::max<size_t>(tile_work, 6 * coarse_cells) : 0;
+    // the tree fold and the V-cycle never run at the same time: one region serves both
+    smem_ = sizeof(double) * std::max<size_t>((size_t)H.n_leaves, mg_work);
     if (smem_ > 200 * 1024) {
         err = "Helmholtz grid too large for the single-pass reduction tree";
         return OC_ERR_UNSUPPORTED;

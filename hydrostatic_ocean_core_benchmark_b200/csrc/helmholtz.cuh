@@ -24,6 +24,8 @@ struct HLevel {
 
 struct HelmParams {
     int n_levels, kind, max_iter, coarse_from;
+    int wide0;      // level 0 runs 128 x 16 tiles
+    int fused_res;  // ... whose rows are NumPy's leaves: the up phase forms the residual sums
     double coef, rtol;
     HLevel lv[OC_MAX_LEVELS];
     double *r, *z, *p, *Ap;  // level-0 work vectors

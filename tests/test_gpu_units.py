@@ -110,10 +110,14 @@ def test_binary_refuses_open_boundaries(tmp_path):
     assert "FATAL" in proc.stderr
 
 
-@pytest.mark.parametrize("nx,ny", [(66, 66), (50, 50), (96, 80), (256, 256), (40, 24)])
+@pytest.mark.parametrize("nx,ny", [(66, 66), (50, 50), (96, 80), (256, 256), (40, 24), (512, 512),
+                                   (640, 256), (512, 300)])
 def test_multigrid_paths_match_oracle(nx, ny):
     """Every V-cycle layout: all levels on the grid (66: the coarsening stops at an odd
-    33x33), partial tiles (50, 96x80), grid levels above CTA-0 levels (256), all in CTA 0 (40x24)."""
+    33x33), partial tiles (50, 96x80), grid levels above CTA-0 levels (256), all in CTA 0
+    (40x24); level 0 in 128x16 tiles whose rows are NumPy's leaves, so the up phase forms
+    the residual sums (512), wide tiles with unaligned leaves (640x256), and wide partial
+    tiles above a grid-wide coarsest level (512x300)."""
     from hydrostatic_ocean_core_benchmark_b200 import cases
     from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
     s = cases.seamount_basin(nx=nx, ny=ny, nz=8, seed=nx * 1000 + ny, solver_kind="multigrid")
