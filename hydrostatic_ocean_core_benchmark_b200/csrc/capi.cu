@@ -102,6 +102,9 @@ struct oc_handle {
         long long steps, tridiag, rebuilds, substeps, solves, launches;
     };
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // second stream for the old-state kernels that do not depend on the closure
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     Counters graph_delta[2] = {};
     cudaStream_t capture_stream = nullptr;
 };
@@ -322,9 +325,9 @@ int ensure_log(oc_handle* h, long long needed, cudaStream_t s) {
 // ---- per-kernel event timing
 void prof_harvest(oc_handle* h) {
     if (h->ev_marks.empty()) return;
-    cudaEventSynchronize(h->ev_pool[h->ev_used - 1]);
     for (const auto& m : h->ev_marks) {
         float ms = 0.0f;
+        cudaEventSynchronize(h->ev_pool[m.second + 1]);  // launches on two streams complete out of order
         cudaEventElapsedTime(&ms, h->ev_pool[m.second], h->ev_pool[m.second + 1]);
         h->prof_ms[m.first] += ms;
     }
@@ -379,6 +382,22 @@ int step_once(oc_handle* h, cudaStream_t s) {
     double *u = h->U[cur], *v = h->V[cur], *b = h->B[cur], *eta = h->ETA[cur];
     double *un = h->U[nxt], *vn = h->V[nxt], *etan = h->ETA[nxt];
     const bool theta = c.scheme == OC_SCHEME_THETA, split = c.scheme == OC_SCHEME_SPLIT;
+    // The kernels of the old state that do not depend on the closure (w, phi, the
+    // barotropic gradient, transports and divergence) run on a second stream,
+    // beside the closure chain (TKE closure -> Ku/Kv -> multigrid rebuild);
+    // both join before the explicit momentum terms.
+    cudaStream_t a = h->aux;
+    cudaEventRecord(h->fork, s);
+    cudaStreamWaitEvent(a, h->fork, 0);
+    { Prof pr(h, a, "wcol"); launch_wcol(P, u, v, h->w, a); }
+    { Prof pr(h, a, "phi"); launch_phi(P, b, h->phi, a); }
+    if (!split) { Prof pr(h, a, "grad2"); launch_grad2(P, eta, h->gx2, h->gy2, a); }
+    if (theta) {
+        { Prof pr(h, a, "transport"); launch_transport(P, u, v, h->Uold, h->Vold, a); }
+        { Prof pr(h, a, "div2"); launch_div2(P, h->Uold, h->Vold, h->div_old, a); }
+    }
+    if (split) { Prof pr(h, a, "transport"); launch_transport(P, u, v, h->bt[0], h->bt[1], a); }  // U0, V0
+    cudaEventRecord(h->join, a);
     if (c.closure == OC_CLOSURE_TKE) {
         { Prof pr(h, s, "closure"); launch_closure(P, u, v, b, h->e, h->km, h->kh, h->q, s); }
         h->tridiag += 2;
@@ -388,19 +407,12 @@ int step_once(oc_handle* h, cudaStream_t s) {
             h->rebuilds += 1;
         }
     }
-    { Prof pr(h, s, "wcol"); launch_wcol(P, u, v, h->w, s); }
-    { Prof pr(h, s, "phi"); launch_phi(P, b, h->phi, s); }
+    cudaStreamWaitEvent(s, h->join, 0);
     {
         Prof pr(h, s, "mom_explicit");
         launch_mom_explicit(P, u, v, b, h->phi, h->w, h->km, h->pgx, h->pgy, h->avpv, h->avpu, h->dzu,
                             h->dzv, h->stu, h->stv, s);
     }
-    if (!split) { Prof pr(h, s, "grad2"); launch_grad2(P, eta, h->gx2, h->gy2, s); }
-    if (theta) {
-        { Prof pr(h, s, "transport"); launch_transport(P, u, v, h->Uold, h->Vold, s); }
-        { Prof pr(h, s, "div2"); launch_div2(P, h->Uold, h->Vold, h->div_old, s); }
-    }
-    if (split) { Prof pr(h, s, "transport"); launch_transport(P, u, v, h->bt[0], h->bt[1], s); }  // U0, V0
     const double *uit = u, *vit = v;
     double *last_gu = nullptr, *last_gv = nullptr;
     for (int m = 0; m < c.n_picard; ++m) {
@@ -566,6 +578,13 @@ int oc_create(const oc_config* cfg, oc_handle** out) {
     }
     oc_handle* h = new oc_handle();
     h->cfg = *cfg;
+    if (cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming) != cudaSuccess) {
+        std::fprintf(stderr, "oc_create: stream or event creation failed\n");
+        delete h;
+        return OC_ERR_CUDA;
+    }
     h->nx = cfg->nx;
     h->ny = cfg->ny;
     h->nz = cfg->nz;
@@ -1102,6 +1121,9 @@ void oc_destroy(oc_handle* h) {
     cudaDeviceSynchronize();
     drop_graphs(h);
     if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
+    if (h->aux) cudaStreamDestroy(h->aux);
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join) cudaEventDestroy(h->join);
     delete h->solver;
     for (void* p : h->allocs) cudaFree(p);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
