@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(128) k_qsolve(KP P, const double* __restrict__
 // at a level is read just before) and q. With the Gaspar lengths, the lengths
 // of interface k are formed inside the forward sweep.
 template <int NZM>
-__global__ void __launch_bounds__(128) k_closure(KP P, const double* __restrict__ u,
+__global__ void __launch_bounds__(128, 8) k_closure(KP P, const double* __restrict__ u,
                                                  const double* __restrict__ v,
                                                  const double* __restrict__ b,
                                                  double* __restrict__ e, double* __restrict__ km,
@@ -407,7 +407,7 @@ __global__ void k_kukv(KP P, const double* __restrict__ q, double* __restrict__ 
 // ------------------------------------------------------------------ w from transport divergence
 // w[k] = -sum_{k'>=k} div(dz3u u, dz3v v)[k'], accumulated from the bottom
 // (vertical_var.py:109-121); w[nz] = 0.
-__global__ void k_wcol(KP P, const double* __restrict__ u, const double* __restrict__ v,
+__global__ void __launch_bounds__(128, 8) k_wcol(KP P, const double* __restrict__ u, const double* __restrict__ v,
                        double* __restrict__ w) {
     COLUMN_PROLOGUE
     const int nz = P.nz;
