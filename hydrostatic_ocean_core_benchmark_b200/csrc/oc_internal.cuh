@@ -116,6 +116,17 @@ struct ColGeo {
         if (k < kf) return P.dzr[k];
         return k == kf ? d0 : d1;
     }
+    // depth of the top of level k: the sequential sum of the thicknesses above
+    // (col_above with the column's geometry in registers)
+    __device__ __forceinline__ double above(const KP& P, int k) const {
+        const int m = k < kf ? k : kf;
+        double a = P.edge[m];
+        if (k > kf && kf < kb) {
+            a = (m == 0) ? d0 : a + d0;
+            if (k > kf + 1 && kf + 1 < kb) a = a + d1;
+        }
+        return a;
+    }
 };
 
 __device__ __forceinline__ double col_m3(const KP& P, int c, int k) { return k < P.kinfo[c].y ? 1.0 : 0.0; }

@@ -509,142 +509,6 @@ __device__ __forceinline__ double u_on_v(const KP& P, const Nbr& nb, const doubl
     return avg * m3v_at(P, nb, 0, 0, k);
 }
 
-// ------------------------------------------------------------------ momentum advection
-// x-, y- and z-flux divergence of u at its east face (advection_v06.py:77-99 for
-// the kappa/TVD scheme, advection.py:62-79 for the centred one).
-__device__ double mom_adv_u(const KP& P, const Nbr& nb, const double* __restrict__ u,
-                            const double* __restrict__ v, const double* __restrict__ w, int k) {
-    const size_t n2 = P.n2;
-    const size_t o = (size_t)k * n2;
-    const int nz = P.nz;
-    auto U = [&](int dj, int di) { return u[o + nb.at(dj, di)]; };
-    auto V = [&](int dj, int di) { return v[o + nb.at(dj, di)]; };
-    auto Uk = [&](int kk) { return u[(size_t)kk * n2 + nb.c]; };
-    auto W = [&](int kk, int di) { return w[(size_t)kk * n2 + nb.at(0, di)]; };
-    const bool up3 = P.advection >= 3;
-    const bool lim = P.advection == 4;
-    double ax, ay, az;
-    if (up3) {
-        const double ub_c0 = 0.5 * (U(0, -1) + U(0, 0));
-        const double ub_c1 = 0.5 * (U(0, 0) + U(0, 1));
-        const double uc0 = kappa_face(P, U(0, -2), U(0, -1), U(0, 0), U(0, 1), ub_c0,
-                                      m3u_at(P, nb, 0, -2, k), m3u_at(P, nb, 0, 1, k), lim);
-        const double uc1 = kappa_face(P, U(0, -1), U(0, 0), U(0, 1), U(0, 2), ub_c1,
-                                      m3u_at(P, nb, 0, -1, k), m3u_at(P, nb, 0, 2, k), lim);
-        ax = (ub_c1 * uc1 - ub_c0 * uc0) / P.dx;
-        const double vb0 = 0.5 * (V(0, 0) + V(0, 1));
-        const double vbm = 0.5 * (V(-1, 0) + V(-1, 1));
-        const double fy0 = vb0 * kappa_face(P, U(-1, 0), U(0, 0), U(1, 0), U(2, 0), vb0,
-                                            m3u_at(P, nb, -1, 0, k), m3u_at(P, nb, 2, 0, k), lim);
-        const double fym = vbm * kappa_face(P, U(-2, 0), U(-1, 0), U(0, 0), U(1, 0), vbm,
-                                            m3u_at(P, nb, -2, 0, k), m3u_at(P, nb, 1, 0, k), lim);
-        ay = (fy0 - fym) / P.dy;
-        double fz[2];
-        for (int t = 0; t < 2; ++t) {
-            const int kk = k + t;
-            if (kk == 0 || kk == nz) {
-                fz[t] = 0.0;
-                continue;
-            }
-            const double wb = 0.5 * (W(kk, 0) + W(kk, 1));
-            const double fu = (kk >= 2) ? Uk(kk - 2) : 0.0;
-            const double fd = (kk + 1 <= nz - 1) ? Uk(kk + 1) : 0.0;
-            const bool hu = (kk >= 2) && m3u_at(P, nb, 0, 0, kk - 2) > 0.0;
-            const bool hd = (kk + 1 <= nz - 1) && m3u_at(P, nb, 0, 0, kk + 1) > 0.0;
-            fz[t] = wb * kappa_face_z(P, fu, Uk(kk - 1), Uk(kk), fd, wb, hu, hd, lim);
-        }
-        az = (fz[0] - fz[1]) / P.dz_nom[k];
-    } else {
-        const double ub_c0 = 0.5 * (U(0, -1) + U(0, 0));
-        const double ub_c1 = 0.5 * (U(0, 0) + U(0, 1));
-        ax = (ub_c1 * ub_c1 - ub_c0 * ub_c0) / P.dx;
-        const double vb0 = 0.5 * (V(0, 0) + V(0, 1));
-        const double vbm = 0.5 * (V(-1, 0) + V(-1, 1));
-        const double fy0 = vb0 * (0.5 * (U(0, 0) + U(1, 0)));
-        const double fym = vbm * (0.5 * (U(-1, 0) + U(0, 0)));
-        ay = (fy0 - fym) / P.dy;
-        double fz[2];
-        for (int t = 0; t < 2; ++t) {
-            const int kk = k + t;
-            if (kk == 0 || kk == nz) {
-                fz[t] = 0.0;
-                continue;
-            }
-            const double wb = 0.5 * (W(kk, 0) + W(kk, 1));
-            fz[t] = wb * 0.5 * (Uk(kk - 1) + Uk(kk));
-        }
-        az = (fz[0] - fz[1]) / P.dz_nom[k];
-    }
-    return ax + ay + az;
-}
-
-// the same for v at its north face (advection_v06.py:100-108, advection.py:81-95)
-__device__ double mom_adv_v(const KP& P, const Nbr& nb, const double* __restrict__ u,
-                            const double* __restrict__ v, const double* __restrict__ w, int k) {
-    const size_t n2 = P.n2;
-    const size_t o = (size_t)k * n2;
-    const int nz = P.nz;
-    auto U = [&](int dj, int di) { return u[o + nb.at(dj, di)]; };
-    auto V = [&](int dj, int di) { return v[o + nb.at(dj, di)]; };
-    auto Vk = [&](int kk) { return v[(size_t)kk * n2 + nb.c]; };
-    auto W = [&](int kk, int dj) { return w[(size_t)kk * n2 + nb.at(dj, 0)]; };
-    const bool up3 = P.advection >= 3;
-    const bool lim = P.advection == 4;
-    double bx, by, bz;
-    if (up3) {
-        const double vb_c0 = 0.5 * (V(-1, 0) + V(0, 0));
-        const double vb_c1 = 0.5 * (V(0, 0) + V(1, 0));
-        const double vc0 = kappa_face(P, V(-2, 0), V(-1, 0), V(0, 0), V(1, 0), vb_c0,
-                                      m3v_at(P, nb, -2, 0, k), m3v_at(P, nb, 1, 0, k), lim);
-        const double vc1 = kappa_face(P, V(-1, 0), V(0, 0), V(1, 0), V(2, 0), vb_c1,
-                                      m3v_at(P, nb, -1, 0, k), m3v_at(P, nb, 2, 0, k), lim);
-        by = (vb_c1 * vc1 - vb_c0 * vc0) / P.dy;
-        const double ub0 = 0.5 * (U(0, 0) + U(1, 0));
-        const double ubm = 0.5 * (U(0, -1) + U(1, -1));
-        const double fx0 = ub0 * kappa_face(P, V(0, -1), V(0, 0), V(0, 1), V(0, 2), ub0,
-                                            m3v_at(P, nb, 0, -1, k), m3v_at(P, nb, 0, 2, k), lim);
-        const double fxm = ubm * kappa_face(P, V(0, -2), V(0, -1), V(0, 0), V(0, 1), ubm,
-                                            m3v_at(P, nb, 0, -2, k), m3v_at(P, nb, 0, 1, k), lim);
-        bx = (fx0 - fxm) / P.dx;
-        double fz[2];
-        for (int t = 0; t < 2; ++t) {
-            const int kk = k + t;
-            if (kk == 0 || kk == nz) {
-                fz[t] = 0.0;
-                continue;
-            }
-            const double wb = 0.5 * (W(kk, 0) + W(kk, 1));
-            const double fu = (kk >= 2) ? Vk(kk - 2) : 0.0;
-            const double fd = (kk + 1 <= nz - 1) ? Vk(kk + 1) : 0.0;
-            const bool hu = (kk >= 2) && m3v_at(P, nb, 0, 0, kk - 2) > 0.0;
-            const bool hd = (kk + 1 <= nz - 1) && m3v_at(P, nb, 0, 0, kk + 1) > 0.0;
-            fz[t] = wb * kappa_face_z(P, fu, Vk(kk - 1), Vk(kk), fd, wb, hu, hd, lim);
-        }
-        bz = (fz[0] - fz[1]) / P.dz_nom[k];
-    } else {
-        const double vb_c0 = 0.5 * (V(-1, 0) + V(0, 0));
-        const double vb_c1 = 0.5 * (V(0, 0) + V(1, 0));
-        by = (vb_c1 * vb_c1 - vb_c0 * vb_c0) / P.dy;
-        const double ub0 = 0.5 * (U(0, 0) + U(1, 0));
-        const double ubm = 0.5 * (U(0, -1) + U(1, -1));
-        const double fx0 = ub0 * (0.5 * (V(0, 0) + V(0, 1)));
-        const double fxm = ubm * (0.5 * (V(0, -1) + V(0, 0)));
-        bx = (fx0 - fxm) / P.dx;
-        double fz[2];
-        for (int t = 0; t < 2; ++t) {
-            const int kk = k + t;
-            if (kk == 0 || kk == nz) {
-                fz[t] = 0.0;
-                continue;
-            }
-            const double wb = 0.5 * (W(kk, 0) + W(kk, 1));
-            fz[t] = wb * 0.5 * (Vk(kk - 1) + Vk(kk));
-        }
-        bz = (fz[0] - fz[1]) / P.dz_nom[k];
-    }
-    return bx + by + bz;
-}
-
 // horizontal Laplacian D o G with the given face masks (operators_masked.py:64-68);
 // which = 0: u (x-mask m3u, y-mask m3v, cell mask m3u), 1: v (cell mask m3v),
 // 2: tracer (cell mask m3)
@@ -690,12 +554,120 @@ __device__ __forceinline__ double explicit_dz(const KP& P, int k, double fkm1, d
     return (out - dragc * idz) * (m3k > 0.0 ? 1.0 : 0.0);
 }
 
+// ------------------------------------------------------------------ momentum advection
+// x- and y-flux divergence of u at its east face at level k (advection_v06.py:77-99
+// for the kappa/TVD scheme, advection.py:62-79 for the centred one); the
+// reference forms ax + ay + az left to right, so (ax + ay) + az is its sum
+__device__ __forceinline__ double mom_adv_u_xy(const KP& P, const Nbr& nb, const double* __restrict__ u,
+                                               const double* __restrict__ v, int k) {
+    const size_t o = (size_t)k * P.n2;
+    auto U = [&](int dj, int di) { return u[o + nb.at(dj, di)]; };
+    auto V = [&](int dj, int di) { return v[o + nb.at(dj, di)]; };
+    if (P.advection >= 3) {
+        const bool lim = P.advection == 4;
+        const double ub_c0 = 0.5 * (U(0, -1) + U(0, 0));
+        const double ub_c1 = 0.5 * (U(0, 0) + U(0, 1));
+        const double uc0 = kappa_face(P, U(0, -2), U(0, -1), U(0, 0), U(0, 1), ub_c0,
+                                      m3u_at(P, nb, 0, -2, k), m3u_at(P, nb, 0, 1, k), lim);
+        const double uc1 = kappa_face(P, U(0, -1), U(0, 0), U(0, 1), U(0, 2), ub_c1,
+                                      m3u_at(P, nb, 0, -1, k), m3u_at(P, nb, 0, 2, k), lim);
+        const double ax = (ub_c1 * uc1 - ub_c0 * uc0) / P.dx;
+        const double vb0 = 0.5 * (V(0, 0) + V(0, 1));
+        const double vbm = 0.5 * (V(-1, 0) + V(-1, 1));
+        const double fy0 = vb0 * kappa_face(P, U(-1, 0), U(0, 0), U(1, 0), U(2, 0), vb0,
+                                            m3u_at(P, nb, -1, 0, k), m3u_at(P, nb, 2, 0, k), lim);
+        const double fym = vbm * kappa_face(P, U(-2, 0), U(-1, 0), U(0, 0), U(1, 0), vbm,
+                                            m3u_at(P, nb, -2, 0, k), m3u_at(P, nb, 1, 0, k), lim);
+        return ax + (fy0 - fym) / P.dy;
+    }
+    const double ub_c0 = 0.5 * (U(0, -1) + U(0, 0));
+    const double ub_c1 = 0.5 * (U(0, 0) + U(0, 1));
+    const double ax = (ub_c1 * ub_c1 - ub_c0 * ub_c0) / P.dx;
+    const double vb0 = 0.5 * (V(0, 0) + V(0, 1));
+    const double vbm = 0.5 * (V(-1, 0) + V(-1, 1));
+    const double fy0 = vb0 * (0.5 * (U(0, 0) + U(1, 0)));
+    const double fym = vbm * (0.5 * (U(-1, 0) + U(0, 0)));
+    return ax + (fy0 - fym) / P.dy;
+}
+
+// the same for v at its north face (advection_v06.py:100-108, advection.py:81-95):
+// bx + by, formed in that order
+__device__ __forceinline__ double mom_adv_v_xy(const KP& P, const Nbr& nb, const double* __restrict__ u,
+                                               const double* __restrict__ v, int k) {
+    const size_t o = (size_t)k * P.n2;
+    auto U = [&](int dj, int di) { return u[o + nb.at(dj, di)]; };
+    auto V = [&](int dj, int di) { return v[o + nb.at(dj, di)]; };
+    if (P.advection >= 3) {
+        const bool lim = P.advection == 4;
+        const double vb_c0 = 0.5 * (V(-1, 0) + V(0, 0));
+        const double vb_c1 = 0.5 * (V(0, 0) + V(1, 0));
+        const double vc0 = kappa_face(P, V(-2, 0), V(-1, 0), V(0, 0), V(1, 0), vb_c0,
+                                      m3v_at(P, nb, -2, 0, k), m3v_at(P, nb, 1, 0, k), lim);
+        const double vc1 = kappa_face(P, V(-1, 0), V(0, 0), V(1, 0), V(2, 0), vb_c1,
+                                      m3v_at(P, nb, -1, 0, k), m3v_at(P, nb, 2, 0, k), lim);
+        const double by = (vb_c1 * vc1 - vb_c0 * vc0) / P.dy;
+        const double ub0 = 0.5 * (U(0, 0) + U(1, 0));
+        const double ubm = 0.5 * (U(0, -1) + U(1, -1));
+        const double fx0 = ub0 * kappa_face(P, V(0, -1), V(0, 0), V(0, 1), V(0, 2), ub0,
+                                            m3v_at(P, nb, 0, -1, k), m3v_at(P, nb, 0, 2, k), lim);
+        const double fxm = ubm * kappa_face(P, V(0, -2), V(0, -1), V(0, 0), V(0, 1), ubm,
+                                            m3v_at(P, nb, 0, -2, k), m3v_at(P, nb, 0, 1, k), lim);
+        return (fx0 - fxm) / P.dx + by;
+    }
+    const double vb_c0 = 0.5 * (V(-1, 0) + V(0, 0));
+    const double vb_c1 = 0.5 * (V(0, 0) + V(1, 0));
+    const double by = (vb_c1 * vb_c1 - vb_c0 * vb_c0) / P.dy;
+    const double ub0 = 0.5 * (U(0, 0) + U(1, 0));
+    const double ubm = 0.5 * (U(0, -1) + U(1, -1));
+    const double fx0 = ub0 * (0.5 * (V(0, 0) + V(0, 1)));
+    const double fxm = ubm * (0.5 * (V(0, -1) + V(0, 0)));
+    return (fx0 - fxm) / P.dx + by;
+}
+
+// advective flux of a face velocity through interface kk of its column (0 =
+// surface), from the velocity at kk-2 .. kk+1, the interface w averaged over
+// the two cells of the face, and the face's wet levels kf
+// (advection_v06.py:50-74 and :86-99; advection.py:75-79)
+__device__ __forceinline__ double mom_vflux(const KP& P, int kk, int kf, double f_m2, double f_m1, double f_0,
+                                            double f_p1, double wa, double wb_) {
+    const int nz = P.nz;
+    if (kk == 0 || kk == nz) return 0.0;
+    const double wb = 0.5 * (wa + wb_);
+    if (P.advection >= 3) {
+        const double fu = (kk >= 2) ? f_m2 : 0.0;
+        const double fd = (kk + 1 <= nz - 1) ? f_p1 : 0.0;
+        const bool hu = (kk >= 2) && kk - 2 < kf;
+        const bool hd = (kk + 1 <= nz - 1) && kk + 1 < kf;
+        return wb * kappa_face_z(P, fu, f_m1, f_0, fd, wb, hu, hd, P.advection == 4);
+    }
+    return wb * 0.5 * (f_m1 + f_0);
+}
+
+// the diffusive flux K (f_above - f_below) / dzi through interface k of a face
+// velocity column (vertical_var.py:80-106), zero when the level above is the
+// column's last wet one
+__device__ __forceinline__ double diff_flux(double Kk, double f_above, double f_below, double dzf_above,
+                                           double dzf_below, double bottom_above) {
+    const double dzi = 0.5 * (dzf_above + dzf_below);
+    const double flux = Kk * (f_above - f_below) * inv_pos(dzi);
+    return bottom_above > 0.0 ? 0.0 : flux;
+}
+
 // ------------------------------------------------------------------ explicit momentum terms
-// One thread per cell: everything of the predictor that depends on the old
-// state only -- the common-depth pressure gradient, the old-state Coriolis
-// average, the explicit vertical diffusion and the stress + advection/viscosity
-// increment (model3d_v05.py:352-370).
-__global__ void __launch_bounds__(256, 4) k_mom_cell(
+// Everything of the predictor that depends on the old state only: the
+// common-depth pressure gradient, the old-state Coriolis average, the explicit
+// vertical diffusion and the stress + advection/viscosity increment
+// (model3d_v05.py:352-370), in level-marching form: one thread per column of
+// a 32 x 8 tile marches MOM_KL levels. The neighbour table and the compact
+// geometry of the column and of its east and north neighbours are formed once;
+// the velocity, viscosity and face-thickness values of the levels above and
+// below roll in registers; the vertical advective flux at the bottom of a level
+// and the diffusive flux there are carried to the next level as the fluxes at
+// its top (a per-cell form forms each of them twice). Every value is formed by
+// the reference's operations in its order.
+constexpr int MOM_KL = 10;
+
+__global__ void __launch_bounds__(256, 3) k_mom_column(
     KP P, const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ b,
     const double* __restrict__ phi, const double* __restrict__ w, const double* __restrict__ km,
     double* __restrict__ pgx, double* __restrict__ pgy, double* __restrict__ avpv,
@@ -703,82 +675,146 @@ __global__ void __launch_bounds__(256, 4) k_mom_cell(
     double* __restrict__ stu, double* __restrict__ stv) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
     if (i >= P.nx || j >= P.ny) return;
+    const int nz = P.nz;
+    const int kbeg = blockIdx.z * MOM_KL;
+    const int kend = kbeg + MOM_KL < nz ? kbeg + MOM_KL : nz;
     Nbr nb;
     nb.init(i, j, P.nx, P.ny);
     const size_t n2 = (size_t)P.n2;
-    const int nz = P.nz;
     const int c = nb.c, ce = nb.at(0, 1), cn = nb.at(1, 0);
-    const size_t o = (size_t)k * n2;
-    // geometry of this level, the faces above and below, the bottom flags
-    double m3c, m3e, m3n;
-    const double dz_c = col_dz(P, c, k, m3c), dz_e = col_dz(P, ce, k, m3e), dz_n = col_dz(P, cn, k, m3n);
-    const double m3u_k = m3c * m3e * P.mask_u[c];
-    const double m3v_k = m3c * m3n * P.mask_v[c];
-    const double dzu_k = m3u_k * face_combine(P, dz_c, dz_e);
-    const double dzv_k = m3v_k * face_combine(P, dz_c, dz_n);
-    double m, dzu_p1 = 0.0, dzv_p1 = 0.0, dzu_m1 = 0.0, dzv_m1 = 0.0;
-    const double m3_cn = (k + 1 < nz) ? col_m3(P, c, k + 1) : 0.0;
-    if (k + 1 < nz) {
-        ufacek(P, nb, 0, 0, k + 1, m, dzu_p1);
-        vfacek(P, nb, 0, 0, k + 1, m, dzv_p1);
+    const ColGeo gc = ColGeo::load(P, c), ge = ColGeo::load(P, ce), gn = ColGeo::load(P, cn);
+    const int2 kf = P.kface[c];
+    const double tau_u = P.tau_u[c], tau_v = P.tau_v[c];
+    // face thickness of the u and v faces of the column at level kk (0 outside)
+    auto dzu_at = [&](int kk) {
+        if (kk < 0 || kk >= nz) return 0.0;
+        double m;
+        return face_dz(P, kf.x, kk, gc.dz(P, kk, m), ge.dz(P, kk, m));
+    };
+    auto dzv_at = [&](int kk) {
+        if (kk < 0 || kk >= nz) return 0.0;
+        double m;
+        return face_dz(P, kf.y, kk, gc.dz(P, kk, m), gn.dz(P, kk, m));
+    };
+    auto m3c_at = [&](int kk) { return (kk >= 0 && kk < gc.kb) ? 1.0 : 0.0; };
+    auto Uc = [&](int kk) { return (kk >= 0 && kk < nz) ? u[(size_t)kk * n2 + c] : 0.0; };
+    auto Vc = [&](int kk) { return (kk >= 0 && kk < nz) ? v[(size_t)kk * n2 + c] : 0.0; };
+    // rolling column values at k-1, k, k+1 (and k+2 for the advected velocity)
+    double u_m1 = Uc(kbeg - 1), u_0 = Uc(kbeg), u_p1 = Uc(kbeg + 1);
+    double v_m1 = Vc(kbeg - 1), v_0 = Vc(kbeg), v_p1 = Vc(kbeg + 1);
+    double dzu_m1 = dzu_at(kbeg - 1), dzu_0 = dzu_at(kbeg);
+    double dzv_m1 = dzv_at(kbeg - 1), dzv_0 = dzv_at(kbeg);
+    double K_0 = km[(size_t)kbeg * n2 + c];
+    // fluxes through the top of level kbeg
+    double fz_u = 0.0, fz_v = 0.0, dfu = 0.0, dfv = 0.0;
+    {
+        const int kk = kbeg;
+        const double wc = w[(size_t)kk * n2 + c];
+        if (P.advection != 0) {
+            fz_u = mom_vflux(P, kk, kf.x, Uc(kk - 2), u_m1, u_0, u_p1, wc, w[(size_t)kk * n2 + ce]);
+            fz_v = mom_vflux(P, kk, kf.y, Vc(kk - 2), v_m1, v_0, v_p1, wc, w[(size_t)kk * n2 + cn]);
+        }
+        if (kk == 0) {
+            dfu = tau_u;
+            dfv = tau_v;
+        } else {
+            const double bot = (m3c_at(kk - 1) > 0.0 && m3c_at(kk) == 0.0) ? 1.0 : 0.0;
+            dfu = diff_flux(K_0, u_m1, u_0, dzu_m1, dzu_0, bot);
+            dfv = diff_flux(K_0, v_m1, v_0, dzv_m1, dzv_0, bot);
+        }
     }
-    double bottom_m1 = 0.0;
-    if (k > 0) {
-        ufacek(P, nb, 0, 0, k - 1, m, dzu_m1);
-        vfacek(P, nb, 0, 0, k - 1, m, dzv_m1);
-        bottom_m1 = (col_m3(P, c, k - 1) > 0.0 && m3c == 0.0) ? 1.0 : 0.0;
+    for (int k = kbeg; k < kend; ++k) {
+        const size_t o = (size_t)k * n2;
+        const double u_p2 = Uc(k + 2), v_p2 = Vc(k + 2);
+        const double dzu_p1 = dzu_at(k + 1), dzv_p1 = dzv_at(k + 1);
+        const double K_1 = km[o + n2 + c];
+        double m3c, m3e, m3n;
+        const double dz_c = gc.dz(P, k, m3c), dz_e = ge.dz(P, k, m3e), dz_n = gn.dz(P, k, m3n);
+        const double m3u_k = k < kf.x ? 1.0 : 0.0;
+        const double m3v_k = k < kf.y ? 1.0 : 0.0;
+        const double m3_cn = m3c_at(k + 1);
+        const double bottom_k = (m3c > 0.0 && m3_cn == 0.0) ? 1.0 : 0.0;
+        // ---- pressure gradient at a common depth (model3d_v05.py:211-230)
+        const double phc = phi[o + c], phe = phi[o + ce], phn = phi[o + cn];
+        const double bc = b[o + c], be = b[o + ce], bn = b[o + cn];
+        double px, py;
+        if (P.pgf_correction) {
+            const double zc_c = gc.above(P, k) + 0.5 * dz_c;
+            const double zc_e = ge.above(P, k) + 0.5 * dz_e;
+            const double zc_n = gn.above(P, k) + 0.5 * dz_n;
+            const double zfx = 0.5 * (zc_c + zc_e);
+            px = m3u_k * ((phe + be * (zfx - zc_e)) - (phc + bc * (zfx - zc_c))) / P.dx;
+            const double zfy = 0.5 * (zc_c + zc_n);
+            py = m3v_k * ((phn + bn * (zfy - zc_n)) - (phc + bc * (zfy - zc_c))) / P.dy;
+        } else {
+            px = m3u_k * (phe - phc) / P.dx * m3u_k;
+            py = m3v_k * (phn - phc) / P.dy * m3v_k;
+        }
+        pgx[o + c] = px;
+        pgy[o + c] = py;
+        // ---- Coriolis averages of the old state
+        avpv[o + c] = v_on_u(P, nb, v, o, k);
+        avpu[o + c] = u_on_v(P, nb, u, o, k);
+        // ---- explicit vertical diffusion: top flux carried, bottom flux formed here
+        double dbu = 0.0, dbv = 0.0;
+        if (k < nz - 1) {
+            dbu = diff_flux(K_1, u_0, u_p1, dzu_0, dzu_p1, bottom_k);
+            dbv = diff_flux(K_1, v_0, v_p1, dzv_0, dzv_p1, bottom_k);
+        }
+        {
+            const double mk = m3c > 0.0 ? 1.0 : 0.0;
+            const double idu = inv_pos(dzu_0);
+            const double outu = (dfu - dbu) * idu;
+            const double dragu = P.bottom_drag * u_0 * bottom_k;
+            dzu[o + c] = (outu - dragu * idu) * mk;
+            const double idv = inv_pos(dzv_0);
+            const double outv = (dfv - dbv) * idv;
+            const double dragv = P.bottom_drag * v_0 * bottom_k;
+            dzv[o + c] = (outv - dragv * idv) * mk;
+        }
+        // ---- advection and horizontal viscosity, then the stress increment
+        double exu = 0.0, exv = 0.0;
+        double fbu = 0.0, fbv = 0.0;
+        if (P.advection != 0) {
+            const double wc1 = w[o + n2 + c];
+            fbu = mom_vflux(P, k + 1, kf.x, u_m1, u_0, u_p1, u_p2, wc1, w[o + n2 + ce]);
+            fbv = mom_vflux(P, k + 1, kf.y, v_m1, v_0, v_p1, v_p2, wc1, w[o + n2 + cn]);
+            const double au = mom_adv_u_xy(P, nb, u, v, k) + (fz_u - fbu) / P.dz_nom[k];
+            const double av = mom_adv_v_xy(P, nb, u, v, k) + (fz_v - fbv) / P.dz_nom[k];
+            exu = exu - au * m3u_k;
+            exv = exv - av * m3v_k;
+        }
+        if (P.a_h > 0.0) {
+            exu = exu + P.a_h * hlap(P, nb, u, k, 0);
+            exv = exv + P.a_h * hlap(P, nb, v, k, 1);
+        }
+        if (k == 0) {
+            stu[o + c] = P.thv_dt * tau_u * inv_pos(dzu_0) + P.dt * exu;
+            stv[o + c] = P.thv_dt * tau_v * inv_pos(dzv_0) + P.dt * exv;
+        } else {
+            stu[o + c] = 0.0 + P.dt * exu;
+            stv[o + c] = 0.0 + P.dt * exv;
+        }
+        // roll down one level
+        fz_u = fbu;
+        fz_v = fbv;
+        dfu = dbu;
+        dfv = dbv;
+        u_m1 = u_0;
+        u_0 = u_p1;
+        u_p1 = u_p2;
+        v_m1 = v_0;
+        v_0 = v_p1;
+        v_p1 = v_p2;
+        dzu_m1 = dzu_0;
+        dzu_0 = dzu_p1;
+        dzv_m1 = dzv_0;
+        dzv_0 = dzv_p1;
+        K_0 = K_1;
     }
-    const double bottom_k = (m3c > 0.0 && m3_cn == 0.0) ? 1.0 : 0.0;
-    // ---- pressure gradient at a common depth (model3d_v05.py:211-230)
-    const double phc = phi[o + c], phe = phi[o + ce], phn = phi[o + cn];
-    const double bc = b[o + c], be = b[o + ce], bn = b[o + cn];
-    double px, py;
-    if (P.pgf_correction) {
-        const double zc_c = col_above(P, c, k) + 0.5 * dz_c;
-        const double zc_e = col_above(P, ce, k) + 0.5 * dz_e;
-        const double zc_n = col_above(P, cn, k) + 0.5 * dz_n;
-        const double zfx = 0.5 * (zc_c + zc_e);
-        px = m3u_k * ((phe + be * (zfx - zc_e)) - (phc + bc * (zfx - zc_c))) / P.dx;
-        const double zfy = 0.5 * (zc_c + zc_n);
-        py = m3v_k * ((phn + bn * (zfy - zc_n)) - (phc + bc * (zfy - zc_c))) / P.dy;
-    } else {
-        px = m3u_k * (phe - phc) / P.dx * m3u_k;
-        py = m3v_k * (phn - phc) / P.dy * m3v_k;
-    }
-    pgx[o + c] = px;
-    pgy[o + c] = py;
-    // ---- Coriolis averages of the old state
-    avpv[o + c] = v_on_u(P, nb, v, o, k);
-    avpu[o + c] = u_on_v(P, nb, u, o, k);
-    // ---- explicit vertical diffusion (viscosity of the cell column)
-    const double K_k = km[o + c], K_k1 = km[o + n2 + c];
-    const double uk = u[o + c], vk = v[o + c];
-    const double ukm = (k > 0) ? u[o - n2 + c] : 0.0, vkm = (k > 0) ? v[o - n2 + c] : 0.0;
-    const double ukp = (k + 1 < nz) ? u[o + n2 + c] : 0.0;
-    const double vkp = (k + 1 < nz) ? v[o + n2 + c] : 0.0;
-    dzu[o + c] = explicit_dz(P, k, ukm, uk, ukp, K_k, K_k1, dzu_m1, dzu_k, dzu_p1, bottom_m1, bottom_k,
-                             m3c, P.tau_u[c], P.bottom_drag);
-    dzv[o + c] = explicit_dz(P, k, vkm, vk, vkp, K_k, K_k1, dzv_m1, dzv_k, dzv_p1, bottom_m1, bottom_k,
-                             m3c, P.tau_v[c], P.bottom_drag);
-    // ---- advection and horizontal viscosity, then the stress increment
-    double exu = 0.0, exv = 0.0;
-    if (P.advection != 0) {
-        exu = exu - mom_adv_u(P, nb, u, v, w, k) * m3u_k;
-        exv = exv - mom_adv_v(P, nb, u, v, w, k) * m3v_k;
-    }
-    if (P.a_h > 0.0) {
-        exu = exu + P.a_h * hlap(P, nb, u, k, 0);
-        exv = exv + P.a_h * hlap(P, nb, v, k, 1);
-    }
-    if (k == 0) {
-        stu[o + c] = P.thv_dt * P.tau_u[c] * inv_pos(dzu_k) + P.dt * exu;
-        stv[o + c] = P.thv_dt * P.tau_v[c] * inv_pos(dzv_k) + P.dt * exv;
-    } else {
-        stu[o + c] = 0.0 + P.dt * exu;
-        stv[o + c] = 0.0 + P.dt * exv;
-    }
+    (void)dzu_m1;
+    (void)dzv_m1;
 }
 
 // ------------------------------------------------------------------ predictor + column solves
@@ -1457,8 +1493,9 @@ void launch_mom_explicit(const KP& P, const double* u, const double* v, const do
                          const double* phi, const double* w, const double* km, double* pgx,
                          double* pgy, double* avpv, double* avpu, double* dzu, double* dzv,
                          double* stu, double* stv, cudaStream_t s) {
-    k_mom_cell<<<cell_grid(P), cell_block(), 0, s>>>(P, u, v, b, phi, w, km, pgx, pgy, avpv, avpu, dzu,
-                                                    dzv, stu, stv);
+    const dim3 grid((P.nx + 31) / 32, (P.ny + 7) / 8, (P.nz + MOM_KL - 1) / MOM_KL);
+    k_mom_column<<<grid, dim3(32, 8), 0, s>>>(P, u, v, b, phi, w, km, pgx, pgy, avpv, avpu, dzu, dzv, stu,
+                                             stv);
 }
 
 void launch_predictor_rhs(const KP& P, const double* u, const double* v, const double* u_it,
