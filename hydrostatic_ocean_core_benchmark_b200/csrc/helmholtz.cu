@@ -39,8 +39,13 @@ struct TileShape {
     static constexpr int TX = TX_, TY = TY_;
     static constexpr int RW = TX + 2 * HALO, RH = TY + 2 * HALO, RN = RW * RH;
 };
-using Tile32 = TileShape<32, 32>;    // every grid level by default
+using Tile32 = TileShape<32, 32>;
+using Tile3216 = TileShape<32, 16>;
+using Tile16 = TileShape<16, 16>;
+using Tile8 = TileShape<8, 8>;
 using TileWide = TileShape<128, 16>;  // level 0 of large grids: one tile per CTA, one NumPy leaf per row
+// per-level tile shape codes (HLevel::shape)
+enum { SHAPE_32 = 0, SHAPE_3216 = 1, SHAPE_16 = 2, SHAPE_8 = 3, SHAPE_WIDE = 4 };
 
 // ------------------------------------------------------------------ barrier
 __device__ __forceinline__ bool grid_sync(const HelmParams& H) {
@@ -567,10 +572,15 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, b
     }
     const int ndown = cf < nl ? cf : nl - 1;
     for (int l = 0; l < ndown && ok; ++l) {
-        if (l == 0 && H.wide0)
-            mg_down<TileWide>(H, 0, x0, x0b, smem);
-        else
-            mg_down<Tile32>(H, l, l == 0 ? x0 : nullptr, l == 0 ? x0b : H.lv[l].x, smem);
+        const double* xin = l == 0 ? x0 : nullptr;
+        double* xout = l == 0 ? x0b : H.lv[l].x;
+        switch (H.lv[l].shape) {
+            case SHAPE_WIDE: mg_down<TileWide>(H, l, xin, xout, smem); break;
+            case SHAPE_3216: mg_down<Tile3216>(H, l, xin, xout, smem); break;
+            case SHAPE_16: mg_down<Tile16>(H, l, xin, xout, smem); break;
+            case SHAPE_8: mg_down<Tile8>(H, l, xin, xout, smem); break;
+            default: mg_down<Tile32>(H, l, xin, xout, smem); break;
+        }
         ok = grid_sync(H);
     }
     if (!ok) return x0;
@@ -594,10 +604,13 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, b
         double* xout = (l == 0) ? x0 : H.lv[l].x2;
         HLevel C = H.lv[l + 1];
         C.x = H.lv[l + 1].x2;
-        if (l == 0 && H.wide0)
-            mg_up<TileWide>(H, 0, xin, C, xout, smem, H.fused_res ? H.leafA : nullptr);
-        else
-            mg_up<Tile32>(H, l, xin, C, xout, smem, nullptr);
+        switch (H.lv[l].shape) {
+            case SHAPE_WIDE: mg_up<TileWide>(H, l, xin, C, xout, smem, H.fused_res ? H.leafA : nullptr); break;
+            case SHAPE_3216: mg_up<Tile3216>(H, l, xin, C, xout, smem, nullptr); break;
+            case SHAPE_16: mg_up<Tile16>(H, l, xin, C, xout, smem, nullptr); break;
+            case SHAPE_8: mg_up<Tile8>(H, l, xin, C, xout, smem, nullptr); break;
+            default: mg_up<Tile32>(H, l, xin, C, xout, smem, nullptr); break;
+        }
         ok = grid_sync(H);
     }
     return x0;
@@ -966,11 +979,29 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     const bool grid_levels = kind == HK_MULTIGRID && H.n_levels >= 2 && H.coarse_from >= 1;
     const long long tiles32 = (long long)((nx + 31) / 32) * ((ny + 31) / 32);
     H.wide0 = (grid_levels && nx % TileWide::TX == 0 && tiles32 > sms) ? 1 : 0;
+    // every other grid level takes the smallest tile whose count fits one round
+    // over the SMs: the phases are latency-bound, so less work per CTA is faster
+    // as long as no CTA takes a second tile
+    int max_rn = Tile32::RN;
+    for (int l = 0; l < H.n_levels; ++l) {
+        HLevel& L = H.lv[l];
+        L.shape = SHAPE_32;
+        if (kind != HK_MULTIGRID) continue;
+        if (l == 0 && H.wide0) {
+            L.shape = SHAPE_WIDE;
+            max_rn = std::max(max_rn, TileWide::RN);
+            continue;
+        }
+        auto count = [&](int tx, int ty) { return (long long)((L.nx + tx - 1) / tx) * ((L.ny + ty - 1) / ty); };
+        if (count(8, 8) <= sms) L.shape = SHAPE_8;
+        else if (count(16, 16) <= sms) L.shape = SHAPE_16;
+        else if (count(32, 16) <= sms) L.shape = SHAPE_3216;
+    }
     bool aligned = H.n_leaves > 0;
     for (int q = 0; q < H.n_leaves && aligned; ++q)
         aligned = leaves[q] == 128 * q && leaves[q + 1] - leaves[q] == 128;
     H.fused_res = (H.wide0 && aligned) ? 1 : 0;
-    const size_t tile_work = 6 * (size_t)(H.wide0 ? std::max(TileWide::RN, Tile32::RN) : Tile32::RN);
+    const size_t tile_work = 6 * (size_t)max_rn;
     const size_t mg_work = (kind == HK_MULTIGRID) ? std::max<size_t>(tile_work, 6 * coarse_cells) : 0;
     // the tree fold and the V-cycle never run at the same time: one region serves both
     smem_ = sizeof(double) * std::max<size_t>((size_t)H.n_leaves, mg_work);

@@ -11,6 +11,7 @@ enum { HK_PCG_JACOBI = 0, HK_PCG_RBGS = 1, HK_RBGS = 2, HK_MULTIGRID = 3 };
 
 struct HLevel {
     int nx, ny, n;
+    int shape;        // tile shape of the level's grid phases
     double dx2, dy2;  // dx**2, dy**2 of the level
     double cx, cy;    // coef * (1 / dx**2)
     const double* mask;
