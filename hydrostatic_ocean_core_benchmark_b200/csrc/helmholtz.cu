@@ -429,6 +429,14 @@ struct CoarseRefs {
     double *x, *b, *ku, *kv, *id, *m;
 };
 
+// the coarse levels' arrays take 6 x (sum of their cells) doubles; the restriction
+// scratch (one value per cell of the first coarse level) follows them
+__device__ __forceinline__ double* coarse_scratch(const HelmParams& H, double* base) {
+    int tot = 0;
+    for (int q = H.coarse_from; q < H.n_levels; ++q) tot += H.lv[q].n;
+    return base + 6 * tot;
+}
+
 __device__ __forceinline__ CoarseRefs coarse_refs(const HelmParams& H, double* base, int l) {
     int off = 0, tot = 0;
     for (int q = H.coarse_from; q < H.n_levels; ++q) {
@@ -445,26 +453,45 @@ __device__ __forceinline__ CoarseRefs coarse_refs(const HelmParams& H, double* b
     return c;
 }
 
+// Gauss-Seidel update of coarse cell (i, j) = e; with C, the neighbours carry
+// the coarse correction x + prolong(e) * mask (the first reverse half-sweep)
+__device__ __forceinline__ void coarse_cell_update(const HLevel& L, CoarseRefs s, int i, int j, int e,
+                                                   const CoarseRefs* C, const HLevel* LC) {
+    const int nx = L.nx;
+    const int i_e = i + 1 == nx ? 0 : i + 1, i_w = i == 0 ? nx - 1 : i - 1;
+    const int j_n = j + 1 == L.ny ? 0 : j + 1, j_s = j == 0 ? L.ny - 1 : j - 1;
+    const int ie = j * nx + i_e, iw = j * nx + i_w, jn = j_n * nx + i, js = j_s * nx + i;
+    double xe = s.x[ie], xw = s.x[iw], xn = s.x[jn], xs = s.x[js];
+    if (C) {
+        const int cnx = LC->nx;
+        xe = xe + C->x[(j >> 1) * cnx + (i_e >> 1)] * s.m[ie];
+        xw = xw + C->x[(j >> 1) * cnx + (i_w >> 1)] * s.m[iw];
+        xn = xn + C->x[(j_n >> 1) * cnx + (i >> 1)] * s.m[jn];
+        xs = xs + C->x[(j_s >> 1) * cnx + (i >> 1)] * s.m[js];
+    }
+    const double nb = L.cx * (s.ku[e] * xe + s.ku[iw] * xw) + L.cy * (s.kv[e] * xn + s.kv[js] * xs);
+    s.x[e] = s.id[e] * (s.b[e] + nb) * s.m[e];
+}
+
+// one colour of a coarse-level sweep by the CTA. On even-sized levels only the
+// cells of that colour are visited (cell q of the colour: row q / (nx/2), column
+// 2 (q mod nx/2) + the row's parity offset); odd-sized levels test each cell.
 __device__ void coarse_half_sweep(const HLevel& L, CoarseRefs s, int colour, const CoarseRefs* C,
                                   const HLevel* LC) {
-    for (int e = threadIdx.x; e < L.n; e += blockDim.x) {
-        const int j = e / L.nx, i = e - j * L.nx;
-        if (((i + j) & 1) != colour) continue;
-        const int ie = j * L.nx + (i + 1 == L.nx ? 0 : i + 1), iw = j * L.nx + (i == 0 ? L.nx - 1 : i - 1);
-        const int jn = (j + 1 == L.ny ? 0 : j + 1) * L.nx + i, js = (j == 0 ? L.ny - 1 : j - 1) * L.nx + i;
-        double xe = s.x[ie], xw = s.x[iw], xn = s.x[jn], xs = s.x[js];
-        if (C) {  // neighbours after the coarse correction x + prolong(e) * mask
-            auto corr = [&](int q) {
-                const int qj = q / L.nx, qi = q - qj * L.nx;
-                return C->x[(qj >> 1) * LC->nx + (qi >> 1)] * s.m[q];
-            };
-            xe = xe + corr(ie);
-            xw = xw + corr(iw);
-            xn = xn + corr(jn);
-            xs = xs + corr(js);
+    const int nx = L.nx;
+    if (((nx | L.ny) & 1) == 0) {
+        const int hx = nx >> 1, nh = L.n >> 1;
+        for (int q = threadIdx.x; q < nh; q += blockDim.x) {
+            const int j = q / hx;
+            const int i = 2 * (q - j * hx) + ((j + colour) & 1);
+            coarse_cell_update(L, s, i, j, j * nx + i, C, LC);
         }
-        const double nb = L.cx * (s.ku[e] * xe + s.ku[iw] * xw) + L.cy * (s.kv[e] * xn + s.kv[js] * xs);
-        s.x[e] = s.id[e] * (s.b[e] + nb) * s.m[e];
+    } else {
+        for (int e = threadIdx.x; e < L.n; e += blockDim.x) {
+            const int j = e / nx, i = e - j * nx;
+            if (((i + j) & 1) != colour) continue;
+            coarse_cell_update(L, s, i, j, e, C, LC);
+        }
     }
     __syncthreads();
 }
@@ -507,16 +534,18 @@ __device__ void mg_coarse(const HelmParams& H, double* smem, const double* xin_c
         CoarseRefs s = coarse_refs(H, smem, l);
         for (int h = 0; h < 4; ++h) coarse_half_sweep(L, s, h & 1, nullptr, nullptr);
         if (l + 1 < nl) {
+            // the residual of every cell of level l (a coarser level exists only
+            // below an even-sized one, so they are exactly the 2x2 children),
+            // then the children's mean per coarse cell
             const HLevel& C = H.lv[l + 1];
             CoarseRefs c = coarse_refs(H, smem, l + 1);
+            double* res = coarse_scratch(H, smem);
+            for (int f = threadIdx.x; f < L.n; f += blockDim.x) res[f] = coarse_residual(L, H.coef, s, f);
+            __syncthreads();
             for (int e = threadIdx.x; e < C.n; e += blockDim.x) {
                 const int J = e / C.nx, I = e - J * C.nx;
                 const int f00 = (2 * J) * L.nx + 2 * I;
-                const double a = coarse_residual(L, H.coef, s, f00);
-                const double b = coarse_residual(L, H.coef, s, f00 + 1);
-                const double cc = coarse_residual(L, H.coef, s, f00 + L.nx);
-                const double d = coarse_residual(L, H.coef, s, f00 + L.nx + 1);
-                c.b[e] = 0.25 * (a + b + cc + d);
+                c.b[e] = 0.25 * (res[f00] + res[f00 + 1] + res[f00 + L.nx] + res[f00 + L.nx + 1]);
                 c.x[e] = 0.0;
             }
             __syncthreads();
@@ -1002,7 +1031,8 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
         aligned = leaves[q] == 128 * q && leaves[q + 1] - leaves[q] == 128;
     H.fused_res = (H.wide0 && aligned) ? 1 : 0;
     const size_t tile_work = 6 * (size_t)max_rn;
-    const size_t mg_work = (kind == HK_MULTIGRID) ? std::max<size_t>(tile_work, 6 * coarse_cells) : 0;
+    const size_t coarse_work = 6 * coarse_cells + (H.coarse_from < H.n_levels ? (size_t)H.lv[H.coarse_from].n : 0);
+    const size_t mg_work = (kind == HK_MULTIGRID) ? std::max<size_t>(tile_work, coarse_work) : 0;
     // the tree fold and the V-cycle never run at the same time: one region serves both
     smem_ = sizeof(double) * std::max<size_t>((size_t)H.n_leaves, mg_work);
     if (smem_ > 200 * 1024) {
