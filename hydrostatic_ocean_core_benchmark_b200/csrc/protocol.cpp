@@ -266,9 +266,13 @@ extern "C" int oc_run_namelist(const char* nml_path) {
     bool run_diverged = false;
     for (int rep = 0; rep < n_warmup && !run_diverged; ++rep) {
         if ((rc = oc_reset_mixing(h)) || (rc = oc_set_state(h, &init, 0))) break;
-        for (int s = 0; s < n_steps; ++s) {
-            if ((rc = oc_step(h, 1, nullptr))) break;
-            if (s % 10 == 9 && diverged()) {
+        for (int s = 0; s < n_steps;) {
+            // chunks of up to ten steps, replayed as CUDA graphs, ending where the
+            // reference checks for divergence (every tenth step)
+            const int chunk = std::min(10 - s % 10, n_steps - s);
+            if ((rc = oc_step_graph(h, chunk, nullptr))) break;
+            s += chunk;
+            if (s % 10 == 0 && diverged()) {
                 run_diverged = true;
                 break;
             }
@@ -284,9 +288,13 @@ extern "C" int oc_run_namelist(const char* nml_path) {
         oc_reset_stats(h);
         cudaDeviceSynchronize();
         const auto t0 = std::chrono::steady_clock::now();
-        for (int s = 0; s < n_steps; ++s) {
-            if ((rc = oc_step(h, 1, nullptr))) break;
-            if (s % 10 == 9 && diverged()) {
+        for (int s = 0; s < n_steps;) {
+            // chunks of up to ten steps, replayed as CUDA graphs, ending where the
+            // reference checks for divergence (every tenth step)
+            const int chunk = std::min(10 - s % 10, n_steps - s);
+            if ((rc = oc_step_graph(h, chunk, nullptr))) break;
+            s += chunk;
+            if (s % 10 == 0 && diverged()) {
                 run_diverged = true;
                 break;
             }
