@@ -266,23 +266,60 @@ __device__ __forceinline__ TileRefs tile_refs(double* base) {
 
 // load a tile region of level L whose interior starts at (i0, j0); x from xin
 // (or zero), plus the coarse correction e * mask when C is given
+// (with `coef` false the coefficients ku, kv, id, m are already in place)
 template <class S>
 __device__ void tile_load(const HLevel& L, int i0, int j0, const double* xin, const HLevel* C,
-                          TileRefs t) {
+                          TileRefs t, bool coef = true) {
 #pragma unroll 4
     for (int r = threadIdx.x; r < S::RN; r += blockDim.x) {
         const int rj = r / S::RW, ri = r - rj * S::RW;
         const int gi = wrap_any(i0 - HALO + ri, L.nx), gj = wrap_any(j0 - HALO + rj, L.ny);
         const int g = gj * L.nx + gi;
-        const double m = L.mask[g];
+        const double m = coef ? L.mask[g] : t.m[r];
         double x = xin ? __ldcg(xin + g) : 0.0;
         if (C) x = x + __ldcg(C->x + (gj >> 1) * C->nx + (gi >> 1)) * m;
         t.x[r] = x;
         t.b[r] = __ldcg(L.b + g);
-        t.ku[r] = L.Ku[g];
-        t.kv[r] = L.Kv[g];
-        t.id[r] = L.inv_diag[g];
-        t.m[r] = m;
+        if (coef) {
+            t.ku[r] = L.Ku[g];
+            t.kv[r] = L.Kv[g];
+            t.id[r] = L.inv_diag[g];
+            t.m[r] = m;
+        }
+    }
+    __syncthreads();
+}
+
+// Level 0's coefficients stay in shared memory for a whole solve when every
+// level-0 tile has a CTA of its own (H.persist0): the first RN x 4 doubles hold
+// the CTA's tile's ku, kv, id and m, and the tile phases of level 0 load only x
+// and b. Everything else works above them.
+template <class S>
+__device__ __forceinline__ TileRefs tile_refs_persist(double* persist, double* work) {
+    TileRefs t;
+    t.ku = persist;
+    t.kv = persist + S::RN;
+    t.id = persist + 2 * S::RN;
+    t.m = persist + 3 * S::RN;
+    t.x = work;
+    t.b = work + S::RN;
+    return t;
+}
+
+__device__ void persist_level0(const HelmParams& H, double* persist) {
+    using S = TileWide;
+    const HLevel& L = H.lv[0];
+    const int tx = (L.nx + S::TX - 1) / S::TX;
+    const int tile = blockIdx.x;
+    if (tile >= tx * ((L.ny + S::TY - 1) / S::TY)) return;
+    const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
+    for (int r = threadIdx.x; r < S::RN; r += blockDim.x) {
+        const int rj = r / S::RW, ri = r - rj * S::RW;
+        const int g = wrap_any(j0 - HALO + rj, L.ny) * L.nx + wrap_any(i0 - HALO + ri, L.nx);
+        persist[r] = L.Ku[g];
+        persist[S::RN + r] = L.Kv[g];
+        persist[2 * S::RN + r] = L.inv_diag[g];
+        persist[3 * S::RN + r] = L.mask[g];
     }
     __syncthreads();
 }
@@ -362,14 +399,16 @@ __device__ void tile_store_x(const HLevel& L, int i0, int j0, TileRefs t, double
 // down phase of level l: pre-smoothing, restricted residual into level l+1
 // (solvers_var.py:141-147); x of level l+1 starts at zero implicitly
 template <class S>
-__device__ void mg_down(const HelmParams& H, int l, const double* xin, double* xout, double* smem) {
+__device__ void mg_down(const HelmParams& H, int l, const double* xin, double* xout, double* smem,
+                        double* persist = nullptr) {
     const HLevel& L = H.lv[l];
     const HLevel& C = H.lv[l + 1];
     const int tx = (L.nx + S::TX - 1) / S::TX, ty = (L.ny + S::TY - 1) / S::TY;
-    TileRefs t = tile_refs<S>(smem);
+    const bool keep = persist != nullptr;
+    TileRefs t = keep ? tile_refs_persist<S>(persist, smem) : tile_refs<S>(smem);
     for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
         const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
-        tile_load<S>(L, i0, j0, xin, nullptr, t);
+        tile_load<S>(L, i0, j0, xin, nullptr, t, !keep);
         tile_four_half_sweeps<S>(L, i0, j0, t, 0);
         for (int r = threadIdx.x; r < (S::TX / 2) * (S::TY / 2); r += blockDim.x) {
             const int cj = r / (S::TX / 2), ci = r - cj * (S::TX / 2);
@@ -395,13 +434,14 @@ __device__ void mg_down(const HelmParams& H, int l, const double* xin, double* x
 // -- the per-cycle residual norm without another pass over the grid.
 template <class S>
 __device__ void mg_up(const HelmParams& H, int l, const double* xin, const HLevel& C, double* xout,
-                      double* smem, double* leaves) {
+                      double* smem, double* leaves, double* persist = nullptr) {
     const HLevel& L = H.lv[l];
     const int tx = (L.nx + S::TX - 1) / S::TX, ty = (L.ny + S::TY - 1) / S::TY;
-    TileRefs t = tile_refs<S>(smem);
+    const bool keep = persist != nullptr;
+    TileRefs t = keep ? tile_refs_persist<S>(persist, smem) : tile_refs<S>(smem);
     for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
         const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
-        tile_load<S>(L, i0, j0, xin, &C, t);
+        tile_load<S>(L, i0, j0, xin, &C, t, !keep);
         tile_four_half_sweeps<S>(L, i0, j0, t, 1);
         tile_store_x<S>(L, i0, j0, t, xout);
         if constexpr (S::TX == 128) {
@@ -591,7 +631,7 @@ __device__ void mg_smooth(const HelmParams& H, int l, const double* xin, double*
 // new x (x0 or level 0's second buffer). Levels below coarse_from have a grid
 // down and up phase; the rest run in CTA 0, or, when every level is too large
 // for it, the coarsest level is smoothed on the grid.
-__device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, bool& ok) {
+__device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, double* persist, bool& ok) {
     const int cf = H.coarse_from, nl = H.n_levels;
     double* x0b = (x0 == H.lv[0].x) ? H.lv[0].x2 : H.lv[0].x;
     if (cf == 0) {
@@ -604,7 +644,7 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, b
         const double* xin = l == 0 ? x0 : nullptr;
         double* xout = l == 0 ? x0b : H.lv[l].x;
         switch (H.lv[l].shape) {
-            case SHAPE_WIDE: mg_down<TileWide>(H, l, xin, xout, smem); break;
+            case SHAPE_WIDE: mg_down<TileWide>(H, l, xin, xout, smem, l == 0 ? persist : nullptr); break;
             case SHAPE_3216: mg_down<Tile3216>(H, l, xin, xout, smem); break;
             case SHAPE_16: mg_down<Tile16>(H, l, xin, xout, smem); break;
             case SHAPE_8: mg_down<Tile8>(H, l, xin, xout, smem); break;
@@ -634,7 +674,9 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, b
         HLevel C = H.lv[l + 1];
         C.x = H.lv[l + 1].x2;
         switch (H.lv[l].shape) {
-            case SHAPE_WIDE: mg_up<TileWide>(H, l, xin, C, xout, smem, H.fused_res ? H.leafA : nullptr); break;
+            case SHAPE_WIDE:
+                mg_up<TileWide>(H, l, xin, C, xout, smem, H.fused_res ? H.leafA : nullptr, l == 0 ? persist : nullptr);
+                break;
             case SHAPE_3216: mg_up<Tile3216>(H, l, xin, C, xout, smem, nullptr); break;
             case SHAPE_16: mg_up<Tile16>(H, l, xin, C, xout, smem, nullptr); break;
             case SHAPE_8: mg_up<Tile8>(H, l, xin, C, xout, smem, nullptr); break;
@@ -647,7 +689,11 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, b
 
 // ------------------------------------------------------------------ the solve kernel
 __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
-    extern __shared__ double sm[];
+    extern __shared__ double smem_all[];
+    // with H.persist0 the first 4 RN doubles hold level 0's coefficient tile for the
+    // whole solve; every other use of shared memory works above them
+    double* persist = H.persist0 ? smem_all : nullptr;
+    double* sm = H.persist0 ? smem_all + 4 * TileWide::RN : smem_all;
     const HLevel& L0 = H.lv[0];
     const double* rhs = H.rhs;
     double* x = L0.x;
@@ -667,6 +713,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                H.leafA, nullptr);
     ok = grid_sync(H);
     const double norm_b = ok ? sqrt(tree_fold(H, H.leafA, sm)) : 0.0;
+    if (persist) persist_level0(H, persist);  // the coefficients are fixed during the solve
     if (!ok || norm_b == 0.0) goto done;
     {
         const double tol = H.rtol * norm_b;
@@ -676,7 +723,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
             double* xc = x;  // the level-0 buffer holding the current iterate
             for (int it = 1; it <= H.max_iter && ok; ++it) {
                 if (H.kind == HK_MULTIGRID) {
-                    xc = vcycle_tiled(H, xc, sm, ok);
+                    xc = vcycle_tiled(H, xc, sm, persist, ok);
                 } else {
                     colour_phase(L0, x, b0, 0, grid_team());
                     ok = grid_sync(H);
@@ -1011,14 +1058,12 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     // every other grid level takes the smallest tile whose count fits one round
     // over the SMs: the phases are latency-bound, so less work per CTA is faster
     // as long as no CTA takes a second tile
-    int max_rn = Tile32::RN;
     for (int l = 0; l < H.n_levels; ++l) {
         HLevel& L = H.lv[l];
         L.shape = SHAPE_32;
         if (kind != HK_MULTIGRID) continue;
         if (l == 0 && H.wide0) {
             L.shape = SHAPE_WIDE;
-            max_rn = std::max(max_rn, TileWide::RN);
             continue;
         }
         auto count = [&](int tx, int ty) { return (long long)((L.nx + tx - 1) / tx) * ((L.ny + ty - 1) / ty); };
@@ -1026,16 +1071,39 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
         else if (count(16, 16) <= sms) L.shape = SHAPE_16;
         else if (count(32, 16) <= sms) L.shape = SHAPE_3216;
     }
+    // level 0's coefficients persist in shared memory when each wide tile has its own CTA
+    const long long wide_tiles = (long long)((nx + TileWide::TX - 1) / TileWide::TX) * ((ny + TileWide::TY - 1) / TileWide::TY);
+    H.persist0 = (H.wide0 && wide_tiles <= sms) ? 1 : 0;
     bool aligned = H.n_leaves > 0;
     for (int q = 0; q < H.n_leaves && aligned; ++q)
         aligned = leaves[q] == 128 * q && leaves[q + 1] - leaves[q] == 128;
     H.fused_res = (H.wide0 && aligned) ? 1 : 0;
-    const size_t tile_work = 6 * (size_t)max_rn;
+    // shared memory: the persistent tile (if any), then the largest of the tree
+    // fold, the grid levels' tiles and the coarse levels of CTA 0
+    size_t tile_work = 0;
+    const int n_grid = H.coarse_from < H.n_levels ? H.coarse_from : H.n_levels;
+    auto rn_of = [](int shape) {
+        switch (shape) {
+            case SHAPE_WIDE: return TileWide::RN;
+            case SHAPE_3216: return Tile3216::RN;
+            case SHAPE_16: return Tile16::RN;
+            case SHAPE_8: return Tile8::RN;
+            default: return Tile32::RN;
+        }
+    };
+    if (kind == HK_MULTIGRID) {
+        for (int l = 0; l < n_grid; ++l)
+            tile_work = std::max<size_t>(tile_work, (l == 0 && H.persist0 ? 2 : 6) * (size_t)rn_of(H.lv[l].shape));
+        if (H.coarse_from >= H.n_levels) tile_work = std::max<size_t>(tile_work, 6 * (size_t)Tile32::RN);
+    }
     const size_t coarse_work = 6 * coarse_cells + (H.coarse_from < H.n_levels ? (size_t)H.lv[H.coarse_from].n : 0);
     const size_t mg_work = (kind == HK_MULTIGRID) ? std::max<size_t>(tile_work, coarse_work) : 0;
     // the tree fold and the V-cycle never run at the same time: one region serves both
-    smem_ = sizeof(double) * std::max<size_t>((size_t)H.n_leaves, mg_work);
-    if (smem_ > 200 * 1024) {
+    smem_ = sizeof(double) * ((H.persist0 ? 4 * (size_t)TileWide::RN : 0) +
+                              std::max<size_t>((size_t)H.n_leaves, mg_work));
+    int smem_optin = 0;
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem_ > (size_t)smem_optin) {
         err = "Helmholtz grid too large for the single-pass reduction tree";
         return OC_ERR_UNSUPPORTED;
     }
