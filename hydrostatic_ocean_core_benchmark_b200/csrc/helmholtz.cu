@@ -134,12 +134,6 @@ __device__ __forceinline__ Team grid_team() {
     return t;
 }
 
-__device__ __forceinline__ Team block_team() {
-    Team t;
-    t.first = threadIdx.x;
-    t.stride = blockDim.x;
-    return t;
-}
 
 // one colour of a Gauss-Seidel sweep; the cell mask multiply of the sweep end
 // is folded into each assignment (identical for wet cells, 0 for dry ones)

@@ -151,36 +151,12 @@ __device__ __forceinline__ double col_above(const KP& P, int c, int k) {
     return above;
 }
 
-__device__ __forceinline__ double col_zc(const KP& P, int c, int k) {
-    double m3;
-    const double dz = col_dz(P, c, k, m3);
-    return col_above(P, c, k) + 0.5 * dz;
-}
 
 __device__ __forceinline__ double face_combine(const KP& P, double a, double b) {
     if (P.face_rule == 0) return fmin(a, b);
     if (P.face_rule == 1) return 0.5 * (a + b);
     double tot = a + b;
     return tot > 0.0 ? 2.0 * a * b / tot : 0.0;
-}
-
-// Geometry of one column and its face toward a neighbour column at level k.
-struct CellGeo {
-    double dz, m3;
-};
-
-__device__ __forceinline__ CellGeo cell_geo(const KP& P, int c2, int k) {
-    CellGeo g;
-    g.dz = col_dz(P, c2, k, g.m3);
-    return g;
-}
-
-// face mask and face thickness between cell a and its +1 neighbour b, with the
-// 2D face mask mf (reference domain.py:93-96, 142-146)
-__device__ __forceinline__ void face_geo(const KP& P, const CellGeo& a, const CellGeo& b, double mf,
-                                         double& m3f, double& dzf) {
-    m3f = a.m3 * b.m3 * mf;
-    dzf = m3f * face_combine(P, a.dz, b.dz);
 }
 
 // Superbee limiter of the TVD face (reference advection_v06.py:35-43)

@@ -1,23 +1,26 @@
 // Column and stencil kernels of the ocean-core step (sm_100a, fp64).
 //
-// Each kernel maps one thread to one water column (i, j) and marches over the
-// levels k, so every vertical recurrence of the reference (cumulative sums,
-// Thomas sweeps, the closure's mixing-length marches) runs in registers and
-// local memory in the reference's order, while the 32 threads of a warp read
-// 32 consecutive i of each level plane (coalesced 256-byte rows).
+// The column kernels map one thread to one water column (i, j) and march over
+// the levels k, so every vertical recurrence of the reference (cumulative sums,
+// Thomas sweeps, the closure's mixing-length marches) runs in the reference's
+// order; the 32 threads of a warp read 32 consecutive i of each level plane
+// (coalesced 256-byte rows). The stencil kernels (k_mom_column, k_tracer_rhs,
+// k_predictor_rhs) work on tiles of columns over a range of levels.
 //
 // Reference correspondence (paths inside the reference project):
-//   k_closure        libs/core/closure.py:43-205 + model3d_v05.py:141-157 (q = A^-1 1)
-//   k_qsolve         model3d_v05.py:147-153 (constant-coefficient q)
-//   k_kukv           model3d_v05.py:154-157
-//   k_wcol           vertical_var.py:109-121 + model3d_v05.py:232-235
-//   k_phi            vertical_var.py:132-145
-//   k_mom_explicit   model3d_v05.py:195-230, 241-260, 352-370; advection_v06.py:77-108;
-//                    advection.py:62-95; operators_masked.py:45-68; vertical_var.py:80-106
-//   k_predictor      model3d_v05.py:387-395, 426-433 + vertical.py:17-44
-//   k_backsub        model3d_v05.py:404-406
-//   k_tracers        model3d_v05.py:466-533 + eos.py:68-133
-//   2D kernels       model3d_v05.py:290-335, 376-384, 396-400, 410-413, 440-461
+//   k_closure         libs/core/closure.py:43-205 + model3d_v05.py:141-157 (q = A^-1 1)
+//   k_qsolve          model3d_v05.py:147-153 (constant-coefficient q)
+//   k_kukv            model3d_v05.py:154-157
+//   k_wcol            vertical_var.py:109-121 + model3d_v05.py:232-235
+//   k_phi             vertical_var.py:132-145
+//   k_mom_column      model3d_v05.py:195-230, 241-260, 352-370; advection_v06.py:77-108;
+//                     advection.py:62-95; operators_masked.py:45-68; vertical_var.py:80-106
+//   k_predictor_rhs   model3d_v05.py:387-393
+//   k_momentum_solve  model3d_v05.py:394-395, 426-433 + vertical.py:17-44
+//   k_backsub         model3d_v05.py:404-406
+//   k_tracer_rhs      model3d_v05.py:466-512
+//   k_tracer_solve    model3d_v05.py:514-533 + eos.py:68-133
+//   2D kernels        model3d_v05.py:290-335, 376-384, 396-400, 410-413, 440-461
 
 #include "oc_internal.cuh"
 #include "step_kernels.cuh"
@@ -74,24 +77,6 @@ struct Nbr {
     __device__ __forceinline__ int at(int dj, int di) const { return jy[dj + 3] + ix[di + 3]; }
 };
 
-__device__ __forceinline__ CellGeo geo_off(const KP& P, const Nbr& n, int dj, int di, int k) {
-    return cell_geo(P, n.at(dj, di), k);
-}
-
-// east face of column (j+dj, i+di): wet mask and thickness at level k
-__device__ __forceinline__ void ufacek(const KP& P, const Nbr& n, int dj, int di, int k, double& m3f,
-                                       double& dzf) {
-    const CellGeo a = geo_off(P, n, dj, di, k), b = geo_off(P, n, dj, di + 1, k);
-    face_geo(P, a, b, P.mask_u[n.at(dj, di)], m3f, dzf);
-}
-
-// north face of column (j+dj, i+di)
-__device__ __forceinline__ void vfacek(const KP& P, const Nbr& n, int dj, int di, int k, double& m3f,
-                                       double& dzf) {
-    const CellGeo a = geo_off(P, n, dj, di, k), b = geo_off(P, n, dj + 1, di, k);
-    face_geo(P, a, b, P.mask_v[n.at(dj, di)], m3f, dzf);
-}
-
 __device__ __forceinline__ double m3u_at(const KP& P, const Nbr& n, int dj, int di, int k) {
     return col_m3u(P, n.at(dj, di), k);
 }
@@ -101,11 +86,12 @@ __device__ __forceinline__ double m3v_at(const KP& P, const Nbr& n, int dj, int 
 }
 
 __device__ __forceinline__ double m3_at(const KP& P, const Nbr& n, int dj, int di, int k) {
-    return geo_off(P, n, dj, di, k).m3;
+    return col_m3(P, n.at(dj, di), k);
 }
 
 // face thickness at level k of a face whose wet levels are the top kf ones,
-// between cells of thickness dza and dzb (equals face_geo's dzf)
+// between cells of thickness dza and dzb: mask3_face x face_combine(dza, dzb)
+// (reference domain.py:93-96, 142-146)
 __device__ __forceinline__ double face_dz(const KP& P, int kf, int k, double dza, double dzb) {
     return (k < kf ? 1.0 : 0.0) * face_combine(P, dza, dzb);
 }
