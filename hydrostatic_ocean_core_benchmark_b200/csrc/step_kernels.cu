@@ -1026,9 +1026,16 @@ __global__ void __launch_bounds__(TRX * TRY, 4) k_tracer_rhs(KP P, const double*
                                                              const double* __restrict__ kh,
                                                              double* __restrict__ rT,
                                                              double* __restrict__ rS) {
-    __shared__ double sfx[2][2][TRY][TRX + 1];  // [buffer][field][row][west face of column]
-    __shared__ double sfy[2][2][TRY + 1][TRX];  // [buffer][field][south face of row][column]
+    // the tile's columns plus a 2-column ring: flat 2D index and compact geometry
+    // (once), then each level's tracers and face velocities (staged per level)
+    constexpr int RX = TRX + 4, RY = TRY + 4, RNC = RX * RY;
+    __shared__ int s_g[RNC], s_kf[RNC], s_kb[RNC], s_ku[RNC], s_kv[RNC];
+    __shared__ double s_d0[RNC], s_d1[RNC];
+    __shared__ double s_f[2][RNC], s_u[RNC], s_v[RNC];
+    __shared__ double sfx[2][TRY][TRX + 1];  // [field][row][west face of column]
+    __shared__ double sfy[2][TRY + 1][TRX];  // [field][south face of row][column]
     const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tid = ty * TRX + tx;
     const int i0 = blockIdx.x * TRX, j0 = blockIdx.y * TRY;
     const int i = i0 + tx, j = j0 + ty;
     const int nx = P.nx, ny = P.ny, nz = P.nz;
@@ -1046,6 +1053,48 @@ __global__ void __launch_bounds__(TRX * TRY, 4) k_tracer_rhs(KP P, const double*
     const ColGeo g = ColGeo::load(P, c);
     const double* __restrict__ C0 = ts ? T : bold;
     double* __restrict__ R0 = rT;
+    for (int r = tid; r < RNC; r += TRX * TRY) {
+        const int rj = r / RX, ri = r - rj * RX;
+        const int gc = wrapi(j0 - 2 + rj, ny) * nx + wrapi(i0 - 2 + ri, nx);
+        const int2 ki = P.kinfo[gc], kfc = P.kface[gc];
+        const double2 dx = P.dzx[gc];
+        s_g[r] = gc;
+        s_kf[r] = ki.x;
+        s_kb[r] = ki.y;
+        s_ku[r] = kfc.x;
+        s_kv[r] = kfc.y;
+        s_d0[r] = dx.x;
+        s_d1[r] = dx.y;
+    }
+    // thickness and wet flag of region column r at level k (col_dz from the staged geometry)
+    auto sdz = [&](int r, int k, double& m3) {
+        if (k >= s_kb[r]) {
+            m3 = 0.0;
+            return 0.0;
+        }
+        m3 = 1.0;
+        if (k < s_kf[r]) return P.dzr[k];
+        return k == s_kf[r] ? s_d0[r] : s_d1[r];
+    };
+    // flux through a face with stencil cells (cm, c0, c1, cp) of the region,
+    // normal velocity vel and face wet levels kfa (tracer_flux from shared memory)
+    auto sflux = [&](const double* F, int cm, int c0, int c1, int cp, double vel, int kfa, int k) {
+        double m;
+        const double dzf = face_dz(P, kfa, k, sdz(c0, k, m), sdz(c1, k, m));
+        const double a = F[c0], b = F[c1];
+        double val;
+        if (P.advection == 1)
+            val = 0.5 * (a + b);
+        else if (P.advection >= 3)
+            val = kappa_face(P, F[cm], a, b, F[cp], vel, k < s_kb[cm] ? 1.0 : 0.0, k < s_kb[cp] ? 1.0 : 0.0,
+                             P.advection == 4);
+        else
+            val = vel > 0.0 ? a : b;
+        return dzf * vel * val;
+    };
+    const int rc = (ty + 2) * RX + tx + 2;                    // this thread's cell in the region
+    const int rce = (tx + 2) * RX + TRX + 1;                  // east-column cell of row tx (x extras)
+    const int rcn = (TRY + 1) * RX + tx + 2;                  // north-row cell of column tx (y extras)
     // rolling column values of each field at k-1, k, k+1 and the face at the top of level k
     double fm1[2] = {0.0, 0.0}, f0[2] = {0.0, 0.0}, fp1[2] = {0.0, 0.0}, ftop[2] = {0.0, 0.0};
     double w_k = 0.0, kh_k = 0.0;
@@ -1064,16 +1113,27 @@ __global__ void __launch_bounds__(TRX * TRY, 4) k_tracer_rhs(KP P, const double*
         kh_k = kh[(size_t)kbeg * n2 + c];
     }
     for (int k = kbeg; k < kend; ++k) {
-        const int buf = (k - kbeg) & 1;
         const size_t o = (size_t)k * n2;
         if (adv) {
+            // stage the level (the previous level's faces and cells are done)
+            __syncthreads();
+            for (int r = tid; r < RNC; r += TRX * TRY) {
+                const size_t g = o + s_g[r];
+                s_f[0][r] = C0[g];
+                if (ts) s_f[1][r] = S[g];
+                s_u[r] = u[g];
+                s_v[r] = v[g];
+            }
+            __syncthreads();
 #pragma unroll 1
             for (int f = 0; f < nf; ++f) {
-                const double* __restrict__ C = f == 0 ? C0 : S;
-                sfx[buf][f][ty][tx] = tracer_flux(P, C, u, o, xstencil(j, i - 1, nx, ny), k, 0);
-                sfy[buf][f][ty][tx] = tracer_flux(P, C, v, o, ystencil(j - 1, i, nx, ny), k, 1);
-                if (xextra) sfx[buf][f][tx][TRX] = tracer_flux(P, C, u, o, xstencil(j0 + tx, i0 + TRX - 1, nx, ny), k, 0);
-                if (yextra) sfy[buf][f][TRY][tx] = tracer_flux(P, C, v, o, ystencil(j0 + TRY - 1, i, nx, ny), k, 1);
+                const double* F = s_f[f];
+                // west face of this cell (cells rc-2 .. rc+1), south face (rc-2RX .. rc+RX)
+                sfx[f][ty][tx] = sflux(F, rc - 2, rc - 1, rc, rc + 1, s_u[rc - 1], s_ku[rc - 1], k);
+                sfy[f][ty][tx] = sflux(F, rc - 2 * RX, rc - RX, rc, rc + RX, s_v[rc - RX], s_kv[rc - RX], k);
+                if (xextra) sfx[f][tx][TRX] = sflux(F, rce - 1, rce, rce + 1, rce + 2, s_u[rce], s_ku[rce], k);
+                if (yextra)
+                    sfy[f][TRY][tx] = sflux(F, rcn - RX, rcn, rcn + RX, rcn + 2 * RX, s_v[rcn], s_kv[rcn], k);
             }
             __syncthreads();
         }
@@ -1097,8 +1157,8 @@ __global__ void __launch_bounds__(TRX * TRY, 4) k_tracer_rhs(KP P, const double*
             double fbot = 0.0;
             if (adv) {
                 fbot = tracer_vface(P, g, k + 1, fm1[f], f0[f], fp1[f], fp2, w_k1);
-                const double hdiv = ((sfx[buf][f][ty][tx + 1] - sfx[buf][f][ty][tx]) / P.dx +
-                                     (sfy[buf][f][ty + 1][tx] - sfy[buf][f][ty][tx]) / P.dy) *
+                const double hdiv = ((sfx[f][ty][tx + 1] - sfx[f][ty][tx]) / P.dx +
+                                     (sfy[f][ty + 1][tx] - sfy[f][ty][tx]) / P.dy) *
                                     inv;
                 const double vdiv = (w_k * ftop[f] - w_k1 * fbot) * inv;
                 tend = tend - (hdiv + vdiv) * m3k;
