@@ -456,14 +456,29 @@ __global__ void k_phi(KP P, const double* __restrict__ b, double* __restrict__ p
     }
 }
 
+// ------------------------------------------------------------------ stencil accessors
+// The horizontal stencils below read the face velocities and face masks of one
+// level through an accessor: U(dj, di) / V(dj, di) are u / v of column
+// (j + dj, i + di), MU / MV the 0/1 wet flags of its east / north face.
+struct GlobalLevel {  // straight from the level planes in global memory
+    const KP& P;
+    const Nbr& nb;
+    const double* __restrict__ u;
+    const double* __restrict__ v;
+    size_t o;
+    int k;
+    __device__ __forceinline__ double U(int dj, int di) const { return u[o + nb.at(dj, di)]; }
+    __device__ __forceinline__ double V(int dj, int di) const { return v[o + nb.at(dj, di)]; }
+    __device__ __forceinline__ double MU(int dj, int di) const { return col_m3u(P, nb.at(dj, di), k); }
+    __device__ __forceinline__ double MV(int dj, int di) const { return col_m3v(P, nb.at(dj, di), k); }
+};
+
 // ------------------------------------------------------------------ Coriolis averages
 // v averaged onto u points over wet v faces (operators_masked.py:45-52)
-__device__ __forceinline__ double v_on_u(const KP& P, const Nbr& nb, const double* __restrict__ v,
-                                         size_t o, int k) {
-    const double f0 = v[o + nb.at(0, 0)], f1 = v[o + nb.at(-1, 0)];
-    const double f2 = v[o + nb.at(0, 1)], f3 = v[o + nb.at(-1, 1)];
-    const double w0 = m3v_at(P, nb, 0, 0, k), w1 = m3v_at(P, nb, -1, 0, k);
-    const double w2 = m3v_at(P, nb, 0, 1, k), w3 = m3v_at(P, nb, -1, 1, k);
+template <class A>
+__device__ __forceinline__ double v_on_u_at(const A& a) {
+    const double f0 = a.V(0, 0), f1 = a.V(-1, 0), f2 = a.V(0, 1), f3 = a.V(-1, 1);
+    const double w0 = a.MV(0, 0), w1 = a.MV(-1, 0), w2 = a.MV(0, 1), w3 = a.MV(-1, 1);
     double num = 0.0 + w0 * f0;
     num = num + w1 * f1;
     num = num + w2 * f2;
@@ -473,16 +488,14 @@ __device__ __forceinline__ double v_on_u(const KP& P, const Nbr& nb, const doubl
     den = den + w2;
     den = den + w3;
     const double avg = den > 0.0 ? num / den : 0.0;
-    return avg * m3u_at(P, nb, 0, 0, k);
+    return avg * a.MU(0, 0);
 }
 
 // u averaged onto v points over wet u faces (operators_masked.py:55-61)
-__device__ __forceinline__ double u_on_v(const KP& P, const Nbr& nb, const double* __restrict__ u,
-                                         size_t o, int k) {
-    const double f0 = u[o + nb.at(0, 0)], f1 = u[o + nb.at(0, -1)];
-    const double f2 = u[o + nb.at(1, 0)], f3 = u[o + nb.at(1, -1)];
-    const double w0 = m3u_at(P, nb, 0, 0, k), w1 = m3u_at(P, nb, 0, -1, k);
-    const double w2 = m3u_at(P, nb, 1, 0, k), w3 = m3u_at(P, nb, 1, -1, k);
+template <class A>
+__device__ __forceinline__ double u_on_v_at(const A& a) {
+    const double f0 = a.U(0, 0), f1 = a.U(0, -1), f2 = a.U(1, 0), f3 = a.U(1, -1);
+    const double w0 = a.MU(0, 0), w1 = a.MU(0, -1), w2 = a.MU(1, 0), w3 = a.MU(1, -1);
     double num = 0.0 + w0 * f0;
     num = num + w1 * f1;
     num = num + w2 * f2;
@@ -492,7 +505,17 @@ __device__ __forceinline__ double u_on_v(const KP& P, const Nbr& nb, const doubl
     den = den + w2;
     den = den + w3;
     const double avg = den > 0.0 ? num / den : 0.0;
-    return avg * m3v_at(P, nb, 0, 0, k);
+    return avg * a.MV(0, 0);
+}
+
+__device__ __forceinline__ double v_on_u(const KP& P, const Nbr& nb, const double* __restrict__ v, size_t o,
+                                         int k) {
+    return v_on_u_at(GlobalLevel{P, nb, nullptr, v, o, k});
+}
+
+__device__ __forceinline__ double u_on_v(const KP& P, const Nbr& nb, const double* __restrict__ u, size_t o,
+                                         int k) {
+    return u_on_v_at(GlobalLevel{P, nb, u, nullptr, o, k});
 }
 
 // horizontal Laplacian D o G with the given face masks (operators_masked.py:64-68);
@@ -541,72 +564,66 @@ __device__ __forceinline__ double explicit_dz(const KP& P, int k, double fkm1, d
 }
 
 // ------------------------------------------------------------------ momentum advection
-// x- and y-flux divergence of u at its east face at level k (advection_v06.py:77-99
-// for the kappa/TVD scheme, advection.py:62-79 for the centred one); the
-// reference forms ax + ay + az left to right, so (ax + ay) + az is its sum
-__device__ __forceinline__ double mom_adv_u_xy(const KP& P, const Nbr& nb, const double* __restrict__ u,
-                                               const double* __restrict__ v, int k) {
-    const size_t o = (size_t)k * P.n2;
-    auto U = [&](int dj, int di) { return u[o + nb.at(dj, di)]; };
-    auto V = [&](int dj, int di) { return v[o + nb.at(dj, di)]; };
+// x- and y-flux divergence of u at its east face (advection_v06.py:77-99 for the
+// kappa/TVD scheme, advection.py:62-79 for the centred one); the reference forms
+// ax + ay + az left to right, so (ax + ay) + az is its sum
+template <class A>
+__device__ __forceinline__ double mom_adv_u_xy(const KP& P, const A& a) {
     if (P.advection >= 3) {
         const bool lim = P.advection == 4;
-        const double ub_c0 = 0.5 * (U(0, -1) + U(0, 0));
-        const double ub_c1 = 0.5 * (U(0, 0) + U(0, 1));
-        const double uc0 = kappa_face(P, U(0, -2), U(0, -1), U(0, 0), U(0, 1), ub_c0,
-                                      m3u_at(P, nb, 0, -2, k), m3u_at(P, nb, 0, 1, k), lim);
-        const double uc1 = kappa_face(P, U(0, -1), U(0, 0), U(0, 1), U(0, 2), ub_c1,
-                                      m3u_at(P, nb, 0, -1, k), m3u_at(P, nb, 0, 2, k), lim);
+        const double ub_c0 = 0.5 * (a.U(0, -1) + a.U(0, 0));
+        const double ub_c1 = 0.5 * (a.U(0, 0) + a.U(0, 1));
+        const double uc0 = kappa_face(P, a.U(0, -2), a.U(0, -1), a.U(0, 0), a.U(0, 1), ub_c0, a.MU(0, -2),
+                                      a.MU(0, 1), lim);
+        const double uc1 = kappa_face(P, a.U(0, -1), a.U(0, 0), a.U(0, 1), a.U(0, 2), ub_c1, a.MU(0, -1),
+                                      a.MU(0, 2), lim);
         const double ax = (ub_c1 * uc1 - ub_c0 * uc0) / P.dx;
-        const double vb0 = 0.5 * (V(0, 0) + V(0, 1));
-        const double vbm = 0.5 * (V(-1, 0) + V(-1, 1));
-        const double fy0 = vb0 * kappa_face(P, U(-1, 0), U(0, 0), U(1, 0), U(2, 0), vb0,
-                                            m3u_at(P, nb, -1, 0, k), m3u_at(P, nb, 2, 0, k), lim);
-        const double fym = vbm * kappa_face(P, U(-2, 0), U(-1, 0), U(0, 0), U(1, 0), vbm,
-                                            m3u_at(P, nb, -2, 0, k), m3u_at(P, nb, 1, 0, k), lim);
+        const double vb0 = 0.5 * (a.V(0, 0) + a.V(0, 1));
+        const double vbm = 0.5 * (a.V(-1, 0) + a.V(-1, 1));
+        const double fy0 = vb0 * kappa_face(P, a.U(-1, 0), a.U(0, 0), a.U(1, 0), a.U(2, 0), vb0, a.MU(-1, 0),
+                                            a.MU(2, 0), lim);
+        const double fym = vbm * kappa_face(P, a.U(-2, 0), a.U(-1, 0), a.U(0, 0), a.U(1, 0), vbm, a.MU(-2, 0),
+                                            a.MU(1, 0), lim);
         return ax + (fy0 - fym) / P.dy;
     }
-    const double ub_c0 = 0.5 * (U(0, -1) + U(0, 0));
-    const double ub_c1 = 0.5 * (U(0, 0) + U(0, 1));
+    const double ub_c0 = 0.5 * (a.U(0, -1) + a.U(0, 0));
+    const double ub_c1 = 0.5 * (a.U(0, 0) + a.U(0, 1));
     const double ax = (ub_c1 * ub_c1 - ub_c0 * ub_c0) / P.dx;
-    const double vb0 = 0.5 * (V(0, 0) + V(0, 1));
-    const double vbm = 0.5 * (V(-1, 0) + V(-1, 1));
-    const double fy0 = vb0 * (0.5 * (U(0, 0) + U(1, 0)));
-    const double fym = vbm * (0.5 * (U(-1, 0) + U(0, 0)));
+    const double vb0 = 0.5 * (a.V(0, 0) + a.V(0, 1));
+    const double vbm = 0.5 * (a.V(-1, 0) + a.V(-1, 1));
+    const double fy0 = vb0 * (0.5 * (a.U(0, 0) + a.U(1, 0)));
+    const double fym = vbm * (0.5 * (a.U(-1, 0) + a.U(0, 0)));
     return ax + (fy0 - fym) / P.dy;
 }
 
 // the same for v at its north face (advection_v06.py:100-108, advection.py:81-95):
 // bx + by, formed in that order
-__device__ __forceinline__ double mom_adv_v_xy(const KP& P, const Nbr& nb, const double* __restrict__ u,
-                                               const double* __restrict__ v, int k) {
-    const size_t o = (size_t)k * P.n2;
-    auto U = [&](int dj, int di) { return u[o + nb.at(dj, di)]; };
-    auto V = [&](int dj, int di) { return v[o + nb.at(dj, di)]; };
+template <class A>
+__device__ __forceinline__ double mom_adv_v_xy(const KP& P, const A& a) {
     if (P.advection >= 3) {
         const bool lim = P.advection == 4;
-        const double vb_c0 = 0.5 * (V(-1, 0) + V(0, 0));
-        const double vb_c1 = 0.5 * (V(0, 0) + V(1, 0));
-        const double vc0 = kappa_face(P, V(-2, 0), V(-1, 0), V(0, 0), V(1, 0), vb_c0,
-                                      m3v_at(P, nb, -2, 0, k), m3v_at(P, nb, 1, 0, k), lim);
-        const double vc1 = kappa_face(P, V(-1, 0), V(0, 0), V(1, 0), V(2, 0), vb_c1,
-                                      m3v_at(P, nb, -1, 0, k), m3v_at(P, nb, 2, 0, k), lim);
+        const double vb_c0 = 0.5 * (a.V(-1, 0) + a.V(0, 0));
+        const double vb_c1 = 0.5 * (a.V(0, 0) + a.V(1, 0));
+        const double vc0 = kappa_face(P, a.V(-2, 0), a.V(-1, 0), a.V(0, 0), a.V(1, 0), vb_c0, a.MV(-2, 0),
+                                      a.MV(1, 0), lim);
+        const double vc1 = kappa_face(P, a.V(-1, 0), a.V(0, 0), a.V(1, 0), a.V(2, 0), vb_c1, a.MV(-1, 0),
+                                      a.MV(2, 0), lim);
         const double by = (vb_c1 * vc1 - vb_c0 * vc0) / P.dy;
-        const double ub0 = 0.5 * (U(0, 0) + U(1, 0));
-        const double ubm = 0.5 * (U(0, -1) + U(1, -1));
-        const double fx0 = ub0 * kappa_face(P, V(0, -1), V(0, 0), V(0, 1), V(0, 2), ub0,
-                                            m3v_at(P, nb, 0, -1, k), m3v_at(P, nb, 0, 2, k), lim);
-        const double fxm = ubm * kappa_face(P, V(0, -2), V(0, -1), V(0, 0), V(0, 1), ubm,
-                                            m3v_at(P, nb, 0, -2, k), m3v_at(P, nb, 0, 1, k), lim);
+        const double ub0 = 0.5 * (a.U(0, 0) + a.U(1, 0));
+        const double ubm = 0.5 * (a.U(0, -1) + a.U(1, -1));
+        const double fx0 = ub0 * kappa_face(P, a.V(0, -1), a.V(0, 0), a.V(0, 1), a.V(0, 2), ub0, a.MV(0, -1),
+                                            a.MV(0, 2), lim);
+        const double fxm = ubm * kappa_face(P, a.V(0, -2), a.V(0, -1), a.V(0, 0), a.V(0, 1), ubm, a.MV(0, -2),
+                                            a.MV(0, 1), lim);
         return (fx0 - fxm) / P.dx + by;
     }
-    const double vb_c0 = 0.5 * (V(-1, 0) + V(0, 0));
-    const double vb_c1 = 0.5 * (V(0, 0) + V(1, 0));
+    const double vb_c0 = 0.5 * (a.V(-1, 0) + a.V(0, 0));
+    const double vb_c1 = 0.5 * (a.V(0, 0) + a.V(1, 0));
     const double by = (vb_c1 * vb_c1 - vb_c0 * vb_c0) / P.dy;
-    const double ub0 = 0.5 * (U(0, 0) + U(1, 0));
-    const double ubm = 0.5 * (U(0, -1) + U(1, -1));
-    const double fx0 = ub0 * (0.5 * (V(0, 0) + V(0, 1)));
-    const double fxm = ubm * (0.5 * (V(0, -1) + V(0, 0)));
+    const double ub0 = 0.5 * (a.U(0, 0) + a.U(1, 0));
+    const double ubm = 0.5 * (a.U(0, -1) + a.U(1, -1));
+    const double fx0 = ub0 * (0.5 * (a.V(0, 0) + a.V(0, 1)));
+    const double fxm = ubm * (0.5 * (a.V(0, -1) + a.V(0, 0)));
     return (fx0 - fxm) / P.dx + by;
 }
 
@@ -652,23 +669,49 @@ __device__ __forceinline__ double diff_flux(double Kk, double f_above, double f_
 // its top (a per-cell form forms each of them twice). Every value is formed by
 // the reference's operations in its order.
 constexpr int MOM_KL = 10;
+constexpr int MOM_TX = 32, MOM_TY = 8, MOM_RX = MOM_TX + 4, MOM_RY = MOM_TY + 4, MOM_RN = MOM_RX * MOM_RY;
 
-__global__ void __launch_bounds__(256, 3) k_mom_column(
+// the level's u, v and face masks of a tile plus a 2-column ring, in shared memory
+struct TileLevel {
+    const double* su;
+    const double* sv;
+    const int* sku;
+    const int* skv;
+    int rc;  // the thread's column in the region
+    int k;
+    __device__ __forceinline__ double U(int dj, int di) const { return su[rc + dj * MOM_RX + di]; }
+    __device__ __forceinline__ double V(int dj, int di) const { return sv[rc + dj * MOM_RX + di]; }
+    __device__ __forceinline__ double MU(int dj, int di) const { return k < sku[rc + dj * MOM_RX + di] ? 1.0 : 0.0; }
+    __device__ __forceinline__ double MV(int dj, int di) const { return k < skv[rc + dj * MOM_RX + di] ? 1.0 : 0.0; }
+};
+
+__global__ void __launch_bounds__(MOM_TX * MOM_TY, 3) k_mom_column(
     KP P, const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ b,
     const double* __restrict__ phi, const double* __restrict__ w, const double* __restrict__ km,
     double* __restrict__ pgx, double* __restrict__ pgy, double* __restrict__ avpv,
     double* __restrict__ avpu, double* __restrict__ dzu, double* __restrict__ dzv,
     double* __restrict__ stu, double* __restrict__ stv) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= P.nx || j >= P.ny) return;
-    const int nz = P.nz;
+    __shared__ int s_g[MOM_RN], s_ku[MOM_RN], s_kv[MOM_RN];
+    __shared__ double s_u[MOM_RN], s_v[MOM_RN];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * MOM_TX + tx;
+    const int i0 = blockIdx.x * MOM_TX, j0 = blockIdx.y * MOM_TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const bool live = i < nx && j < ny;
     const int kbeg = blockIdx.z * MOM_KL;
     const int kend = kbeg + MOM_KL < nz ? kbeg + MOM_KL : nz;
-    Nbr nb;
-    nb.init(i, j, P.nx, P.ny);
+    for (int r = tid; r < MOM_RN; r += MOM_TX * MOM_TY) {
+        const int rj = r / MOM_RX, ri = r - rj * MOM_RX;
+        const int gc = wrapi(j0 - 2 + rj, ny) * nx + wrapi(i0 - 2 + ri, nx);
+        const int2 kfc = P.kface[gc];
+        s_g[r] = gc;
+        s_ku[r] = kfc.x;
+        s_kv[r] = kfc.y;
+    }
+    const int rc = (ty + 2) * MOM_RX + tx + 2;
     const size_t n2 = (size_t)P.n2;
-    const int c = nb.c, ce = nb.at(0, 1), cn = nb.at(1, 0);
+    const int wi = wrapi(i, nx), wj = wrapi(j, ny);
+    const int c = wj * nx + wi, ce = wj * nx + wrapi(i + 1, nx), cn = wrapi(j + 1, ny) * nx + wi;
     const ColGeo gc = ColGeo::load(P, c), ge = ColGeo::load(P, ce), gn = ColGeo::load(P, cn);
     const int2 kf = P.kface[c];
     const double tau_u = P.tau_u[c], tau_v = P.tau_v[c];
@@ -687,14 +730,21 @@ __global__ void __launch_bounds__(256, 3) k_mom_column(
     auto Uc = [&](int kk) { return (kk >= 0 && kk < nz) ? u[(size_t)kk * n2 + c] : 0.0; };
     auto Vc = [&](int kk) { return (kk >= 0 && kk < nz) ? v[(size_t)kk * n2 + c] : 0.0; };
     // rolling column values at k-1, k, k+1 (and k+2 for the advected velocity)
-    double u_m1 = Uc(kbeg - 1), u_0 = Uc(kbeg), u_p1 = Uc(kbeg + 1);
-    double v_m1 = Vc(kbeg - 1), v_0 = Vc(kbeg), v_p1 = Vc(kbeg + 1);
-    double dzu_m1 = dzu_at(kbeg - 1), dzu_0 = dzu_at(kbeg);
-    double dzv_m1 = dzv_at(kbeg - 1), dzv_0 = dzv_at(kbeg);
-    double K_0 = km[(size_t)kbeg * n2 + c];
+    double u_m1 = 0.0, u_0 = 0.0, u_p1 = 0.0, v_m1 = 0.0, v_0 = 0.0, v_p1 = 0.0;
+    double dzu_0 = 0.0, dzv_0 = 0.0, K_0 = 0.0;
     // fluxes through the top of level kbeg
     double fz_u = 0.0, fz_v = 0.0, dfu = 0.0, dfv = 0.0;
-    {
+    if (live) {
+        u_m1 = Uc(kbeg - 1);
+        u_0 = Uc(kbeg);
+        u_p1 = Uc(kbeg + 1);
+        v_m1 = Vc(kbeg - 1);
+        v_0 = Vc(kbeg);
+        v_p1 = Vc(kbeg + 1);
+        const double dzu_m1 = dzu_at(kbeg - 1), dzv_m1 = dzv_at(kbeg - 1);
+        dzu_0 = dzu_at(kbeg);
+        dzv_0 = dzv_at(kbeg);
+        K_0 = km[(size_t)kbeg * n2 + c];
         const int kk = kbeg;
         const double wc = w[(size_t)kk * n2 + c];
         if (P.advection != 0) {
@@ -712,6 +762,15 @@ __global__ void __launch_bounds__(256, 3) k_mom_column(
     }
     for (int k = kbeg; k < kend; ++k) {
         const size_t o = (size_t)k * n2;
+        // stage the level's u and v of the region (the previous level is done)
+        __syncthreads();
+        for (int r = tid; r < MOM_RN; r += MOM_TX * MOM_TY) {
+            s_u[r] = u[o + s_g[r]];
+            s_v[r] = v[o + s_g[r]];
+        }
+        __syncthreads();
+        if (!live) continue;
+        const TileLevel lv{s_u, s_v, s_ku, s_kv, rc, k};
         const double u_p2 = Uc(k + 2), v_p2 = Vc(k + 2);
         const double dzu_p1 = dzu_at(k + 1), dzv_p1 = dzv_at(k + 1);
         const double K_1 = km[o + n2 + c];
@@ -740,8 +799,8 @@ __global__ void __launch_bounds__(256, 3) k_mom_column(
         pgx[o + c] = px;
         pgy[o + c] = py;
         // ---- Coriolis averages of the old state
-        avpv[o + c] = v_on_u(P, nb, v, o, k);
-        avpu[o + c] = u_on_v(P, nb, u, o, k);
+        avpv[o + c] = v_on_u_at(lv);
+        avpu[o + c] = u_on_v_at(lv);
         // ---- explicit vertical diffusion: top flux carried, bottom flux formed here
         double dbu = 0.0, dbv = 0.0;
         if (k < nz - 1) {
@@ -766,12 +825,14 @@ __global__ void __launch_bounds__(256, 3) k_mom_column(
             const double wc1 = w[o + n2 + c];
             fbu = mom_vflux(P, k + 1, kf.x, u_m1, u_0, u_p1, u_p2, wc1, w[o + n2 + ce]);
             fbv = mom_vflux(P, k + 1, kf.y, v_m1, v_0, v_p1, v_p2, wc1, w[o + n2 + cn]);
-            const double au = mom_adv_u_xy(P, nb, u, v, k) + (fz_u - fbu) / P.dz_nom[k];
-            const double av = mom_adv_v_xy(P, nb, u, v, k) + (fz_v - fbv) / P.dz_nom[k];
+            const double au = mom_adv_u_xy(P, lv) + (fz_u - fbu) / P.dz_nom[k];
+            const double av = mom_adv_v_xy(P, lv) + (fz_v - fbv) / P.dz_nom[k];
             exu = exu - au * m3u_k;
             exv = exv - av * m3v_k;
         }
         if (P.a_h > 0.0) {
+            Nbr nb;
+            nb.init(wi, wj, nx, ny);
             exu = exu + P.a_h * hlap(P, nb, u, k, 0);
             exv = exv + P.a_h * hlap(P, nb, v, k, 1);
         }
@@ -793,14 +854,10 @@ __global__ void __launch_bounds__(256, 3) k_mom_column(
         v_m1 = v_0;
         v_0 = v_p1;
         v_p1 = v_p2;
-        dzu_m1 = dzu_0;
         dzu_0 = dzu_p1;
-        dzv_m1 = dzv_0;
         dzv_0 = dzv_p1;
         K_0 = K_1;
     }
-    (void)dzu_m1;
-    (void)dzv_m1;
 }
 
 // ------------------------------------------------------------------ predictor + column solves
@@ -1539,8 +1596,8 @@ void launch_mom_explicit(const KP& P, const double* u, const double* v, const do
                          const double* phi, const double* w, const double* km, double* pgx,
                          double* pgy, double* avpv, double* avpu, double* dzu, double* dzv,
                          double* stu, double* stv, cudaStream_t s) {
-    const dim3 grid((P.nx + 31) / 32, (P.ny + 7) / 8, (P.nz + MOM_KL - 1) / MOM_KL);
-    k_mom_column<<<grid, dim3(32, 8), 0, s>>>(P, u, v, b, phi, w, km, pgx, pgy, avpv, avpu, dzu, dzv, stu,
+    const dim3 grid((P.nx + MOM_TX - 1) / MOM_TX, (P.ny + MOM_TY - 1) / MOM_TY, (P.nz + MOM_KL - 1) / MOM_KL);
+    k_mom_column<<<grid, dim3(MOM_TX, MOM_TY), 0, s>>>(P, u, v, b, phi, w, km, pgx, pgy, avpv, avpu, dzu, dzv, stu,
                                              stv);
 }
 
