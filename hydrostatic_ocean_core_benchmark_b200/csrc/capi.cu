@@ -382,14 +382,15 @@ int step_once(oc_handle* h, cudaStream_t s) {
     double *u = h->U[cur], *v = h->V[cur], *b = h->B[cur], *eta = h->ETA[cur];
     double *un = h->U[nxt], *vn = h->V[nxt], *etan = h->ETA[nxt];
     const bool theta = c.scheme == OC_SCHEME_THETA, split = c.scheme == OC_SCHEME_SPLIT;
-    // The kernels of the old state that do not depend on the closure (w, phi, the
+    // The kernels of the old state that do not depend on the closure (phi, the
     // barotropic gradient, transports and divergence) run on a second stream,
     // beside the closure chain (TKE closure -> Ku/Kv -> multigrid rebuild);
-    // both join before the explicit momentum terms.
+    // both join before the explicit momentum terms. w of the old velocities is
+    // already in h->w: the state setters compute it and every step ends by
+    // computing it for the velocities it leaves behind.
     cudaStream_t a = h->aux;
     cudaEventRecord(h->fork, s);
     cudaStreamWaitEvent(a, h->fork, 0);
-    { Prof pr(h, a, "wcol"); launch_wcol(P, u, v, h->w, a); }
     { Prof pr(h, a, "phi"); launch_phi(P, b, h->phi, a); }
     if (!split) { Prof pr(h, a, "grad2"); launch_grad2(P, eta, h->gx2, h->gy2, a); }
     if (theta) {
@@ -810,6 +811,8 @@ static int set_state_on(oc_handle* h, const oc_state_view* s, int32_t on_device,
     if (s->km) bad |= copy_in(h->km, s->km, h->n3i, on_device, st);
     if (s->kh) bad |= copy_in(h->kh, s->kh, h->n3i, on_device, st);
     if (bad) return fail(h, OC_ERR_CUDA, "state copy failed");
+    // w of the new velocities (vertical_var.py:109-121), which a step reads first
+    launch_wcol(h->P, h->U[c], h->V[c], h->w, st);
     if (s->km) {
         // coefficients of the given viscosity (model3d_v05.py:141-167)
         launch_qsolve(h->P, h->km, h->q, st);
