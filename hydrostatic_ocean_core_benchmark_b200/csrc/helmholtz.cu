@@ -48,31 +48,64 @@ using TileWide = TileShape<128, 16>;  // level 0 of large grids: one tile per CT
 enum { SHAPE_32 = 0, SHAPE_3216 = 1, SHAPE_16 = 2, SHAPE_8 = 3, SHAPE_WIDE = 4 };
 
 // ------------------------------------------------------------------ barrier
-__device__ __forceinline__ bool grid_sync(const HelmParams& H) {
-    __syncthreads();
+// Grid barrier over a 64-bit arrival counter that only grows: barrier n of a
+// launch completes when the counter reaches base + (n + 1) * gridDim.x, so it
+// needs no reset and no generation word. The first barrier of a launch learns
+// the base from its own arrival (an atomic add with release semantics); later
+// arrivals are release reductions, whose value nobody waits for. The wait is an
+// acquire spin on the counter, bounded in time. A CTA that gives up records
+// OC_ERR_TIMEOUT in the status word, which the waiting CTAs poll, so every CTA
+// leaves the solve; the status is sticky, so a later launch that finds it set
+// makes no arrivals and the counter stays a multiple of the grid. Thread 0
+// hands the outcome to its CTA through shared memory.
+struct GridBar {
+    unsigned long long next;  // counter value that completes the next barrier; 0 before the first
+    int ok;
+};
+static __shared__ GridBar s_gbar;
+
+__device__ __forceinline__ void grid_sync_begin(const HelmParams& H) {
     if (threadIdx.x == 0) {
-        volatile unsigned* gen = H.bar_gen;
-        const unsigned g0 = *gen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(H.bar_count, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(H.bar_count, 0u);
-            __threadfence();
-            atomicAdd(H.bar_gen, 1u);
-        } else {
-            const long long t0 = clock64();
-            while (*gen == g0) {
-                if (clock64() - t0 > kBarrierCycles) {
-                    atomicExch(H.status, OC_ERR_TIMEOUT);
-                    break;
-                }
-                __nanosleep(32);
+        s_gbar.next = 0;
+        s_gbar.ok = *((volatile int*)H.status) == 0;
+    }
+}
+
+// thread 0's arrival and wait, out of line: the solve calls the barrier from many places
+__device__ __noinline__ void grid_arrive_wait(unsigned long long* cnt, int* status) {
+    unsigned long long target = s_gbar.next;
+    if (target == 0) {
+        unsigned long long old;
+        asm volatile("atom.add.release.gpu.u64 %0, [%1], 1;" : "=l"(old) : "l"(cnt) : "memory");
+        target = old - old % gridDim.x + gridDim.x;
+    } else {
+        asm volatile("red.add.release.gpu.u64 [%0], 1;" ::"l"(cnt) : "memory");
+    }
+    s_gbar.next = target + gridDim.x;
+    const long long t0 = clock64();
+    for (unsigned spin = 1;; ++spin) {
+        unsigned long long v;
+        asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(v) : "l"(cnt) : "memory");
+        if (v >= target) break;
+        if ((spin & 63) == 0) {
+            if (*((volatile int*)status) != 0) {
+                s_gbar.ok = 0;
+                break;
+            }
+            if (clock64() - t0 > kBarrierCycles) {
+                atomicExch(status, OC_ERR_TIMEOUT);
+                s_gbar.ok = 0;
+                break;
             }
         }
-        __threadfence();
     }
+}
+
+__device__ __forceinline__ bool grid_sync(const HelmParams& H) {
     __syncthreads();
-    return *((volatile int*)H.status) == 0;
+    if (threadIdx.x == 0 && s_gbar.ok) grid_arrive_wait(H.bar_count, H.status);
+    __syncthreads();
+    return s_gbar.ok != 0;
 }
 
 // ------------------------------------------------------------------ level operators
@@ -694,6 +727,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
     double* b0 = L0.b;
     bool ok = true;
     int iters = 0, conv = 1;
+    grid_sync_begin(H);
 
     // norm of the masked right-hand side (solvers_var.py:163-168)
     leaf_phase(H,
@@ -1014,7 +1048,7 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     int2* d_ops = (int2*)dalloc(sizeof(int2) * std::max<size_t>(1, ops.size()));
     H.leafA = (double*)dalloc(sizeof(double) * H.n_leaves);
     H.leafB = (double*)dalloc(sizeof(double) * H.n_leaves);
-    unsigned* bar = (unsigned*)dalloc(sizeof(unsigned) * 2);
+    unsigned long long* bar = (unsigned long long*)dalloc(sizeof(unsigned long long));
     H.log_cap = log_cap;
     H.log_iters = (int*)dalloc(sizeof(int) * log_cap);
     H.log_conv = (int*)dalloc(sizeof(int) * log_cap);
@@ -1031,7 +1065,6 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     H.height_start = d_hstart;
     H.ops = d_ops;
     H.bar_count = bar;
-    H.bar_gen = bar + 1;
     // co-resident grid for the cooperative launch
     int dev = 0, sms = 0, coop = 0;
     cudaGetDevice(&dev);
@@ -1097,7 +1130,9 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
                               std::max<size_t>((size_t)H.n_leaves, mg_work));
     int smem_optin = 0;
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (smem_ > (size_t)smem_optin) {
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k_helm_solve);  // static shared memory (the barrier's word) comes first
+    if (smem_ + fa.sharedSizeBytes > (size_t)smem_optin) {
         err = "Helmholtz grid too large for the single-pass reduction tree";
         return OC_ERR_UNSUPPORTED;
     }

@@ -41,8 +41,7 @@ struct HelmParams {
     double* leafA;
     double* leafB;
     // grid barrier and status
-    unsigned* bar_count;
-    unsigned* bar_gen;
+    unsigned long long* bar_count;  // grid barrier arrivals (only grows)
     int* status;
     // per-solve log
     int* log_iters;
