@@ -240,14 +240,21 @@ __device__ void leaf_phase(const HelmParams& H, F f, double* outA, double* outB)
     }
 }
 
+// the fold's plan (ops, then the height offsets): a shared-memory copy made at
+// the start of the solve when it fits, else the global arrays
+struct FoldPlan {
+    const int2* ops;
+    const int* height_start;
+};
+
 // fold the leaf sums by NumPy's tree, in every CTA (the result is the same
 // everywhere); sm holds n_leaves doubles
-__device__ double tree_fold(const HelmParams& H, const double* leaf, double* sm) {
+__device__ double tree_fold(const HelmParams& H, const FoldPlan& F, const double* leaf, double* sm) {
     for (int t = threadIdx.x; t < H.n_leaves; t += blockDim.x) sm[t] = __ldcg(leaf + t);
     __syncthreads();
     for (int h = 0; h < H.n_heights; ++h) {
-        for (int t = H.height_start[h] + threadIdx.x; t < H.height_start[h + 1]; t += blockDim.x) {
-            const int2 op = H.ops[t];
+        for (int t = F.height_start[h] + threadIdx.x; t < F.height_start[h + 1]; t += blockDim.x) {
+            const int2 op = F.ops[t];
             sm[op.x] = sm[op.x] + sm[op.y];
         }
         __syncthreads();
@@ -720,7 +727,16 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
     // with H.persist0 the first 4 RN doubles hold level 0's coefficient tile for the
     // whole solve; every other use of shared memory works above them
     double* persist = H.persist0 ? smem_all : nullptr;
-    double* sm = H.persist0 ? smem_all + 4 * TileWide::RN : smem_all;
+    double* const ops_base = smem_all + (H.persist0 ? 4 * TileWide::RN : 0);
+    double* sm = ops_base + H.ops_smem;
+    FoldPlan fold{H.ops, H.height_start};
+    if (H.ops_smem) {
+        int2* so = reinterpret_cast<int2*>(ops_base);
+        int* sh = reinterpret_cast<int*>(so + H.n_ops);
+        for (int t = threadIdx.x; t < H.n_ops; t += blockDim.x) so[t] = H.ops[t];
+        for (int t = threadIdx.x; t <= H.n_heights; t += blockDim.x) sh[t] = H.height_start[t];
+        fold = FoldPlan{so, sh};  // first read after the barrier that ends the first leaf phase
+    }
     const HLevel& L0 = H.lv[0];
     const double* rhs = H.rhs;
     double* x = L0.x;
@@ -740,7 +756,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                },
                H.leafA, nullptr);
     ok = grid_sync(H);
-    const double norm_b = ok ? sqrt(tree_fold(H, H.leafA, sm)) : 0.0;
+    const double norm_b = ok ? sqrt(tree_fold(H, fold, H.leafA, sm)) : 0.0;
     if (persist) persist_level0(H, persist);  // the coefficients are fixed during the solve
     if (!ok || norm_b == 0.0) goto done;
     {
@@ -774,7 +790,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                     if (!ok) break;
                 }
                 iters = it;
-                const double res = sqrt(tree_fold(H, H.leafA, sm));
+                const double res = sqrt(tree_fold(H, fold, H.leafA, sm));
                 if (res <= tol) {
                     conv = 1;
                     break;
@@ -815,7 +831,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                        H.leafA, nullptr);
             ok = grid_sync(H);
             if (!ok) goto done;
-            double rz = tree_fold(H, H.leafA, sm);
+            double rz = tree_fold(H, fold, H.leafA, sm);
             conv = 0;
             for (int it = 1; it <= H.max_iter; ++it) {
                 leaf_phase(H,
@@ -827,7 +843,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                            H.leafA, nullptr);
                 ok = grid_sync(H);
                 if (!ok) break;
-                const double alpha = rz / tree_fold(H, H.leafA, sm);
+                const double alpha = rz / tree_fold(H, fold, H.leafA, sm);
                 leaf_phase(H,
                            [&](int e) {
                                const double pe = __ldcg(p + e);
@@ -847,7 +863,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                 ok = grid_sync(H);
                 if (!ok) break;
                 iters = it;
-                const double res = sqrt(tree_fold(H, H.leafA, sm));
+                const double res = sqrt(tree_fold(H, fold, H.leafA, sm));
                 if (res <= tol) {
                     conv = 1;
                     break;
@@ -864,7 +880,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                     ok = grid_sync(H);
                     if (!ok) break;
                 }
-                const double rz_new = tree_fold(H, H.leafB, sm);
+                const double rz_new = tree_fold(H, fold, H.leafB, sm);
                 const double beta = rz_new / rz;
                 for (int e = grid_team().first; e < L0.n; e += grid_team().stride)
                     p[e] = __ldcg(z + e) + beta * __ldcg(p + e);
@@ -1064,6 +1080,7 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     H.leaf_start = d_leaves;
     H.height_start = d_hstart;
     H.ops = d_ops;
+    H.n_ops = (int)ops.size();
     H.bar_count = bar;
     // co-resident grid for the cooperative launch
     int dev = 0, sms = 0, coop = 0;
@@ -1132,6 +1149,13 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncAttributes fa{};
     cudaFuncGetAttributes(&fa, k_helm_solve);  // static shared memory (the barrier's word) comes first
+    // the fold's plan joins shared memory when it fits beside the rest
+    const size_t plan_doubles = (sizeof(int2) * ops.size() + sizeof(int) * hstart.size() + sizeof(double) - 1) / sizeof(double);
+    H.ops_smem = 0;
+    if (smem_ + sizeof(double) * plan_doubles + fa.sharedSizeBytes <= (size_t)smem_optin) {
+        H.ops_smem = (int)plan_doubles;
+        smem_ += sizeof(double) * plan_doubles;
+    }
     if (smem_ + fa.sharedSizeBytes > (size_t)smem_optin) {
         err = "Helmholtz grid too large for the single-pass reduction tree";
         return OC_ERR_UNSUPPORTED;

@@ -38,6 +38,8 @@ struct HelmParams {
     int n_heights;
     const int* height_start;  // n_heights + 1 offsets into ops
     const int2* ops;          // (lo, mid): value[lo] += value[mid]
+    int n_ops;
+    int ops_smem;             // doubles of shared memory holding a copy of ops and height_start (0: none)
     double* leafA;
     double* leafB;
     // grid barrier and status
