@@ -660,14 +660,15 @@ __device__ __forceinline__ double diff_flux(double Kk, double f_above, double f_
 // Everything of the predictor that depends on the old state only: the
 // common-depth pressure gradient, the old-state Coriolis average, the explicit
 // vertical diffusion and the stress + advection/viscosity increment
-// (model3d_v05.py:352-370), in level-marching form: one thread per column of
-// a 32 x 8 tile marches MOM_KL levels. The neighbour table and the compact
-// geometry of the column and of its east and north neighbours are formed once;
-// the velocity, viscosity and face-thickness values of the levels above and
-// below roll in registers; the vertical advective flux at the bottom of a level
-// and the diffusive flux there are carried to the next level as the fluxes at
-// its top (a per-cell form forms each of them twice). Every value is formed by
-// the reference's operations in its order.
+// (model3d_v05.py:352-370), in level-marching form: two threads per column of
+// a 32 x 8 tile, one for the u terms and one for the v terms, march MOM_KL
+// levels over the level planes the CTA stages in shared memory. The compact
+// geometry of the column and of its face's far neighbour is formed once; the
+// component's velocity and face thickness at the levels above and below roll
+// in registers; the vertical advective flux at the bottom of a level and the
+// diffusive flux there are carried to the next level as the fluxes at its top
+// (a per-cell form forms each of them twice). Every value is formed by the
+// reference's operations in its order.
 constexpr int MOM_KL = 10;
 constexpr int MOM_TX = 32, MOM_TY = 8, MOM_RX = MOM_TX + 4, MOM_RY = MOM_TY + 4, MOM_RN = MOM_RX * MOM_RY;
 
@@ -685,7 +686,7 @@ struct TileLevel {
     __device__ __forceinline__ double MV(int dj, int di) const { return k < skv[rc + dj * MOM_RX + di] ? 1.0 : 0.0; }
 };
 
-__global__ void __launch_bounds__(MOM_TX * MOM_TY, 3) k_mom_column(
+__global__ void __launch_bounds__(MOM_TX * MOM_TY * 2, 2) k_mom_column(
     KP P, const double* __restrict__ u, const double* __restrict__ v, const double* __restrict__ b,
     const double* __restrict__ phi, const double* __restrict__ w, const double* __restrict__ km,
     double* __restrict__ pgx, double* __restrict__ pgy, double* __restrict__ avpv,
@@ -693,170 +694,129 @@ __global__ void __launch_bounds__(MOM_TX * MOM_TY, 3) k_mom_column(
     double* __restrict__ stu, double* __restrict__ stv) {
     __shared__ int s_g[MOM_RN], s_ku[MOM_RN], s_kv[MOM_RN];
     __shared__ double s_u[MOM_RN], s_v[MOM_RN];
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * MOM_TX + tx;
+    // threadIdx.z selects the component: 0 the u terms at the column's east face,
+    // 1 the v terms at its north face (whole warps, so no divergence)
+    const int tx = threadIdx.x, ty = threadIdx.y, comp = threadIdx.z;
+    const int tid = (comp * MOM_TY + ty) * MOM_TX + tx;
+    const int nthreads = MOM_TX * MOM_TY * 2;
     const int i0 = blockIdx.x * MOM_TX, j0 = blockIdx.y * MOM_TY;
     const int i = i0 + tx, j = j0 + ty;
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const bool live = i < nx && j < ny;
     const int kbeg = blockIdx.z * MOM_KL;
     const int kend = kbeg + MOM_KL < nz ? kbeg + MOM_KL : nz;
-    for (int r = tid; r < MOM_RN; r += MOM_TX * MOM_TY) {
+    for (int r = tid; r < MOM_RN; r += nthreads) {
         const int rj = r / MOM_RX, ri = r - rj * MOM_RX;
-        const int gc = wrapi(j0 - 2 + rj, ny) * nx + wrapi(i0 - 2 + ri, nx);
-        const int2 kfc = P.kface[gc];
-        s_g[r] = gc;
+        const int gcol = wrapi(j0 - 2 + rj, ny) * nx + wrapi(i0 - 2 + ri, nx);
+        const int2 kfc = P.kface[gcol];
+        s_g[r] = gcol;
         s_ku[r] = kfc.x;
         s_kv[r] = kfc.y;
     }
     const int rc = (ty + 2) * MOM_RX + tx + 2;
     const size_t n2 = (size_t)P.n2;
     const int wi = wrapi(i, nx), wj = wrapi(j, ny);
-    const int c = wj * nx + wi, ce = wj * nx + wrapi(i + 1, nx), cn = wrapi(j + 1, ny) * nx + wi;
-    const ColGeo gc = ColGeo::load(P, c), ge = ColGeo::load(P, ce), gn = ColGeo::load(P, cn);
-    const int2 kf = P.kface[c];
-    const double tau_u = P.tau_u[c], tau_v = P.tau_v[c];
-    // face thickness of the u and v faces of the column at level kk (0 outside)
-    auto dzu_at = [&](int kk) {
+    const int c = wj * nx + wi;
+    // the face's far column (east for u, north for v) and its wet levels
+    const int cf = comp ? wrapi(j + 1, ny) * nx + wi : wj * nx + wrapi(i + 1, nx);
+    const ColGeo gc = ColGeo::load(P, c), gf = ColGeo::load(P, cf);
+    const int kff = comp ? P.kface[c].y : P.kface[c].x;
+    const double tau = comp ? P.tau_v[c] : P.tau_u[c];
+    const double* __restrict__ X = comp ? v : u;
+    // face thickness of the column's face at level kk (0 outside)
+    auto dzf_at = [&](int kk) {
         if (kk < 0 || kk >= nz) return 0.0;
         double m;
-        return face_dz(P, kf.x, kk, gc.dz(P, kk, m), ge.dz(P, kk, m));
-    };
-    auto dzv_at = [&](int kk) {
-        if (kk < 0 || kk >= nz) return 0.0;
-        double m;
-        return face_dz(P, kf.y, kk, gc.dz(P, kk, m), gn.dz(P, kk, m));
+        return face_dz(P, kff, kk, gc.dz(P, kk, m), gf.dz(P, kk, m));
     };
     auto m3c_at = [&](int kk) { return (kk >= 0 && kk < gc.kb) ? 1.0 : 0.0; };
-    auto Uc = [&](int kk) { return (kk >= 0 && kk < nz) ? u[(size_t)kk * n2 + c] : 0.0; };
-    auto Vc = [&](int kk) { return (kk >= 0 && kk < nz) ? v[(size_t)kk * n2 + c] : 0.0; };
-    // rolling column values at k-1, k, k+1 (and k+2 for the advected velocity)
-    double u_m1 = 0.0, u_0 = 0.0, u_p1 = 0.0, v_m1 = 0.0, v_0 = 0.0, v_p1 = 0.0;
-    double dzu_0 = 0.0, dzv_0 = 0.0, K_0 = 0.0;
+    auto Xc = [&](int kk) { return (kk >= 0 && kk < nz) ? X[(size_t)kk * n2 + c] : 0.0; };
+    // rolling values of the component at k-1, k, k+1 (and k+2 for advection)
+    double x_m1 = 0.0, x_0 = 0.0, x_p1 = 0.0, dz_0 = 0.0;
     // fluxes through the top of level kbeg
-    double fz_u = 0.0, fz_v = 0.0, dfu = 0.0, dfv = 0.0;
+    double fz = 0.0, df = 0.0;
     if (live) {
-        u_m1 = Uc(kbeg - 1);
-        u_0 = Uc(kbeg);
-        u_p1 = Uc(kbeg + 1);
-        v_m1 = Vc(kbeg - 1);
-        v_0 = Vc(kbeg);
-        v_p1 = Vc(kbeg + 1);
-        const double dzu_m1 = dzu_at(kbeg - 1), dzv_m1 = dzv_at(kbeg - 1);
-        dzu_0 = dzu_at(kbeg);
-        dzv_0 = dzv_at(kbeg);
-        K_0 = km[(size_t)kbeg * n2 + c];
+        x_m1 = Xc(kbeg - 1);
+        x_0 = Xc(kbeg);
+        x_p1 = Xc(kbeg + 1);
+        const double dz_m1 = dzf_at(kbeg - 1);
+        dz_0 = dzf_at(kbeg);
         const int kk = kbeg;
-        const double wc = w[(size_t)kk * n2 + c];
-        if (P.advection != 0) {
-            fz_u = mom_vflux(P, kk, kf.x, Uc(kk - 2), u_m1, u_0, u_p1, wc, w[(size_t)kk * n2 + ce]);
-            fz_v = mom_vflux(P, kk, kf.y, Vc(kk - 2), v_m1, v_0, v_p1, wc, w[(size_t)kk * n2 + cn]);
-        }
+        if (P.advection != 0)
+            fz = mom_vflux(P, kk, kff, Xc(kk - 2), x_m1, x_0, x_p1, w[(size_t)kk * n2 + c], w[(size_t)kk * n2 + cf]);
         if (kk == 0) {
-            dfu = tau_u;
-            dfv = tau_v;
+            df = tau;
         } else {
             const double bot = (m3c_at(kk - 1) > 0.0 && m3c_at(kk) == 0.0) ? 1.0 : 0.0;
-            dfu = diff_flux(K_0, u_m1, u_0, dzu_m1, dzu_0, bot);
-            dfv = diff_flux(K_0, v_m1, v_0, dzv_m1, dzv_0, bot);
+            df = diff_flux(km[(size_t)kbeg * n2 + c], x_m1, x_0, dz_m1, dz_0, bot);
         }
     }
     for (int k = kbeg; k < kend; ++k) {
         const size_t o = (size_t)k * n2;
         // stage the level's u and v of the region (the previous level is done)
         __syncthreads();
-        for (int r = tid; r < MOM_RN; r += MOM_TX * MOM_TY) {
+        for (int r = tid; r < MOM_RN; r += nthreads) {
             s_u[r] = u[o + s_g[r]];
             s_v[r] = v[o + s_g[r]];
         }
         __syncthreads();
         if (!live) continue;
         const TileLevel lv{s_u, s_v, s_ku, s_kv, rc, k};
-        const double u_p2 = Uc(k + 2), v_p2 = Vc(k + 2);
-        const double dzu_p1 = dzu_at(k + 1), dzv_p1 = dzv_at(k + 1);
+        const double x_p2 = Xc(k + 2);
+        const double dz_p1 = dzf_at(k + 1);
         const double K_1 = km[o + n2 + c];
-        double m3c, m3e, m3n;
-        const double dz_c = gc.dz(P, k, m3c), dz_e = ge.dz(P, k, m3e), dz_n = gn.dz(P, k, m3n);
-        const double m3u_k = k < kf.x ? 1.0 : 0.0;
-        const double m3v_k = k < kf.y ? 1.0 : 0.0;
-        const double m3_cn = m3c_at(k + 1);
-        const double bottom_k = (m3c > 0.0 && m3_cn == 0.0) ? 1.0 : 0.0;
+        double m3c, m3f;
+        const double dz_c = gc.dz(P, k, m3c), dz_f = gf.dz(P, k, m3f);
+        const double m3f_k = k < kff ? 1.0 : 0.0;
+        const double bottom_k = (m3c > 0.0 && m3c_at(k + 1) == 0.0) ? 1.0 : 0.0;
         // ---- pressure gradient at a common depth (model3d_v05.py:211-230)
-        const double phc = phi[o + c], phe = phi[o + ce], phn = phi[o + cn];
-        const double bc = b[o + c], be = b[o + ce], bn = b[o + cn];
-        double px, py;
+        const double phc = phi[o + c], phf = phi[o + cf];
+        const double bc = b[o + c], bf = b[o + cf];
+        const double dxy = comp ? P.dy : P.dx;
+        double pg;
         if (P.pgf_correction) {
             const double zc_c = gc.above(P, k) + 0.5 * dz_c;
-            const double zc_e = ge.above(P, k) + 0.5 * dz_e;
-            const double zc_n = gn.above(P, k) + 0.5 * dz_n;
-            const double zfx = 0.5 * (zc_c + zc_e);
-            px = m3u_k * ((phe + be * (zfx - zc_e)) - (phc + bc * (zfx - zc_c))) / P.dx;
-            const double zfy = 0.5 * (zc_c + zc_n);
-            py = m3v_k * ((phn + bn * (zfy - zc_n)) - (phc + bc * (zfy - zc_c))) / P.dy;
+            const double zc_f = gf.above(P, k) + 0.5 * dz_f;
+            const double zf = 0.5 * (zc_c + zc_f);
+            pg = m3f_k * ((phf + bf * (zf - zc_f)) - (phc + bc * (zf - zc_c))) / dxy;
         } else {
-            px = m3u_k * (phe - phc) / P.dx * m3u_k;
-            py = m3v_k * (phn - phc) / P.dy * m3v_k;
+            pg = m3f_k * (phf - phc) / dxy * m3f_k;
         }
-        pgx[o + c] = px;
-        pgy[o + c] = py;
-        // ---- Coriolis averages of the old state
-        avpv[o + c] = v_on_u_at(lv);
-        avpu[o + c] = u_on_v_at(lv);
+        (comp ? pgy : pgx)[o + c] = pg;
+        // ---- Coriolis average of the old state (v at u points, u at v points)
+        if (comp)
+            avpu[o + c] = u_on_v_at(lv);
+        else
+            avpv[o + c] = v_on_u_at(lv);
         // ---- explicit vertical diffusion: top flux carried, bottom flux formed here
-        double dbu = 0.0, dbv = 0.0;
-        if (k < nz - 1) {
-            dbu = diff_flux(K_1, u_0, u_p1, dzu_0, dzu_p1, bottom_k);
-            dbv = diff_flux(K_1, v_0, v_p1, dzv_0, dzv_p1, bottom_k);
-        }
+        const double db = (k < nz - 1) ? diff_flux(K_1, x_0, x_p1, dz_0, dz_p1, bottom_k) : 0.0;
         {
             const double mk = m3c > 0.0 ? 1.0 : 0.0;
-            const double idu = inv_pos(dzu_0);
-            const double outu = (dfu - dbu) * idu;
-            const double dragu = P.bottom_drag * u_0 * bottom_k;
-            dzu[o + c] = (outu - dragu * idu) * mk;
-            const double idv = inv_pos(dzv_0);
-            const double outv = (dfv - dbv) * idv;
-            const double dragv = P.bottom_drag * v_0 * bottom_k;
-            dzv[o + c] = (outv - dragv * idv) * mk;
+            const double id = inv_pos(dz_0);
+            const double out = (df - db) * id;
+            const double drag = P.bottom_drag * x_0 * bottom_k;
+            (comp ? dzv : dzu)[o + c] = (out - drag * id) * mk;
         }
         // ---- advection and horizontal viscosity, then the stress increment
-        double exu = 0.0, exv = 0.0;
-        double fbu = 0.0, fbv = 0.0;
+        double ex = 0.0, fb = 0.0;
         if (P.advection != 0) {
-            const double wc1 = w[o + n2 + c];
-            fbu = mom_vflux(P, k + 1, kf.x, u_m1, u_0, u_p1, u_p2, wc1, w[o + n2 + ce]);
-            fbv = mom_vflux(P, k + 1, kf.y, v_m1, v_0, v_p1, v_p2, wc1, w[o + n2 + cn]);
-            const double au = mom_adv_u_xy(P, lv) + (fz_u - fbu) / P.dz_nom[k];
-            const double av = mom_adv_v_xy(P, lv) + (fz_v - fbv) / P.dz_nom[k];
-            exu = exu - au * m3u_k;
-            exv = exv - av * m3v_k;
+            fb = mom_vflux(P, k + 1, kff, x_m1, x_0, x_p1, x_p2, w[o + n2 + c], w[o + n2 + cf]);
+            const double a = (comp ? mom_adv_v_xy(P, lv) : mom_adv_u_xy(P, lv)) + (fz - fb) / P.dz_nom[k];
+            ex = ex - a * m3f_k;
         }
         if (P.a_h > 0.0) {
             Nbr nb;
             nb.init(wi, wj, nx, ny);
-            exu = exu + P.a_h * hlap(P, nb, u, k, 0);
-            exv = exv + P.a_h * hlap(P, nb, v, k, 1);
+            ex = ex + P.a_h * hlap(P, nb, X, k, comp);
         }
-        if (k == 0) {
-            stu[o + c] = P.thv_dt * tau_u * inv_pos(dzu_0) + P.dt * exu;
-            stv[o + c] = P.thv_dt * tau_v * inv_pos(dzv_0) + P.dt * exv;
-        } else {
-            stu[o + c] = 0.0 + P.dt * exu;
-            stv[o + c] = 0.0 + P.dt * exv;
-        }
+        (comp ? stv : stu)[o + c] = (k == 0) ? P.thv_dt * tau * inv_pos(dz_0) + P.dt * ex : 0.0 + P.dt * ex;
         // roll down one level
-        fz_u = fbu;
-        fz_v = fbv;
-        dfu = dbu;
-        dfv = dbv;
-        u_m1 = u_0;
-        u_0 = u_p1;
-        u_p1 = u_p2;
-        v_m1 = v_0;
-        v_0 = v_p1;
-        v_p1 = v_p2;
-        dzu_0 = dzu_p1;
-        dzv_0 = dzv_p1;
-        K_0 = K_1;
+        fz = fb;
+        df = db;
+        x_m1 = x_0;
+        x_0 = x_p1;
+        x_p1 = x_p2;
+        dz_0 = dz_p1;
     }
 }
 
@@ -1597,7 +1557,7 @@ void launch_mom_explicit(const KP& P, const double* u, const double* v, const do
                          double* pgy, double* avpv, double* avpu, double* dzu, double* dzv,
                          double* stu, double* stv, cudaStream_t s) {
     const dim3 grid((P.nx + MOM_TX - 1) / MOM_TX, (P.ny + MOM_TY - 1) / MOM_TY, (P.nz + MOM_KL - 1) / MOM_KL);
-    k_mom_column<<<grid, dim3(MOM_TX, MOM_TY), 0, s>>>(P, u, v, b, phi, w, km, pgx, pgy, avpv, avpu, dzu, dzv, stu,
+    k_mom_column<<<grid, dim3(MOM_TX, MOM_TY, 2), 0, s>>>(P, u, v, b, phi, w, km, pgx, pgy, avpv, avpu, dzu, dzv, stu,
                                              stv);
 }
 
