@@ -800,7 +800,13 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                 for (int e = grid_team().first; e < L0.n; e += grid_team().stride) x[e] = __ldcg(xc + e);
             }
         } else {
-            // preconditioned CG (solvers_var.py:181-197)
+            // preconditioned CG (solvers_var.py:181-197). A fold reads its leaf
+            // sums after a grid barrier, and a leaf phase that follows a fold with
+            // no barrier between them writes a different buffer: a CTA that leaves
+            // its fold early must not overwrite sums another CTA is still reading.
+            // <r,z> at the start: leafB (leafA holds |b|); <p,Ap>: leafC; <r,r>
+            // and <r,z> of the update: leafA and leafB, read last before the
+            // barrier that ends the previous iteration.
             double* r = H.r;
             double* z = H.z;
             double* p = H.p;
@@ -828,10 +834,10 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                            p[e] = ze;
                            return make_double2(re * ze, 0.0);
                        },
-                       H.leafA, nullptr);
+                       H.leafB, nullptr);
             ok = grid_sync(H);
             if (!ok) goto done;
-            double rz = tree_fold(H, fold, H.leafA, sm);
+            double rz = tree_fold(H, fold, H.leafB, sm);
             conv = 0;
             for (int it = 1; it <= H.max_iter; ++it) {
                 leaf_phase(H,
@@ -840,10 +846,10 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                                Ap[e] = a;
                                return make_double2(__ldcg(p + e) * a, 0.0);
                            },
-                           H.leafA, nullptr);
+                           H.leafC, nullptr);
                 ok = grid_sync(H);
                 if (!ok) break;
-                const double alpha = rz / tree_fold(H, fold, H.leafA, sm);
+                const double alpha = rz / tree_fold(H, fold, H.leafC, sm);
                 leaf_phase(H,
                            [&](int e) {
                                const double pe = __ldcg(p + e);
@@ -1064,12 +1070,13 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     int2* d_ops = (int2*)dalloc(sizeof(int2) * std::max<size_t>(1, ops.size()));
     H.leafA = (double*)dalloc(sizeof(double) * H.n_leaves);
     H.leafB = (double*)dalloc(sizeof(double) * H.n_leaves);
+    H.leafC = (double*)dalloc(sizeof(double) * H.n_leaves);
     unsigned long long* bar = (unsigned long long*)dalloc(sizeof(unsigned long long));
     H.log_cap = log_cap;
     H.log_iters = (int*)dalloc(sizeof(int) * log_cap);
     H.log_conv = (int*)dalloc(sizeof(int) * log_cap);
     H.log_count = (int*)dalloc(sizeof(int));
-    if (!H.r || !H.z || !H.p || !H.Ap || !d_leaves || !d_hstart || !d_ops || !H.leafA || !H.leafB ||
+    if (!H.r || !H.z || !H.p || !H.Ap || !d_leaves || !d_hstart || !d_ops || !H.leafA || !H.leafB || !H.leafC ||
         !bar || !H.log_iters || !H.log_conv || !H.log_count) {
         err = "cudaMalloc failed (Helmholtz work)";
         return OC_ERR_CUDA;

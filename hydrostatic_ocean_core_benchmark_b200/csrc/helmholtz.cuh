@@ -42,6 +42,7 @@ struct HelmParams {
     int ops_smem;             // doubles of shared memory holding a copy of ops and height_start (0: none)
     double* leafA;
     double* leafB;
+    double* leafC;
     // grid barrier and status
     unsigned long long* bar_count;  // grid barrier arrivals (only grows)
     int* status;
