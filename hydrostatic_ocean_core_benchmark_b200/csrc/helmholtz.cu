@@ -300,27 +300,63 @@ __device__ __forceinline__ TileRefs tile_refs(double* base) {
 
 // load a tile region of level L whose interior starts at (i0, j0); x from xin
 // (or zero), plus the coarse correction e * mask when C is given
-// (with `coef` false the coefficients ku, kv, id, m are already in place)
+// (with `coef` false the coefficients ku, kv, id, m are already in place).
+// A thread gathers CH of its cells at a time into registers and only then
+// writes them to shared memory: the tile arrays reach here as plain pointers,
+// so the compiler may not move a later cell's global loads above an earlier
+// cell's stores, and cell by cell the loads of a thread would run one L2 round
+// trip after another.
+template <class S, int CH, bool COEF>
+__device__ __forceinline__ void tile_load_chunks(const HLevel& L, int i0, int j0, const double* xin,
+                                                 const HLevel* C, TileRefs t) {
+    const int nt = blockDim.x;
+    for (int base = threadIdx.x; base < S::RN; base += CH * nt) {
+        double xv[CH], bv[CH], mv[CH], kuv[CH], kvv[CH], idv[CH];
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int r = base + q * nt;
+            xv[q] = bv[q] = mv[q] = kuv[q] = kvv[q] = idv[q] = 0.0;
+            if (r < S::RN) {
+                const int rj = r / S::RW, ri = r - rj * S::RW;
+                const int gi = wrap_any(i0 - HALO + ri, L.nx), gj = wrap_any(j0 - HALO + rj, L.ny);
+                const int g = gj * L.nx + gi;
+                const double m = COEF ? L.mask[g] : t.m[r];
+                double x = xin ? __ldcg(xin + g) : 0.0;
+                if (C) x = x + __ldcg(C->x + (gj >> 1) * C->nx + (gi >> 1)) * m;
+                xv[q] = x;
+                bv[q] = __ldcg(L.b + g);
+                mv[q] = m;
+                if (COEF) {
+                    kuv[q] = L.Ku[g];
+                    kvv[q] = L.Kv[g];
+                    idv[q] = L.inv_diag[g];
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int r = base + q * nt;
+            if (r < S::RN) {
+                t.x[r] = xv[q];
+                t.b[r] = bv[q];
+                if (COEF) {
+                    t.ku[r] = kuv[q];
+                    t.kv[r] = kvv[q];
+                    t.id[r] = idv[q];
+                    t.m[r] = mv[q];
+                }
+            }
+        }
+    }
+}
+
 template <class S>
 __device__ void tile_load(const HLevel& L, int i0, int j0, const double* xin, const HLevel* C,
                           TileRefs t, bool coef = true) {
-#pragma unroll 4
-    for (int r = threadIdx.x; r < S::RN; r += blockDim.x) {
-        const int rj = r / S::RW, ri = r - rj * S::RW;
-        const int gi = wrap_any(i0 - HALO + ri, L.nx), gj = wrap_any(j0 - HALO + rj, L.ny);
-        const int g = gj * L.nx + gi;
-        const double m = coef ? L.mask[g] : t.m[r];
-        double x = xin ? __ldcg(xin + g) : 0.0;
-        if (C) x = x + __ldcg(C->x + (gj >> 1) * C->nx + (gi >> 1)) * m;
-        t.x[r] = x;
-        t.b[r] = __ldcg(L.b + g);
-        if (coef) {
-            t.ku[r] = L.Ku[g];
-            t.kv[r] = L.Kv[g];
-            t.id[r] = L.inv_diag[g];
-            t.m[r] = m;
-        }
-    }
+    if (coef)
+        tile_load_chunks<S, 2, true>(L, i0, j0, xin, C, t);
+    else
+        tile_load_chunks<S, 4, false>(L, i0, j0, xin, C, t);
     __syncthreads();
 }
 
