@@ -117,6 +117,11 @@ _SIGNATURES = {
     "oc_density": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "oc_get_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),
+    "oc_set_domain_slab": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_double, C.c_double]),
+    "oc_halo_values_per_row": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "oc_pack_rows": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    "oc_unpack_rows": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "oc_run_namelist": (C.c_int, [C.c_char_p]),
     "oc_last_error": (C.c_char_p, [C.c_void_p]),
     "oc_destroy": (None, [C.c_void_p]),

@@ -597,7 +597,11 @@ int oc_create(const oc_config* cfg, oc_handle** out) {
     return OC_OK;
 }
 
-int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const double* dzrh) {
+// the domain: masks, partial cells, face thicknesses and the device buffers.
+// mask_u_in / mask_v_in, when given, replace the face masks the boundary
+// conditions would give (a slab of a larger domain carries the larger domain's).
+static int set_domain_impl(oc_handle* h, const double* Hh, const double* maskh, const double* dzrh,
+                           const double* mask_u_in, const double* mask_v_in) {
     if (!h || !Hh || !maskh) return fail(h, OC_ERR_ARG, "H and mask are required");
     if (h->has_domain) return fail(h, OC_ERR_STATE, "the domain is already set");
     cudaSetDevice(h->cfg.device);
@@ -626,6 +630,15 @@ int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const dou
             if (h->cfg.bc_x != OC_BC_PERIODIC && i == nx - 1) h->mask_u[c] = 0.0;
             if (h->cfg.bc_y != OC_BC_PERIODIC && j == ny - 1) h->mask_v[c] = 0.0;
         }
+    if (mask_u_in && mask_v_in) {
+        for (size_t c = 0; c < n2; ++c) {
+            const double mu = mask_u_in[c], mv = mask_v_in[c];
+            if ((mu != 0.0 && mu != 1.0) || (mv != 0.0 && mv != 1.0))
+                return fail(h, OC_ERR_ARG, "face mask values must be 0 or 1");
+            h->mask_u[c] = mu;
+            h->mask_v[c] = mv;
+        }
+    }
     h->dzr.assign(nz, hmax / nz);
     if (dzrh) {
         for (int k = 0; k < nz; ++k) {
@@ -756,6 +769,114 @@ int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const dou
     if (e != cudaSuccess) return cuda_fail(h, e, "oc_set_domain");
     h->has_domain = true;
     return OC_OK;
+}
+
+int oc_set_domain(oc_handle* h, const double* Hh, const double* maskh, const double* dzrh) {
+    return set_domain_impl(h, Hh, maskh, dzrh, nullptr, nullptr);
+}
+
+int oc_set_domain_slab(oc_handle* h, const double* Hh, const double* maskh, const double* dzrh,
+                       const double* mask_u, const double* mask_v, double dx, double dy) {
+    if (!h) return OC_ERR_ARG;
+    if (h->has_domain) return fail(h, OC_ERR_STATE, "the domain is already set");
+    if (h->cfg.scheme != OC_SCHEME_FB)
+        return fail(h, OC_ERR_UNSUPPORTED,
+                    "a slab of a larger domain steps with scheme fb only: theta needs a global elliptic solve "
+                    "and split_explicit a halo exchange per substep");
+    if (!dzrh || !mask_u || !mask_v)
+        return fail(h, OC_ERR_ARG, "a slab needs the larger domain's level table and face masks");
+    if (!(dx > 0.0) || !(dy > 0.0) || !std::isfinite(dx) || !std::isfinite(dy))
+        return fail(h, OC_ERR_ARG, "dx and dy must be finite and > 0");
+    h->P.dx = dx;
+    h->P.dy = dy;
+    return set_domain_impl(h, Hh, maskh, dzrh, mask_u, mask_v);
+}
+
+namespace {
+
+// the fields a slab exchanges with its neighbours, in packing order, with their levels
+struct HaloField {
+    double* ptr;
+    int levels;
+};
+
+int halo_fields(oc_handle* h, HaloField* out) {
+    const int c = h->cur, nz = h->nz;
+    int n = 0;
+    out[n++] = {h->ETA[c], 1};
+    out[n++] = {h->U[c], nz};
+    out[n++] = {h->V[c], nz};
+    out[n++] = {h->B[c], nz};
+    if (h->cfg.tracers == OC_TRACERS_TS) {
+        out[n++] = {h->Tt[c], nz};
+        out[n++] = {h->Ss[c], nz};
+    }
+    if (h->cfg.closure == OC_CLOSURE_TKE) {
+        out[n++] = {h->e, nz + 1};
+        out[n++] = {h->km, nz + 1};
+        out[n++] = {h->kh, nz + 1};
+    }
+    return n;
+}
+
+int rows_check(oc_handle* h, int32_t j0, int32_t nrows, const void* buf) {
+    if (!h || !buf) return OC_ERR_ARG;
+    if (!h->has_state) return fail(h, OC_ERR_STATE, "set the state before exchanging rows");
+    if (j0 < 0 || nrows < 1 || (int64_t)j0 + nrows > h->ny) return fail(h, OC_ERR_ARG, "rows outside the domain");
+    return OC_OK;
+}
+
+// copy rows [j0, j0 + nrows) of every exchanged field between the state and a
+// packed device buffer (field after field, level after level, row-major)
+int copy_rows(oc_handle* h, int32_t j0, int32_t nrows, double* buf, bool pack, cudaStream_t s) {
+    HaloField f[9];
+    const int n = halo_fields(h, f);
+    const size_t nx = h->nx, row_bytes = nx * nrows * sizeof(double);
+    size_t off = 0;
+    for (int q = 0; q < n; ++q) {
+        double* field = f[q].ptr + (size_t)j0 * nx;
+        double* packed = buf + off;
+        const cudaError_t e =
+            pack ? cudaMemcpy2DAsync(packed, row_bytes, field, h->n2 * sizeof(double), row_bytes, f[q].levels,
+                                     cudaMemcpyDeviceToDevice, s)
+                 : cudaMemcpy2DAsync(field, h->n2 * sizeof(double), packed, row_bytes, row_bytes, f[q].levels,
+                                     cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return cuda_fail(h, e, pack ? "oc_pack_rows" : "oc_unpack_rows");
+        off += nx * nrows * f[q].levels;
+    }
+    return OC_OK;
+}
+
+}  // namespace
+
+int oc_halo_values_per_row(oc_handle* h, int64_t* count) {
+    if (!h || !count) return OC_ERR_ARG;
+    if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain first");
+    HaloField f[9];
+    const int n = halo_fields(h, f);
+    int64_t levels = 0;
+    for (int q = 0; q < n; ++q) levels += f[q].levels;
+    *count = levels * h->nx;
+    return OC_OK;
+}
+
+int oc_pack_rows(oc_handle* h, int32_t j0, int32_t nrows, double* buf, void* stream) {
+    int rc = rows_check(h, j0, nrows, buf);
+    if (rc) return rc;
+    cudaSetDevice(h->cfg.device);
+    return copy_rows(h, j0, nrows, buf, true, (cudaStream_t)stream);
+}
+
+int oc_unpack_rows(oc_handle* h, int32_t j0, int32_t nrows, const double* buf, void* stream) {
+    int rc = rows_check(h, j0, nrows, buf);
+    if (rc) return rc;
+    cudaSetDevice(h->cfg.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = copy_rows(h, j0, nrows, const_cast<double*>(buf), false, s);
+    if (rc) return rc;
+    // w of the velocities now in the state, which a step reads first
+    launch_wcol(h->P, h->U[h->cur], h->V[h->cur], h->w, s);
+    return check_launch(h, "oc_unpack_rows");
 }
 
 int oc_set_forcing(oc_handle* h, const double* taux_c, const double* tauy_c) {

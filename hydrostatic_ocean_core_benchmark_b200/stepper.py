@@ -35,7 +35,11 @@ class OceanStepper:
     """One model instance on one GPU."""
 
     def __init__(self, params: OceanParams, H, mask, dzr=None, taux_c=None, tauy_c=None,
-                 device: int = 0):
+                 device: int = 0, slab=None):
+        """``slab``: for one y-slab of a larger domain (fb scheme, multi-GPU), the
+        tuple (mask_u, mask_v, dx, dy) of the larger domain -- its face masks at
+        this handle's rows and its spacing (oc_set_domain_slab); dzr is then
+        required and is the larger domain's level table."""
         self.lib = _lib.load()
         self.p = params
         cfg = _lib.config_from_params(params, device)
@@ -49,8 +53,17 @@ class OceanStepper:
         mh = np.ascontiguousarray(mask, dtype=np.float64).reshape(self.shape2)
         dz = None if dzr is None else np.ascontiguousarray(dzr, dtype=np.float64).reshape(params.nz)
         self._keep = [Hh, mh, dz]
-        self._call("oc_set_domain", self.lib.oc_set_domain, self.h, Hh.ctypes.data, mh.ctypes.data,
-                   None if dz is None else dz.ctypes.data)
+        if slab is None:
+            self._call("oc_set_domain", self.lib.oc_set_domain, self.h, Hh.ctypes.data, mh.ctypes.data,
+                       None if dz is None else dz.ctypes.data)
+        else:
+            mu, mv, dx, dy = slab
+            mu = np.ascontiguousarray(mu, dtype=np.float64).reshape(self.shape2)
+            mv = np.ascontiguousarray(mv, dtype=np.float64).reshape(self.shape2)
+            self._keep += [mu, mv]
+            self._call("oc_set_domain_slab", self.lib.oc_set_domain_slab, self.h, Hh.ctypes.data,
+                       mh.ctypes.data, None if dz is None else dz.ctypes.data, mu.ctypes.data, mv.ctypes.data,
+                       float(dx), float(dy))
         if taux_c is not None or tauy_c is not None:
             self.set_forcing(taux_c, tauy_c)
 
@@ -143,6 +156,33 @@ class OceanStepper:
         view, dev, keep = self._view(out, self._shapes(), writable=True)
         sp = getattr(stream, "cuda_stream", stream)
         self._call("oc_get_state_async", self.lib.oc_get_state_async, self.h, C.byref(view), dev, sp)
+
+    # ------------------------------------------------------------------ slab halos
+    def halo_values_per_row(self) -> int:
+        """Doubles one row of all exchanged fields takes (oc_halo_values_per_row)."""
+        n = C.c_int64()
+        self._call("oc_halo_values_per_row", self.lib.oc_halo_values_per_row, self.h, C.byref(n))
+        return int(n.value)
+
+    def _rows_buffer(self, buf, nrows: int):
+        import torch
+        if not (_is_tensor(buf) and buf.is_cuda and buf.dtype == torch.float64 and buf.is_contiguous()):
+            raise ValueError("row buffers must be contiguous float64 CUDA tensors")
+        if buf.numel() < self.halo_values_per_row() * nrows:
+            raise ValueError("row buffer too small")
+        return buf.data_ptr()
+
+    def pack_rows(self, j0: int, nrows: int, buf, stream=None):
+        """Rows [j0, j0 + nrows) of every exchanged field into ``buf`` (oc_pack_rows)."""
+        ptr = self._rows_buffer(buf, nrows)
+        sp = getattr(stream, "cuda_stream", stream)
+        self._call("oc_pack_rows", self.lib.oc_pack_rows, self.h, int(j0), int(nrows), ptr, sp)
+
+    def unpack_rows(self, j0: int, nrows: int, buf, stream=None):
+        """``buf`` into rows [j0, j0 + nrows) of every exchanged field (oc_unpack_rows)."""
+        ptr = self._rows_buffer(buf, nrows)
+        sp = getattr(stream, "cuda_stream", stream)
+        self._call("oc_unpack_rows", self.lib.oc_unpack_rows, self.h, int(j0), int(nrows), ptr, sp)
 
     def reset_mixing(self):
         self._call("oc_reset_mixing", self.lib.oc_reset_mixing, self.h)

@@ -128,6 +128,31 @@ int oc_create(const oc_config* cfg, oc_handle** out);
  * partial cells, face thicknesses and the static coefficients. */
 int oc_set_domain(oc_handle* h, const double* H, const double* mask, const double* dzr);
 
+/* One y-slab of a larger domain, for a multi-GPU run of the fb scheme
+ * (reference libs/cuda/src/cfd_exp3d5_cuda_multi.cu:96-118: static arrays built
+ * once on the whole domain and cut by rows, the whole domain's spacing kept).
+ * H, mask, mask_u, mask_v are the larger domain's arrays at the handle's ny rows
+ * (owned rows plus halo rows, wrapped periodically); the face masks carry the
+ * larger domain's walls, so a wall at a slab edge stays a wall. dzr (required)
+ * is the larger domain's level table, dx and dy its spacing. The handle's
+ * configuration has ny = the slab's rows and scheme fb; other schemes are
+ * refused (OC_ERR_UNSUPPORTED): theta needs a global elliptic solve and
+ * split_explicit a halo exchange per substep. */
+int oc_set_domain_slab(oc_handle* h, const double* H, const double* mask, const double* dzr,
+                       const double* mask_u, const double* mask_v, double dx, double dy);
+
+/* Halo exchange of a slab (reference cfd_exp3d5_cuda_multi.cu:133-172: k_pack /
+ * k_unpack over u, v, b, T, S, eta and, with TKE, e, K_m, K_h). The exchanged
+ * fields, in this order: eta, u, v, b, T and S (TS tracers), e, km, kh (TKE
+ * closure). oc_halo_values_per_row gives the doubles one row of all of them
+ * takes; oc_pack_rows copies rows [j0, j0 + nrows) of each field, level after
+ * level, into the device buffer `buf` (values_per_row * nrows doubles), and
+ * oc_unpack_rows writes such a buffer into those rows and recomputes w for the
+ * velocities now in the state. Asynchronous on `stream`. */
+int oc_halo_values_per_row(oc_handle* h, int64_t* count);
+int oc_pack_rows(oc_handle* h, int32_t j0, int32_t nrows, double* buf, void* stream);
+int oc_unpack_rows(oc_handle* h, int32_t j0, int32_t nrows, const double* buf, void* stream);
+
 /* Optional surface stress field at cell centres [ny][nx] in N m-2 (host);
  * NULL for both keeps the scalar tau_x/tau_y of the configuration. */
 int oc_set_forcing(oc_handle* h, const double* taux_c, const double* tauy_c);
