@@ -120,6 +120,12 @@ _SIGNATURES = {
     "oc_set_domain_slab": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_double, C.c_double]),
     "oc_halo_values_per_row": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "oc_set_tiling": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "oc_ensemble_create": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "oc_ensemble_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "oc_ensemble_last_error": (C.c_char_p, [C.c_void_p]),
+    "oc_ensemble_destroy": (C.c_int, [C.c_void_p]),
+    "oc_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "oc_pack_rows": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "oc_unpack_rows": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "oc_run_namelist": (C.c_int, [C.c_char_p]),

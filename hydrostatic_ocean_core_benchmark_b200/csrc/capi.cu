@@ -107,9 +107,17 @@ struct oc_handle {
     cudaEvent_t fork = nullptr, join = nullptr;
     Counters graph_delta[2] = {};
     cudaStream_t capture_stream = nullptr;
+    long long graph_version = 0;  // bumped whenever recorded graphs go stale
+    // while an ensemble records its graph: every Helmholtz solve of every member
+    // waits on this event and records it, so the cooperative solves run one at a
+    // time and never compete for the SMs
+    cudaEvent_t solve_chain = nullptr;
 };
 
 namespace {
+
+// levels one CTA of k_mom_column / k_tracer_rhs marches unless tuned
+constexpr int kDefaultLevelsPerCta = 10;
 
 int fail(oc_handle* h, int code, const std::string& msg) {
     if (h) h->err = msg;
@@ -224,6 +232,8 @@ void fill_scalars(oc_handle* h) {
     const double kap = 1.0 / 3.0;
     P.one_m_kappa3 = 1.0 - kap;
     P.one_p_kappa3 = 1.0 + kap;
+    P.mom_kl = c.nz < kDefaultLevelsPerCta ? c.nz : kDefaultLevelsPerCta;
+    P.tr_kl = P.mom_kl;
 }
 
 double face_host(int rule, double a, double b) {
@@ -440,10 +450,12 @@ int step_once(oc_handle* h, cudaStream_t s) {
             { Prof pr(h, s, "helm_rhs"); launch_helm_rhs(P, eta, h->div_old, h->Ug, h->Vg, h->rhs2, s); }
             int rc = ensure_log(h, h->solves + 1, s);  // graphs reserve the log before recording
             if (rc) return rc;
+            if (h->solve_chain) cudaStreamWaitEvent(s, h->solve_chain, 0);
             {
                 Prof pr(h, s, "helm_solve");
                 rc = h->solver->solve(h->rhs2, etan, s, h->err);
             }
+            if (h->solve_chain) cudaEventRecord(h->solve_chain, s);
             if (rc) return rc;
             h->solves += 1;
             double* ou = last ? un : h->uit;
@@ -511,6 +523,7 @@ int step_once(oc_handle* h, cudaStream_t s) {
 }
 
 void drop_graphs(oc_handle* h) {
+    ++h->graph_version;
     for (auto& g : h->graph)
         if (g) {
             cudaGraphExecDestroy(g);
@@ -879,6 +892,76 @@ int oc_unpack_rows(oc_handle* h, int32_t j0, int32_t nrows, const double* buf, v
     return check_launch(h, "oc_unpack_rows");
 }
 
+int oc_set_tiling(oc_handle* h, int32_t mom_levels, int32_t tracer_levels) {
+    if (!h) return OC_ERR_ARG;
+    if (mom_levels < 1 || mom_levels > h->nz || tracer_levels < 1 || tracer_levels > h->nz)
+        return fail(h, OC_ERR_ARG, "levels per CTA must lie in 1..nz");
+    h->P.mom_kl = mom_levels;
+    h->P.tr_kl = tracer_levels;
+    drop_graphs(h);  // recorded launches carry the old values
+    return OC_OK;
+}
+
+int oc_autotune(oc_handle* h, int32_t* mom_levels, int32_t* tracer_levels) {
+    if (!h) return OC_ERR_ARG;
+    if (!h->has_state) return fail(h, OC_ERR_STATE, "set the state before tuning");
+    cudaSetDevice(h->cfg.device);
+    KP P = h->P;
+    const int c = h->cur, nz = h->nz;
+    std::vector<int> cand;
+    for (int kl : {2, 3, 4, 5, 6, 8, 10, 13, 17, 25, nz})
+        if (kl >= 1 && kl <= nz && std::find(cand.begin(), cand.end(), kl) == cand.end()) cand.push_back(kl);
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    launch_phi(P, h->B[c], h->phi, s);  // the explicit momentum terms read phi
+    // time one kernel class over the candidates; the outputs are scratch that
+    // the next step writes again before reading
+    auto tune = [&](bool mom) {
+        int best = mom ? P.mom_kl : P.tr_kl;
+        float best_ms = 1e30f;
+        for (int kl : cand) {
+            KP Q = P;
+            (mom ? Q.mom_kl : Q.tr_kl) = kl;
+            auto run = [&]() {
+                if (mom)
+                    launch_mom_explicit(Q, h->U[c], h->V[c], h->B[c], h->phi, h->w, h->km, h->pgx, h->pgy, h->avpv,
+                                        h->avpu, h->dzu, h->dzv, h->stu, h->stv, s);
+                else
+                    launch_tracer_rhs(Q, h->Tt[c], h->Ss[c], h->B[c], h->U[c], h->V[c], h->w, h->kh, h->pgx, h->pgy, s);
+            };
+            run();
+            float ms = 1e30f;
+            for (int r = 0; r < 3; ++r) {
+                cudaEventRecord(e0, s);
+                run();
+                cudaEventRecord(e1, s);
+                cudaEventSynchronize(e1);
+                float t = 0.0f;
+                cudaEventElapsedTime(&t, e0, e1);
+                ms = std::min(ms, t);
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = kl;
+            }
+        }
+        return best;
+    };
+    const int mk = tune(true), tk = tune(false);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const int rc = check_launch(h, "oc_autotune");
+    if (rc) return rc;
+    h->P.mom_kl = mk;
+    h->P.tr_kl = tk;
+    drop_graphs(h);
+    if (mom_levels) *mom_levels = mk;
+    if (tracer_levels) *tracer_levels = tk;
+    return OC_OK;
+}
+
 int oc_set_forcing(oc_handle* h, const double* taux_c, const double* tauy_c) {
     if (!h) return OC_ERR_ARG;
     drop_graphs(h);
@@ -1071,6 +1154,208 @@ int oc_step_graph(oc_handle* h, int32_t n_steps, void* stream) {
         const int rc = step_once(h, s);
         if (rc) return rc;
     }
+    return OC_OK;
+}
+
+// ---------------------------------------------------------------------------- ensembles
+struct oc_ensemble {
+    std::vector<oc_handle*> members;
+    std::vector<cudaStream_t> streams;  // one recording branch per member
+    std::vector<cudaEvent_t> joins;
+    cudaStream_t capture = nullptr;
+    cudaEvent_t fork = nullptr, chain = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int> parity;                    // each member's buffer index at recording
+    std::vector<long long> version;             // each member's graph version at recording
+    std::vector<oc_handle::Counters> delta;     // each member's counter increments per replay
+    int device = 0;
+    std::string err;
+    ~oc_ensemble() {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (auto st : streams) cudaStreamDestroy(st);
+        for (auto ev : joins) cudaEventDestroy(ev);
+        if (capture) cudaStreamDestroy(capture);
+        if (fork) cudaEventDestroy(fork);
+        if (chain) cudaEventDestroy(chain);
+    }
+};
+
+namespace {
+
+oc_handle::Counters counters_of(const oc_handle* h) {
+    return {h->steps, h->tridiag, h->rebuilds, h->substeps, h->solves, h->launches};
+}
+
+void set_counters(oc_handle* h, const oc_handle::Counters& c) {
+    h->steps = c.steps;
+    h->tridiag = c.tridiag;
+    h->rebuilds = c.rebuilds;
+    h->substeps = c.substeps;
+    h->solves = c.solves;
+    h->launches = c.launches;
+}
+
+// record two steps of every member into one graph: member m on branch m, the
+// Helmholtz solves of all members chained in recording order
+int ensemble_record(oc_ensemble* e) {
+    if (e->exec) {
+        cudaGraphExecDestroy(e->exec);
+        e->exec = nullptr;
+    }
+    const size_t n = e->members.size();
+    std::vector<oc_handle::Counters> before(n);
+    std::vector<int> cur(n);
+    for (size_t m = 0; m < n; ++m) {
+        oc_handle* h = e->members[m];
+        // the solve log must hold every solve of a replay without moving
+        const long long per_pair = h->solver ? 2LL * h->cfg.n_picard : 0;
+        if (h->solver && h->solves + 2 * per_pair > h->solver->log_capacity()) {
+            const int rc = ensure_log(h, 2 * (h->solves + 2 * per_pair), 0);
+            if (rc) return rc;
+        }
+        before[m] = counters_of(h);
+        cur[m] = h->cur;
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamBeginCapture(e->capture, cudaStreamCaptureModeThreadLocal);
+    int rc = ce == cudaSuccess ? OC_OK : OC_ERR_CUDA;
+    if (rc == OC_OK) {
+        cudaEventRecord(e->fork, e->capture);
+        cudaEventRecord(e->chain, e->capture);  // the chain starts inside the recording
+        for (size_t m = 0; m < n; ++m) cudaStreamWaitEvent(e->streams[m], e->fork, 0);
+        for (int step = 0; step < 2 && rc == OC_OK; ++step)
+            for (size_t m = 0; m < n && rc == OC_OK; ++m) {
+                oc_handle* h = e->members[m];
+                const bool prof = h->profiling;
+                h->profiling = false;
+                h->solve_chain = e->chain;
+                rc = step_once(h, e->streams[m]);
+                h->solve_chain = nullptr;
+                h->profiling = prof;
+            }
+        for (size_t m = 0; m < n; ++m) {
+            cudaEventRecord(e->joins[m], e->streams[m]);
+            cudaStreamWaitEvent(e->capture, e->joins[m], 0);
+        }
+    }
+    ce = cudaStreamEndCapture(e->capture, &g);
+    if (rc == OC_OK && ce != cudaSuccess) rc = OC_ERR_CUDA;
+    if (rc == OC_OK && cudaGraphInstantiate(&e->exec, g, 0) != cudaSuccess) rc = OC_ERR_CUDA;
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    e->parity = cur;
+    e->version.assign(n, 0);
+    e->delta.assign(n, {});
+    for (size_t m = 0; m < n; ++m) {
+        oc_handle* h = e->members[m];
+        const oc_handle::Counters after = counters_of(h);
+        e->delta[m] = {after.steps - before[m].steps, after.tridiag - before[m].tridiag,
+                       after.rebuilds - before[m].rebuilds, after.substeps - before[m].substeps,
+                       after.solves - before[m].solves, after.launches - before[m].launches};
+        set_counters(h, before[m]);
+        h->cur = cur[m];
+        e->version[m] = h->graph_version;
+    }
+    if (rc) {
+        if (e->exec) cudaGraphExecDestroy(e->exec);
+        e->exec = nullptr;
+        e->err = "the ensemble's steps could not be recorded";
+    }
+    return rc;
+}
+
+}  // namespace
+
+int oc_ensemble_create(oc_handle* const* members, int32_t n, oc_ensemble** out) {
+    if (!members || n < 1 || !out) return OC_ERR_ARG;
+    *out = nullptr;
+    auto* e = new oc_ensemble();
+    for (int32_t m = 0; m < n; ++m) {
+        oc_handle* h = members[m];
+        if (!h || !h->has_state || std::find(e->members.begin(), e->members.end(), h) != e->members.end() ||
+            (m > 0 && h->cfg.device != e->members[0]->cfg.device)) {
+            delete e;
+            return OC_ERR_ARG;
+        }
+        e->members.push_back(h);
+    }
+    e->device = e->members[0]->cfg.device;
+    cudaSetDevice(e->device);
+    bool ok = cudaStreamCreateWithFlags(&e->capture, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e->chain, cudaEventDisableTiming) == cudaSuccess;
+    for (int32_t m = 0; m < n && ok; ++m) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+        if (st) e->streams.push_back(st);
+        if (ev) e->joins.push_back(ev);
+    }
+    if (!ok) {
+        delete e;
+        return OC_ERR_CUDA;
+    }
+    *out = e;
+    return OC_OK;
+}
+
+int oc_ensemble_step(oc_ensemble* e, int32_t n_steps, void* stream) {
+    if (!e) return OC_ERR_ARG;
+    if (n_steps < 0) return OC_ERR_ARG;
+    cudaSetDevice(e->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    bool profiling = false;
+    for (auto* h : e->members) profiling = profiling || h->profiling;
+    const int pairs = profiling ? 0 : n_steps / 2;
+    if (pairs > 0) {
+        bool stale = !e->exec;
+        for (size_t m = 0; m < e->members.size() && !stale; ++m) {
+            const oc_handle* h = e->members[m];
+            const long long per_pair = h->solver ? 2LL * h->cfg.n_picard : 0;
+            stale = h->cur != e->parity[m] || h->graph_version != e->version[m] ||
+                    (h->solver && h->solves + per_pair * (pairs + 1) > h->solver->log_capacity());
+        }
+        if (stale) {
+            for (auto* h : e->members) {
+                const long long per_pair = h->solver ? 2LL * h->cfg.n_picard : 0;
+                const int rc = ensure_log(h, h->solves + per_pair * (pairs + 2), s);
+                if (rc) return rc;
+            }
+            const int rc = ensemble_record(e);
+            if (rc) return rc;
+        }
+        for (int i = 0; i < pairs; ++i) {
+            const cudaError_t ce = cudaGraphLaunch(e->exec, s);
+            if (ce != cudaSuccess) {
+                e->err = cudaGetErrorString(ce);
+                return OC_ERR_CUDA;
+            }
+            for (size_t m = 0; m < e->members.size(); ++m) {
+                oc_handle* h = e->members[m];
+                const oc_handle::Counters c = counters_of(h), d = e->delta[m];
+                set_counters(h, {c.steps + d.steps, c.tridiag + d.tridiag, c.rebuilds + d.rebuilds,
+                                 c.substeps + d.substeps, c.solves + d.solves, c.launches + d.launches});
+            }
+        }
+    }
+    // a remaining odd step (or every step while a member profiles): one member after another
+    for (int i = 2 * pairs; i < n_steps; ++i)
+        for (auto* h : e->members) {
+            h->last_stream = s;
+            const int rc = step_once(h, s);
+            if (rc) return rc;
+        }
+    return OC_OK;
+}
+
+const char* oc_ensemble_last_error(const oc_ensemble* e) { return e ? e->err.c_str() : "null ensemble"; }
+
+int oc_ensemble_destroy(oc_ensemble* e) {
+    if (!e) return OC_ERR_ARG;
+    cudaSetDevice(e->device);
+    cudaDeviceSynchronize();
+    delete e;
     return OC_OK;
 }
 

@@ -65,6 +65,9 @@ struct KP {
     const double2* dzx;    // per column: thickness of wet levels kfull and kfull + 1
     const int2* kface;     // per column: wet levels of its east (x) and north (y) face
     int face_rule;         // 0 min, 1 mean, 2 harmonic
+    // levels one CTA marches in k_mom_column and k_tracer_rhs (1..nz); every
+    // value gives the same results, only the speed depends on it
+    int mom_kl, tr_kl;
 };
 
 __device__ __forceinline__ int wrapi(int i, int n) {

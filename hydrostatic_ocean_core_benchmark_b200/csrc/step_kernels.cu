@@ -661,7 +661,7 @@ __device__ __forceinline__ double diff_flux(double Kk, double f_above, double f_
 // common-depth pressure gradient, the old-state Coriolis average, the explicit
 // vertical diffusion and the stress + advection/viscosity increment
 // (model3d_v05.py:352-370), in level-marching form: two threads per column of
-// a 32 x 8 tile, one for the u terms and one for the v terms, march MOM_KL
+// a 32 x 8 tile, one for the u terms and one for the v terms, march P.mom_kl
 // levels over the level planes the CTA stages in shared memory. The compact
 // geometry of the column and of its face's far neighbour is formed once; the
 // component's velocity and face thickness at the levels above and below roll
@@ -669,7 +669,6 @@ __device__ __forceinline__ double diff_flux(double Kk, double f_above, double f_
 // diffusive flux there are carried to the next level as the fluxes at its top
 // (a per-cell form forms each of them twice). Every value is formed by the
 // reference's operations in its order.
-constexpr int MOM_KL = 10;
 constexpr int MOM_TX = 32, MOM_TY = 8, MOM_RX = MOM_TX + 4, MOM_RY = MOM_TY + 4, MOM_RN = MOM_RX * MOM_RY;
 
 // the level's u, v and face masks of a tile plus a 2-column ring, in shared memory
@@ -703,8 +702,8 @@ __global__ void __launch_bounds__(MOM_TX * MOM_TY * 2, 2) k_mom_column(
     const int i = i0 + tx, j = j0 + ty;
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const bool live = i < nx && j < ny;
-    const int kbeg = blockIdx.z * MOM_KL;
-    const int kend = kbeg + MOM_KL < nz ? kbeg + MOM_KL : nz;
+    const int kbeg = blockIdx.z * P.mom_kl;
+    const int kend = kbeg + P.mom_kl < nz ? kbeg + P.mom_kl : nz;
     for (int r = tid; r < MOM_RN; r += nthreads) {
         const int rj = r / MOM_RX, ri = r - rj * MOM_RX;
         const int gcol = wrapi(j0 - 2 + rj, ny) * nx + wrapi(i0 - 2 + ri, nx);
@@ -966,7 +965,7 @@ __global__ void k_backsub(KP P, const double* __restrict__ ghu, const double* __
 
 // ------------------------------------------------------------------ tracers + EOS
 // Tiled right-hand sides of the implicit tracer solves (model3d_v05.py:466-512).
-// A CTA owns a TRX x TRY tile of columns and TR_KL levels and marches down the
+// A CTA owns a TRX x TRY tile of columns and P.tr_kl levels and marches down the
 // levels. At each level the horizontal face fluxes of the tile -- TRX + 1 east
 // faces per row, TRY + 1 north faces per column -- are formed once into shared
 // memory (double-buffered, one barrier per level); a per-cell form would form
@@ -974,7 +973,7 @@ __global__ void k_backsub(KP P, const double* __restrict__ ghu, const double* __
 // cell is carried to the next level as the face at its top, and the column's
 // tracer values, w and K_h roll in registers. Every face and cell value is
 // formed by the reference's operations in the reference's order.
-constexpr int TRX = 32, TRY = 8, TR_KL = 10;
+constexpr int TRX = 32, TRY = 8;
 
 struct Stencil4 {
     int cm, c0, c1, cp;  // far upstream, the two cells of the face, far downstream (flat 2D)
@@ -1061,8 +1060,8 @@ __global__ void __launch_bounds__(TRX * TRY, 4) k_tracer_rhs(KP P, const double*
     const bool ts = P.tracers_ts;
     const int nf = ts ? 2 : 1;
     const bool adv = P.advection != 0;
-    const int kbeg = blockIdx.z * TR_KL;
-    const int kend = kbeg + TR_KL < nz ? kbeg + TR_KL : nz;
+    const int kbeg = blockIdx.z * P.tr_kl;
+    const int kend = kbeg + P.tr_kl < nz ? kbeg + P.tr_kl : nz;
     // faces this thread forms: the west and south faces of its cell, and for two
     // warps the east faces of the tile's last column / north faces of its last row
     const bool xextra = ty == TRY - 2 && tx < TRY, yextra = ty == TRY - 1;
@@ -1556,7 +1555,7 @@ void launch_mom_explicit(const KP& P, const double* u, const double* v, const do
                          const double* phi, const double* w, const double* km, double* pgx,
                          double* pgy, double* avpv, double* avpu, double* dzu, double* dzv,
                          double* stu, double* stv, cudaStream_t s) {
-    const dim3 grid((P.nx + MOM_TX - 1) / MOM_TX, (P.ny + MOM_TY - 1) / MOM_TY, (P.nz + MOM_KL - 1) / MOM_KL);
+    const dim3 grid((P.nx + MOM_TX - 1) / MOM_TX, (P.ny + MOM_TY - 1) / MOM_TY, (P.nz + P.mom_kl - 1) / P.mom_kl);
     k_mom_column<<<grid, dim3(MOM_TX, MOM_TY, 2), 0, s>>>(P, u, v, b, phi, w, km, pgx, pgy, avpv, avpu, dzu, dzv, stu,
                                              stv);
 }
@@ -1583,7 +1582,7 @@ void launch_backsub(const KP& P, const double* ghu, const double* ghv, const dou
 void launch_tracer_rhs(const KP& P, const double* T, const double* S, const double* bold,
                        const double* u, const double* v, const double* w, const double* kh, double* rT,
                        double* rS, cudaStream_t s) {
-    const dim3 grid((P.nx + TRX - 1) / TRX, (P.ny + TRY - 1) / TRY, (P.nz + TR_KL - 1) / TR_KL);
+    const dim3 grid((P.nx + TRX - 1) / TRX, (P.ny + TRY - 1) / TRY, (P.nz + P.tr_kl - 1) / P.tr_kl);
     k_tracer_rhs<<<grid, dim3(TRX, TRY), 0, s>>>(P, T, S, bold, u, v, w, kh, rT, rS);
 }
 

@@ -157,6 +157,17 @@ class OceanStepper:
         sp = getattr(stream, "cuda_stream", stream)
         self._call("oc_get_state_async", self.lib.oc_get_state_async, self.h, C.byref(view), dev, sp)
 
+    # ------------------------------------------------------------------ tiling
+    def set_tiling(self, mom_levels: int, tracer_levels: int):
+        """Levels one CTA marches in the momentum / tracer kernels (oc_set_tiling)."""
+        self._call("oc_set_tiling", self.lib.oc_set_tiling, self.h, int(mom_levels), int(tracer_levels))
+
+    def autotune(self) -> tuple[int, int]:
+        """Time the candidates on the current state and keep the fastest (oc_autotune)."""
+        mk, tk = C.c_int32(), C.c_int32()
+        self._call("oc_autotune", self.lib.oc_autotune, self.h, C.byref(mk), C.byref(tk))
+        return int(mk.value), int(tk.value)
+
     # ------------------------------------------------------------------ slab halos
     def halo_values_per_row(self) -> int:
         """Doubles one row of all exchanged fields takes (oc_halo_values_per_row)."""
@@ -293,6 +304,41 @@ def thomas(sub, diag, sup, rhs):
 
 # ---------------------------------------------------------------------------
 # reference-shaped interface
+
+
+class OceanEnsemble:
+    """Members (``OceanStepper`` objects of any grid size, on one GPU, states set)
+    advanced together by one recorded CUDA graph per two steps (oc_ensemble_*):
+    every member on its own branch, the Helmholtz solves one after another.
+    Each member's results equal those of the member stepped alone."""
+
+    def __init__(self, members):
+        self.lib = _lib.load()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.h.value for m in self.members])
+        e = C.c_void_p()
+        rc = self.lib.oc_ensemble_create(arr, len(self.members), C.byref(e))
+        if rc:
+            raise _lib.OceanError(f"oc_ensemble_create failed ({rc})")
+        self.e = e
+
+    def step(self, n_steps: int = 1, stream=None):
+        sp = getattr(stream, "cuda_stream", stream)
+        rc = self.lib.oc_ensemble_step(self.e, int(n_steps), sp)
+        if rc:
+            msg = self.lib.oc_ensemble_last_error(self.e)
+            raise _lib.OceanError(f"oc_ensemble_step failed ({rc}): {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "e", None):
+            self.lib.oc_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
 
 
 @dataclass(frozen=True)

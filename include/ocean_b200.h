@@ -149,6 +149,31 @@ int oc_set_domain_slab(oc_handle* h, const double* H, const double* mask, const 
  * level, into the device buffer `buf` (values_per_row * nrows doubles), and
  * oc_unpack_rows writes such a buffer into those rows and recomputes w for the
  * velocities now in the state. Asynchronous on `stream`. */
+/* Levels one CTA marches in the explicit-momentum and tracer right-hand-side
+ * kernels (1..nz; 10 or nz by default). Every value gives the same results bit
+ * for bit; only the speed depends on it. oc_set_tiling sets both; oc_autotune
+ * times each kernel on the current state over a candidate list, keeps the
+ * fastest and returns the choice (synchronous). No reference counterpart:
+ * the tile shapes of the batched-ensemble form. */
+int oc_set_tiling(oc_handle* h, int32_t mom_levels, int32_t tracer_levels);
+int oc_autotune(oc_handle* h, int32_t* mom_levels, int32_t* tracer_levels);
+
+/* An ensemble: several handles (members of any grid size, on one device, each
+ * with its state set) advanced together. oc_ensemble_step records two steps of
+ * every member into one CUDA graph -- each member on a branch of its own, its
+ * kernels free to overlap the other members', the cooperative Helmholtz solves
+ * of all members ordered one after another -- and replays it n_steps / 2 times
+ * on `stream`; an odd last step, or any step while a member profiles, runs
+ * member after member. Every member's results and counters equal those of the
+ * member stepped alone. The graph is recorded again when a member's buffers,
+ * forcing, tiling or solve-log capacity changed. No reference counterpart: the
+ * batched-ensemble form. */
+typedef struct oc_ensemble oc_ensemble;
+int oc_ensemble_create(oc_handle* const* members, int32_t n_members, oc_ensemble** out);
+int oc_ensemble_step(oc_ensemble* e, int32_t n_steps, void* stream);
+const char* oc_ensemble_last_error(const oc_ensemble* e);
+int oc_ensemble_destroy(oc_ensemble* e);
+
 int oc_halo_values_per_row(oc_handle* h, int64_t* count);
 int oc_pack_rows(oc_handle* h, int32_t j0, int32_t nrows, double* buf, void* stream);
 int oc_unpack_rows(oc_handle* h, int32_t j0, int32_t nrows, const double* buf, void* stream);

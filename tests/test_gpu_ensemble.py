@@ -1,0 +1,75 @@
+"""Batched-ensemble form on the GPU.
+
+Members of uneven grid sizes advanced together by one recorded CUDA graph per
+two steps (oc_ensemble_*) must equal the same members stepped alone, bit for
+bit, with the same counters and solve logs; the tiling knob (levels per CTA of
+the momentum and tracer kernels, set by hand or by the autotuner) must leave
+every bit unchanged.
+"""
+
+import numpy as np
+import pytest
+
+from hydrostatic_ocean_core_benchmark_b200 import cases
+
+pytestmark = pytest.mark.gpu
+FIELDS = ("eta", "u", "v", "b", "T", "S", "e", "km", "kh")
+MEMBERS = [(40, 36, 12, 3), (48, 40, 10, 4), (32, 56, 8, 5)]  # nx, ny, nz, seed
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    import torch
+    assert torch.cuda.is_available()
+    torch.cuda.set_device(0)
+
+
+def _member(nx, ny, nz, seed):
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=seed)
+    st = OceanStepper(s.params, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
+    return st
+
+
+def _same(a, b, what):
+    sa, sb = a.get_state(), b.get_state()
+    for f in FIELDS:
+        assert np.array_equal(sa[f], sb[f]), f"{what}: {f} differs"
+
+
+def test_levels_per_cta_change_no_bit():
+    a, b, c = (_member(40, 36, 12, 3) for _ in range(3))
+    b.set_tiling(3, 5)
+    mk, tk = c.autotune()
+    assert 1 <= mk <= 12 and 1 <= tk <= 12
+    for st in (a, b, c):
+        st.step(4)
+    _same(a, b, "levels per CTA 3 / 5")
+    _same(a, c, f"autotuned levels per CTA {mk} / {tk}")
+    with pytest.raises(Exception):
+        a.set_tiling(0, 13)
+    for st in (a, b, c):
+        st.close()
+
+
+def test_ensemble_equals_members_stepped_alone():
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanEnsemble
+    together = [_member(*m) for m in MEMBERS]
+    alone = [_member(*m) for m in MEMBERS]
+    for st in together:
+        st.autotune()
+    ens = OceanEnsemble(together)
+    ens.step(5)   # two graph replays, then one step member after member
+    ens.step(4)   # the buffers swapped: recorded again, then two replays
+    for st in alone:
+        st.step(9)
+    keys = ("steps", "solver_iterations", "solver_failures", "solver_rebuilds", "tridiagonal_solves")
+    for m, (a, b) in enumerate(zip(together, alone)):
+        _same(a, b, f"member {m} {MEMBERS[m][:3]}")
+        sa, sb = a.stats(), b.stats()
+        assert all(sa[k] == sb[k] for k in keys), (m, {k: (sa[k], sb[k]) for k in keys})
+        assert a.solve_log() == b.solve_log()
+    ens.close()
+    for st in together + alone:
+        st.close()
