@@ -474,6 +474,90 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+def run_ensemble(args, rank, world, local_rank):
+    """Batched-ensemble form: members with seeded uneven grids (nx, ny drawn from the
+    multiples of 32 in 128..384, nz in {24, 32, 48}: the multigrid halves a grid only
+    while its sizes are even, and on sizes with an odd factor above 8 the stationary
+    multigrid -- the reference's algorithm -- falls back to smoothing and needs
+    thousands of cycles), each the seamount-basin recipe with its own seed, tuned by
+    oc_autotune, advanced together by one recorded graph per two steps
+    (oc_ensemble_step); beside it the same members stepped one after another, each
+    with its own recorded graphs."""
+    import numpy as np
+    import torch
+
+    from hydrostatic_ocean_core_benchmark_b200 import cases
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanEnsemble, OceanStepper
+
+    torch.cuda.set_device(local_rank)
+    rng = np.random.default_rng(args.seed + 5)
+    members, shapes = [], []
+    for m in range(args.ens_members):
+        nx, ny = (32 * int(x) for x in rng.integers(4, 13, 2))
+        nz = int(rng.choice([24, 32, 48]))
+        s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=args.seed + 1000 * (rank + 1) + m)
+        st = OceanStepper(s.params, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c,
+                          device=local_rank)
+        st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
+        members.append(st)
+        shapes.append((nx, ny, nz))
+    cells = sum(nx * ny * nz for nx, ny, nz in shapes)
+    tiling = [st.autotune() for st in members]
+    stream = torch.cuda.Stream(device=local_rank)
+    steps = args.steps + (args.steps % 2)
+    warm = max(args.warmup, 3)
+    warm += warm % 2
+    ens = OceanEnsemble(members)
+    ens.step(warm, stream=stream)
+    ens.step(2, stream=stream)          # the graph of the timed region's starting buffers
+    stream.synchronize()
+    out_dir = ROOT / "gpurun_out"
+    clocks = ClockSampler(local_rank, out_dir / f"clocks_ens_rank{rank}.csv" if out_dir.is_dir() else None)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    ens.step(steps, stream=stream)
+    ev1.record(stream)
+    ev1.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    # the same members one after another, each replaying its own recorded graphs
+    for st in members:
+        st.step(2, stream=stream, graph=True)
+    stream.synchronize()
+    ev0.record(stream)
+    for st in members:
+        st.step(steps, stream=stream, graph=True)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms_seq = ev0.elapsed_time(ev1)
+    failures = sum(st.stats()["solver_failures"] for st in members)
+    diverged = sum(st.stats()["diverged"] for st in members)
+    if failures or diverged:
+        raise RuntimeError(f"ensemble run failed: {failures} solver failures, {diverged} diverged members")
+    line = {"metric": METRIC, "value": world * cells * steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": ms / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded seamount-basin recipe per member; inputs generated on the host)",
+            "config": {"workload": f"ensemble of {len(members)} seamount basins, nx, ny multiples of 32 in 128..384, "
+                                   "nz in {24, 32, 48}, theta=0.6 + multigrid, TKE, TVD3, polyTEOS10",
+                       "members": len(members), "cells": cells,
+                       "grids": [list(g) for g in shapes[:8]] + (["..."] if len(shapes) > 8 else []),
+                       "parallelism": "replicas x1"},
+            "sequential": {"value": world * cells * steps / (ms_seq / 1e3), "unit": UNIT,
+                           "ms_per_step": ms_seq / steps,
+                           "path": "members one after another, each with its own recorded graphs"},
+            "tiling": {"levels_per_cta_momentum": sorted(set(t[0] for t in tiling)),
+                       "levels_per_cta_tracers": sorted(set(t[1] for t in tiling))},
+            "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ens.close()
+    for st in members:
+        st.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -493,12 +577,18 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-nx", type=int, default=128)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["seamount", "ensemble"], default="seamount",
+                    help="seamount: the 512x512x50 basin (the headline line); ensemble: the "
+                         "batched-ensemble form (its own line)")
+    ap.add_argument("--ens-members", type=int, default=64)
     args = ap.parse_args()
     rank = env_int("RANK", 0)
     world = env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         return run_reference_arm(args, rank)
+    if args.workload == "ensemble":
+        return run_ensemble(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

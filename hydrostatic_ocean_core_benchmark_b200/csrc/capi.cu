@@ -1217,8 +1217,10 @@ int ensemble_record(oc_ensemble* e) {
         cur[m] = h->cur;
     }
     cudaGraph_t g = nullptr;
+    std::string why;
     cudaError_t ce = cudaStreamBeginCapture(e->capture, cudaStreamCaptureModeThreadLocal);
     int rc = ce == cudaSuccess ? OC_OK : OC_ERR_CUDA;
+    if (rc) why = std::string("begin capture: ") + cudaGetErrorString(ce);
     if (rc == OC_OK) {
         cudaEventRecord(e->fork, e->capture);
         cudaEventRecord(e->chain, e->capture);  // the chain starts inside the recording
@@ -1232,6 +1234,7 @@ int ensemble_record(oc_ensemble* e) {
                 rc = step_once(h, e->streams[m]);
                 h->solve_chain = nullptr;
                 h->profiling = prof;
+                if (rc) why = "member " + std::to_string(m) + ": " + h->err;
             }
         for (size_t m = 0; m < n; ++m) {
             cudaEventRecord(e->joins[m], e->streams[m]);
@@ -1239,8 +1242,17 @@ int ensemble_record(oc_ensemble* e) {
         }
     }
     ce = cudaStreamEndCapture(e->capture, &g);
-    if (rc == OC_OK && ce != cudaSuccess) rc = OC_ERR_CUDA;
-    if (rc == OC_OK && cudaGraphInstantiate(&e->exec, g, 0) != cudaSuccess) rc = OC_ERR_CUDA;
+    if (rc == OC_OK && ce != cudaSuccess) {
+        rc = OC_ERR_CUDA;
+        why = std::string("end capture: ") + cudaGetErrorString(ce);
+    }
+    if (rc == OC_OK) {
+        ce = cudaGraphInstantiate(&e->exec, g, 0);
+        if (ce != cudaSuccess) {
+            rc = OC_ERR_CUDA;
+            why = std::string("instantiate: ") + cudaGetErrorString(ce);
+        }
+    }
     if (g) cudaGraphDestroy(g);
     cudaGetLastError();
     e->parity = cur;
@@ -1259,7 +1271,7 @@ int ensemble_record(oc_ensemble* e) {
     if (rc) {
         if (e->exec) cudaGraphExecDestroy(e->exec);
         e->exec = nullptr;
-        e->err = "the ensemble's steps could not be recorded";
+        e->err = "the ensemble's steps could not be recorded (" + why + ")";
     }
     return rc;
 }

@@ -20,6 +20,8 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -1203,8 +1205,18 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
         err = "Helmholtz grid too large for the single-pass reduction tree";
         return OC_ERR_UNSUPPORTED;
     }
-    if (smem_ > 48 * 1024)
-        cudaFuncSetAttribute(k_helm_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_);
+    if (smem_ > 48 * 1024) {
+        // the allowance belongs to the kernel on this device, not to this solver:
+        // it only ever grows, so the solvers of other grids keep launching
+        static std::mutex mu;
+        static std::map<int, size_t> allowance;
+        std::lock_guard<std::mutex> lock(mu);
+        size_t& a = allowance[dev];
+        if (smem_ > a) {
+            cudaFuncSetAttribute(k_helm_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_);
+            a = smem_;
+        }
+    }
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_helm_solve, block_, smem_);
     if (per_sm < 1) {

@@ -14,7 +14,9 @@ from hydrostatic_ocean_core_benchmark_b200 import cases
 
 pytestmark = pytest.mark.gpu
 FIELDS = ("eta", "u", "v", "b", "T", "S", "e", "km", "kh")
-MEMBERS = [(40, 36, 12, 3), (48, 40, 10, 4), (32, 56, 8, 5)]  # nx, ny, nz, seed
+# nx, ny, nz, seed: the solvers of the two larger grids need different amounts of
+# shared memory, created largest first
+MEMBERS = [(512, 512, 6, 3), (256, 256, 6, 4), (40, 36, 12, 5)]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -66,6 +68,7 @@ def test_ensemble_equals_members_stepped_alone():
         st.step(9)
     keys = ("steps", "solver_iterations", "solver_failures", "solver_rebuilds", "tridiagonal_solves")
     for m, (a, b) in enumerate(zip(together, alone)):
+        assert a.stats()["solver_failures"] == 0
         _same(a, b, f"member {m} {MEMBERS[m][:3]}")
         sa, sb = a.stats(), b.stats()
         assert all(sa[k] == sb[k] for k in keys), (m, {k: (sa[k], sb[k]) for k in keys})
