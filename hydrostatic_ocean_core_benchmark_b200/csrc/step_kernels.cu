@@ -836,12 +836,20 @@ __global__ void __launch_bounds__(256) k_predictor_rhs(
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
     if (i >= P.nx || j >= P.ny) return;
-    Nbr nb;
-    nb.init(i, j, P.nx, P.ny);
-    const int c = nb.c;
+    const int c = j * P.nx + i;
     const size_t o = (size_t)k * P.n2;
-    const double vcor = P.one_m_tc * avpv[o + c] + P.theta_cor * v_on_u(P, nb, v_it, o, k);
-    const double ucor = P.one_m_tc * avpu[o + c] + P.theta_cor * u_on_v(P, nb, u_it, o, k);
+    const double av_v = avpv[o + c], av_u = avpu[o + c];
+    // the iterate's averages; in the first pass the iterate is the old state,
+    // whose averages the explicit-terms kernel formed already by the same function
+    double it_v = av_v, it_u = av_u;
+    if (u_it != u || v_it != v) {
+        Nbr nb;
+        nb.init(i, j, P.nx, P.ny);
+        it_v = v_on_u(P, nb, v_it, o, k);
+        it_u = u_on_v(P, nb, u_it, o, k);
+    }
+    const double vcor = P.one_m_tc * av_v + P.theta_cor * it_v;
+    const double ucor = P.one_m_tc * av_u + P.theta_cor * it_u;
     double gu, gv;
     if (P.scheme != 2) {
         const double m3u_k = col_m3u(P, c, k), m3v_k = col_m3v(P, c, k);
