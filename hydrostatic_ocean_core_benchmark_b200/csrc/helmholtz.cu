@@ -482,16 +482,34 @@ __device__ void mg_down(const HelmParams& H, int l, const double* xin, double* x
         const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
         tile_load<S>(L, i0, j0, xin, nullptr, t, !keep);
         tile_four_half_sweeps<S>(L, i0, j0, t, 0);
-        for (int r = threadIdx.x; r < (S::TX / 2) * (S::TY / 2); r += blockDim.x) {
-            const int cj = r / (S::TX / 2), ci = r - cj * (S::TX / 2);
-            const int I = i0 / 2 + ci, J = j0 / 2 + cj;
-            if (I >= C.nx || J >= C.ny) continue;
-            const int r00 = (HALO + 2 * cj) * S::RW + HALO + 2 * ci;
-            const double a = tile_residual<S>(L, H.coef, t, r00);
-            const double b = tile_residual<S>(L, H.coef, t, r00 + 1);
-            const double c = tile_residual<S>(L, H.coef, t, r00 + S::RW);
-            const double d = tile_residual<S>(L, H.coef, t, r00 + S::RW + 1);
-            C.b[J * C.nx + I] = 0.25 * (a + b + c + d);
+        constexpr int NC = (S::TX / 2) * (S::TY / 2);  // coarse cells of the tile
+        if constexpr (4 * NC <= 1024 && (4 * NC) % 32 == 0 && S::TX != TileWide::TX) {
+            // four lanes per coarse cell, one child residual each, summed by the
+            // first of them in the order a + b + c + d (the loop bound is a
+            // multiple of 32, so whole warps take part in the shuffles)
+            for (int q = threadIdx.x; q < 4 * NC; q += blockDim.x) {
+                const int r = q >> 2, child = q & 3;
+                const int cj = r / (S::TX / 2), ci = r - cj * (S::TX / 2);
+                const int I = i0 / 2 + ci, J = j0 / 2 + cj;
+                const int rr = (HALO + 2 * cj + (child >> 1)) * S::RW + HALO + 2 * ci + (child & 1);
+                const double val = tile_residual<S>(L, H.coef, t, rr);
+                const double b = __shfl_down_sync(0xffffffffu, val, 1);
+                const double c = __shfl_down_sync(0xffffffffu, val, 2);
+                const double d = __shfl_down_sync(0xffffffffu, val, 3);
+                if (child == 0 && I < C.nx && J < C.ny) C.b[J * C.nx + I] = 0.25 * (val + b + c + d);
+            }
+        } else {
+            for (int r = threadIdx.x; r < NC; r += blockDim.x) {
+                const int cj = r / (S::TX / 2), ci = r - cj * (S::TX / 2);
+                const int I = i0 / 2 + ci, J = j0 / 2 + cj;
+                if (I >= C.nx || J >= C.ny) continue;
+                const int r00 = (HALO + 2 * cj) * S::RW + HALO + 2 * ci;
+                const double a = tile_residual<S>(L, H.coef, t, r00);
+                const double b = tile_residual<S>(L, H.coef, t, r00 + 1);
+                const double c = tile_residual<S>(L, H.coef, t, r00 + S::RW);
+                const double d = tile_residual<S>(L, H.coef, t, r00 + S::RW + 1);
+                C.b[J * C.nx + I] = 0.25 * (a + b + c + d);
+            }
         }
         tile_store_x<S>(L, i0, j0, t, xout);
         __syncthreads();
