@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(128, 8) k_wcol(KP P, const double* __restrict_
     const int kuw = P.kface[cw].x, kvs = P.kface[cs_].y;
     double acc = 0.0;
     w[(size_t)nz * n2 + c] = 0.0;
-#pragma unroll 4
+#pragma unroll 2
     for (int k = nz - 1; k >= 0; --k) {
         const size_t o = (size_t)k * n2;
         double m3, m;
