@@ -32,6 +32,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import sys
 import statistics
 import time
 from pathlib import Path
@@ -271,11 +272,15 @@ def _read_bundle(p: OceanParams):
 def run_namelist(nml: str, halo: int = DEFAULT_HALO) -> int:
     """The multi-device binary's protocol (cfd_exp3d5_cuda_multi.cu:58-265) for the
     rank this process is; rank 0 writes the state and metrics files."""
-    import torch
     p = read_namelist(nml)
     dist = _dist()
     rank = dist.get_rank() if dist else 0
     nranks = dist.get_world_size() if dist else 1
+    # what the run refuses, before any device work (cfd_exp3d5_cuda_multi.cu:73-76)
+    if p.scheme_name != "fb":
+        raise ValueError(f"the multi-device run supports scheme fb only (got {p.scheme_name})")
+    SlabLayout(p.ny, nranks, halo)
+    import torch
     device = int(os.environ.get("LOCAL_RANK", 0)) if torch.cuda.device_count() > 1 else 0
     torch.cuda.set_device(device)
     H, mask, state, dzr, taux, tauy = _read_bundle(p)
@@ -344,12 +349,14 @@ def main(argv=None) -> int:
     import torch
     import torch.distributed as dist
     if "WORLD_SIZE" in os.environ and not dist.is_initialized():
+        import datetime
         backend = "nccl" if torch.cuda.device_count() >= int(os.environ["WORLD_SIZE"]) else "gloo"
-        dist.init_process_group(backend)
+        # a rank that dies ends the others' next exchange with an error, not a hang
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     try:
         rc = run_namelist(args.namelist, args.halo)
     except ValueError as e:
-        print(f"FATAL: {e}", flush=True)
+        print(f"FATAL: {e}", file=sys.stderr, flush=True)
         rc = 2
     if dist.is_initialized():
         dist.destroy_process_group()

@@ -176,3 +176,26 @@ def test_one_rank_exchanges_with_itself():
     want = _global_run("closed", 5)
     for k in want:
         assert np.array_equal(got[k], want[k]), k
+
+
+def _bundle(tmp_path, scheme, ny):
+    from hydrostatic_ocean_core_benchmark_b200.params import write_namelist
+    p = OceanParams(nx=8, ny=ny, nz=4, scheme_name=scheme, out_prefix=str(tmp_path / "out"))
+    return write_namelist(str(tmp_path / "case.nml"), p)
+
+
+@pytest.mark.parametrize("scheme,ny,halo,what", [("theta", 40, 16, "fb only"), ("fb", 12, 16, "halo")])
+def test_front_end_refuses_before_any_device_work(tmp_path, scheme, ny, halo, what):
+    """The multi-device front end refuses other schemes and ranks thinner than the
+    halo with FATAL and exit code 2, as the reference's binary does."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    nml = _bundle(tmp_path, scheme, ny)
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, "-m", "hydrostatic_ocean_core_benchmark_b200.slab", str(nml),
+                        "--halo", str(halo)], capture_output=True, text=True, cwd=root, timeout=300,
+                       env={**env, "PYTHONPATH": str(root)})
+    assert r.returncode == 2, r.stdout + r.stderr
+    assert "FATAL" in r.stderr and what in r.stderr
