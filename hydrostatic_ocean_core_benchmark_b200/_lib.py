@@ -114,6 +114,8 @@ _SIGNATURES = {
                                 C.POINTER(C.c_int32), C.c_void_p]),
     "oc_helm_last_error": (C.c_char_p, [C.c_void_p]),
     "oc_helm_destroy": (C.c_int, [C.c_void_p]),
+    "oc_helm_refine_report": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    "oc_helm_set_inner_rtol": (C.c_int, [C.c_void_p, C.c_double]),
     "oc_density": (C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "oc_get_field": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]),

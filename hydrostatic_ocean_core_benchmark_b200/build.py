@@ -24,7 +24,8 @@ EXE = BIN_DIR / "ocean3d5_b200"
 # executables over the C ABI: (main source, binary)
 MAINS = [("ocean3d5_main.cpp", EXE), ("helmholtz_bench_main.cpp", BIN_DIR / "helmholtz_bench_b200"),
          ("eos_bench_main.cpp", BIN_DIR / "eos_bench_b200")]
-SOURCES = ["step_kernels.cu", "helmholtz.cu", "capi.cu", "thomas_noalloc.cu", "standalone.cu", "protocol.cpp"]
+SOURCES = ["step_kernels.cu", "helmholtz.cu", "helm_refined.cu", "capi.cu", "thomas_noalloc.cu", "standalone.cu",
+           "protocol.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--extended-lambda",
          "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{ROOT / 'include'}", f"-I{CSRC}"]

@@ -27,11 +27,11 @@
 #include <vector>
 
 #include "ocean_b200.h"
+#include "grid_barrier.cuh"
 #include "helmholtz.cuh"
 
 namespace oc {
 
-static constexpr long long kBarrierCycles = 2000000000LL;
 static constexpr int kCoarseCells = 1024;
 // fine-level tiles: interior TX x TY cells plus a halo of HALO cells, enough
 // for four red-black half-sweeps and one residual on a shrinking region
@@ -50,65 +50,10 @@ using TileWide = TileShape<128, 16>;  // level 0 of large grids: one tile per CT
 enum { SHAPE_32 = 0, SHAPE_3216 = 1, SHAPE_16 = 2, SHAPE_8 = 3, SHAPE_WIDE = 4 };
 
 // ------------------------------------------------------------------ barrier
-// Grid barrier over a 64-bit arrival counter that only grows: barrier n of a
-// launch completes when the counter reaches base + (n + 1) * gridDim.x, so it
-// needs no reset and no generation word. The first barrier of a launch learns
-// the base from its own arrival (an atomic add with release semantics); later
-// arrivals are release reductions, whose value nobody waits for. The wait is an
-// acquire spin on the counter, bounded in time. A CTA that gives up records
-// OC_ERR_TIMEOUT in the status word, which the waiting CTAs poll, so every CTA
-// leaves the solve; the status is sticky, so a later launch that finds it set
-// makes no arrivals and the counter stays a multiple of the grid. Thread 0
-// hands the outcome to its CTA through shared memory.
-struct GridBar {
-    unsigned long long next;  // counter value that completes the next barrier; 0 before the first
-    int ok;
-};
-static __shared__ GridBar s_gbar;
+// the bounded grid barrier of grid_barrier.cuh on the solver's counter and status
+__device__ __forceinline__ void grid_sync_begin(const HelmParams& H) { grid_sync_begin(H.status); }
 
-__device__ __forceinline__ void grid_sync_begin(const HelmParams& H) {
-    if (threadIdx.x == 0) {
-        s_gbar.next = 0;
-        s_gbar.ok = *((volatile int*)H.status) == 0;
-    }
-}
-
-// thread 0's arrival and wait, out of line: the solve calls the barrier from many places
-__device__ __noinline__ void grid_arrive_wait(unsigned long long* cnt, int* status) {
-    unsigned long long target = s_gbar.next;
-    if (target == 0) {
-        unsigned long long old;
-        asm volatile("atom.add.release.gpu.u64 %0, [%1], 1;" : "=l"(old) : "l"(cnt) : "memory");
-        target = old - old % gridDim.x + gridDim.x;
-    } else {
-        asm volatile("red.add.release.gpu.u64 [%0], 1;" ::"l"(cnt) : "memory");
-    }
-    s_gbar.next = target + gridDim.x;
-    const long long t0 = clock64();
-    for (unsigned spin = 1;; ++spin) {
-        unsigned long long v;
-        asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(v) : "l"(cnt) : "memory");
-        if (v >= target) break;
-        if ((spin & 63) == 0) {
-            if (*((volatile int*)status) != 0) {
-                s_gbar.ok = 0;
-                break;
-            }
-            if (clock64() - t0 > kBarrierCycles) {
-                atomicExch(status, OC_ERR_TIMEOUT);
-                s_gbar.ok = 0;
-                break;
-            }
-        }
-    }
-}
-
-__device__ __forceinline__ bool grid_sync(const HelmParams& H) {
-    __syncthreads();
-    if (threadIdx.x == 0 && s_gbar.ok) grid_arrive_wait(H.bar_count, H.status);
-    __syncthreads();
-    return s_gbar.ok != 0;
-}
+__device__ __forceinline__ bool grid_sync(const HelmParams& H) { return grid_sync(H.bar_count, H.status); }
 
 // ------------------------------------------------------------------ level operators
 struct Cell {

@@ -14,6 +14,9 @@
 // "residual" is the true relative residual ||rhs - A x|| / ||rhs|| of the
 // returned solution, formed in fp64 on the host with the operator of
 // libs/core/solvers_var.py:47-53.
+// Besides the reference's four solvers, solver "pcg_refined" (no reference
+// counterpart) runs the FP32-inner, FP64-refined solver; its JSON then says
+// "precision": "fp32+fp64-refined".
 
 #include <cuda_runtime.h>
 
@@ -132,6 +135,7 @@ int main(int argc, char** argv) {
     else if (cs.solver == "pcg_rbgs") kind = OC_SOLVER_PCG_RBGS;
     else if (cs.solver == "rbgs") kind = OC_SOLVER_RBGS;
     else if (cs.solver == "multigrid") kind = OC_SOLVER_MULTIGRID;
+    else if (cs.solver == "pcg_refined") kind = OC_SOLVER_PCG_REFINED;  // FP32 inner, FP64 refinement
     if (kind < 0) {
         std::fprintf(stderr, "FATAL: unknown solver %s\n", cs.solver.c_str());
         return 1;
@@ -209,11 +213,11 @@ int main(int argc, char** argv) {
         return 1;
     }
     std::fprintf(f,
-                 "{\n  \"backend\": \"cuda_b200\",\n  \"precision\": \"fp64\",\n  \"solver\": \"%s\",\n"
+                 "{\n  \"backend\": \"cuda_b200\",\n  \"precision\": \"%s\",\n  \"solver\": \"%s\",\n"
                  "  \"nx\": %d,\n  \"ny\": %d,\n  \"iterations\": %d,\n  \"converged\": %s,\n"
                  "  \"wall_s\": %.16e,\n  \"wall_mad_s\": %.16e,\n  \"wall_min_s\": %.16e,\n"
                  "  \"residual\": %.16e,\n  \"l2_rel_vs_reference\": %.16e,\n  \"n_repeat\": %d\n}\n",
-                 cs.solver.c_str(), cs.nx, cs.ny, iters, conv ? "true" : "false", wall, wall_mad, wall_min,
+                 kind == OC_SOLVER_PCG_REFINED ? "fp32+fp64-refined" : "fp64", cs.solver.c_str(), cs.nx, cs.ny, iters, conv ? "true" : "false", wall, wall_mad, wall_min,
                  residual, err, cs.n_repeat);
     std::fclose(f);
     std::printf("solver=%12s iters=%8d wall=%12.5e l2_vs_ref=%12.5e\n", cs.solver.c_str(), iters, wall, err);

@@ -7,18 +7,21 @@
 //   - the three equations of state on flat arrays (reference
 //     libs/cuda/src/eos_bench.cu over libs/core/eos.py) -> oc_density.
 // The solver is the step's own persistent cooperative HelmSolver, so its
-// iteration counts and solutions are those of the step's solves.
+// iteration counts and solutions are those of the step's solves; solver kind
+// OC_SOLVER_PCG_REFINED selects the mixed-precision RefinedHelm instead.
 
 #include <cuda_runtime.h>
 
 #include <string>
 
+#include "helm_refined.cuh"
 #include "helmholtz.cuh"
 #include "ocean_b200.h"
 #include "oc_internal.cuh"
 
 struct oc_helm {
     oc::HelmSolver solver;
+    oc::RefinedHelm* refined = nullptr;  // set for OC_SOLVER_PCG_REFINED
     double* ku = nullptr;
     double* kv = nullptr;
     double* rhs = nullptr;  // device staging for host right-hand sides
@@ -27,6 +30,7 @@ struct oc_helm {
     int nx = 0, ny = 0, device = 0;
     std::string err;
     ~oc_helm() {
+        delete refined;
         for (void* p : {(void*)ku, (void*)kv, (void*)rhs, (void*)x, (void*)status})
             if (p) cudaFree(p);
     }
@@ -60,7 +64,7 @@ extern "C" int oc_helm_create(const oc_helm_config* cfg, const double* ku, const
     *out = nullptr;
     if (cfg->nx < 2 || cfg->ny < 2 || !(cfg->dx > 0.0) || !(cfg->dy > 0.0) || !(cfg->coef >= 0.0) ||
         !(cfg->rtol > 0.0) || cfg->max_iter < 1 || cfg->solver < OC_SOLVER_PCG_JACOBI ||
-        cfg->solver > OC_SOLVER_MULTIGRID)
+        cfg->solver > OC_SOLVER_PCG_REFINED)
         return OC_ERR_ARG;
     if (cudaSetDevice(cfg->device) != cudaSuccess) return OC_ERR_CUDA;
     oc_helm* h = new oc_helm();
@@ -80,13 +84,23 @@ extern "C" int oc_helm_create(const oc_helm_config* cfg, const double* ku, const
     cudaMemset(h->status, 0, sizeof(int));
     cudaMemcpy(h->ku, ku, bytes, cudaMemcpyHostToDevice);
     cudaMemcpy(h->kv, kv, bytes, cudaMemcpyHostToDevice);
-    const int rc = h->solver.init(cfg->nx, cfg->ny, cfg->dx, cfg->dy, cfg->coef, cfg->solver, cfg->rtol,
-                                  cfg->max_iter, mask, h->ku, h->kv, 1, h->status, h->err);
-    if (rc) {
-        delete h;
-        return rc;
+    if (cfg->solver == OC_SOLVER_PCG_REFINED) {
+        h->refined = new oc::RefinedHelm();
+        const int rc = h->refined->init(cfg->nx, cfg->ny, cfg->dx, cfg->dy, cfg->coef, cfg->rtol, cfg->max_iter,
+                                        mask, h->ku, h->kv, h->err);
+        if (rc) {
+            delete h;
+            return rc;
+        }
+    } else {
+        const int rc = h->solver.init(cfg->nx, cfg->ny, cfg->dx, cfg->dy, cfg->coef, cfg->solver, cfg->rtol,
+                                      cfg->max_iter, mask, h->ku, h->kv, 1, h->status, h->err);
+        if (rc) {
+            delete h;
+            return rc;
+        }
+        h->solver.rebuild(0);
     }
-    h->solver.rebuild(0);
     if (cudaDeviceSynchronize() != cudaSuccess) {
         delete h;
         return OC_ERR_CUDA;
@@ -109,13 +123,19 @@ extern "C" int oc_helm_solve(oc_helm* h, const double* rhs, double* x, int32_t o
         d_rhs = h->rhs;
         d_x = h->x;
     }
-    cudaMemsetAsync(h->solver.d_log_count(), 0, sizeof(int), s);
-    int rc = h->solver.solve(d_rhs, d_x, s, h->err);
+    int rc;
+    if (h->refined) {
+        rc = h->refined->solve(d_rhs, d_x, s, h->err);
+    } else {
+        cudaMemsetAsync(h->solver.d_log_count(), 0, sizeof(int), s);
+        rc = h->solver.solve(d_rhs, d_x, s, h->err);
+    }
     if (rc) return rc;
     if (!on_device && cudaMemcpyAsync(x, h->x, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return helm_fail(h, OC_ERR_CUDA, "solution download failed");
     const cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return helm_fail(h, OC_ERR_CUDA, cudaGetErrorString(e));
+    if (h->refined) return h->refined->report(iterations, converged, nullptr, nullptr, h->err);
     int st = 0, it = 0, cv = 0;
     cudaMemcpy(&st, h->status, sizeof(int), cudaMemcpyDeviceToHost);
     if (st) return helm_fail(h, st, "a device-side wait ran out its bound");
@@ -123,6 +143,23 @@ extern "C" int oc_helm_solve(oc_helm* h, const double* rhs, double* x, int32_t o
     cudaMemcpy(&cv, h->solver.d_log_conv(), sizeof(int), cudaMemcpyDeviceToHost);
     if (iterations) *iterations = it;
     if (converged) *converged = cv;
+    return OC_OK;
+}
+
+extern "C" int oc_helm_refine_report(oc_helm* h, int32_t* refinement_steps, double* relative_residual) {
+    if (!h) return OC_ERR_ARG;
+    if (!h->refined) return helm_fail(h, OC_ERR_UNSUPPORTED, "not the refined solver");
+    cudaSetDevice(h->device);
+    int outer = 0;
+    const int rc = h->refined->report(nullptr, nullptr, &outer, relative_residual, h->err);
+    if (rc == OC_OK && refinement_steps) *refinement_steps = outer;
+    return rc;
+}
+
+extern "C" int oc_helm_set_inner_rtol(oc_helm* h, double inner_rtol) {
+    if (!h || !(inner_rtol > 0.0) || !(inner_rtol < 1.0)) return OC_ERR_ARG;
+    if (!h->refined) return helm_fail(h, OC_ERR_UNSUPPORTED, "not the refined solver");
+    h->refined->set_inner_rtol(inner_rtol);
     return OC_OK;
 }
 

@@ -49,6 +49,9 @@ enum {
 /* option codes (the namelist strings of tools/toml2nml.py:209-264) */
 enum { OC_SCHEME_FB = 0, OC_SCHEME_THETA = 1, OC_SCHEME_SPLIT = 2 };
 enum { OC_SOLVER_PCG_JACOBI = 0, OC_SOLVER_PCG_RBGS = 1, OC_SOLVER_RBGS = 2, OC_SOLVER_MULTIGRID = 3 };
+/* standalone Helmholtz solver only (oc_helm_*), no reference counterpart: FP32
+ * inner PCG-Jacobi inside FP64 iterative refinement */
+enum { OC_SOLVER_PCG_REFINED = 4 };
 enum { OC_BC_PERIODIC = 0, OC_BC_CLOSED = 1 };
 enum { OC_FACE_MIN = 0, OC_FACE_MEAN = 1, OC_FACE_HARMONIC = 2 };
 enum { OC_EOS_LINEAR = 0, OC_EOS_SEOS = 1, OC_EOS_TEOS10 = 2 };
@@ -291,6 +294,19 @@ int oc_helm_solve(oc_helm* h, const double* rhs, double* x, int32_t on_device, i
                   int32_t* converged, void* stream);
 const char* oc_helm_last_error(oc_helm* h);
 int oc_helm_destroy(oc_helm* h);
+
+/* Mixed-precision form of the standalone solver (cfg->solver =
+ * OC_SOLVER_PCG_REFINED; no reference counterpart, the reference's precision
+ * variants being whole-program fp32 builds, Makefile:77-113). The operator and
+ * the Krylov vectors of an inner PCG-Jacobi are FP32; the residual b - A x, the
+ * norms, the dot-product sums and the correction x += d are FP64, and the
+ * stopping test is HelmholtzVar's |b - A x|_2 <= rtol |b|_2 evaluated in FP64.
+ * oc_helm_solve then reports the inner iterations summed over the refinement.
+ * oc_helm_refine_report gives the last solve's refinement steps and FP64
+ * relative residual; oc_helm_set_inner_rtol sets the inner solves' relative
+ * tolerance (default 1e-3). Both return OC_ERR_UNSUPPORTED for other solvers. */
+int oc_helm_refine_report(oc_helm* h, int32_t* refinement_steps, double* relative_residual);
+int oc_helm_set_inner_rtol(oc_helm* h, double inner_rtol);
 
 /* The reference EOS bench's per-cell quantity (libs/cuda/src/eos_bench.cu over
  * libs/core/eos.py:68-127) on device buffers of `count` cells: rho' for
