@@ -558,6 +558,118 @@ def run_ensemble(args, rank, world, local_rank):
     return 0
 
 
+def helmholtz_system(n, seed):
+    """A seeded n x n free-surface system of the reference cases' conditioning
+    (c K / dx^2 between 0.25 and 0.5; the reference-written cases reach 0.49): face
+    coefficients in [0.5, 1], a rectangular island whose faces are closed, a
+    normal right-hand side on the wet cells."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    dx = 4.0e6 / n
+    mask = np.ones((n, n))
+    mask[n // 4:n // 3, n // 5:n // 2] = 0.0
+    ku = (0.5 + 0.5 * rng.random((n, n))) * mask * np.roll(mask, -1, 1)
+    kv = (0.5 + 0.5 * rng.random((n, n))) * mask * np.roll(mask, -1, 0)
+    rhs = rng.standard_normal((n, n)) * mask
+    return dx, 0.5 * dx * dx, ku, kv, mask, rhs
+
+
+def refined_bytes_per_cell(inner, outer):
+    """Minimal-pass bytes per cell of one FP32-inner / FP64-refined solve: the
+    start (rhs, mask, 1/diag in; x, r, z, d out: 40 B), every inner iteration
+    (the direction and A p: z, p_old, wet, ax, ay, diag in, p, Ap out, 29 B, no
+    p_old in an inner solve's first iteration; the update: p, d, r, Ap, 1/diag
+    in, d, r, z out, 32 B) and every refinement step (x += d: 20 B; the FP64
+    residual: x, mask, Ku, Kv, rhs, 1/diag in, r, z, d out: 56 B)."""
+    return 40 + 61 * inner - 4 * outer + 76 * outer
+
+
+def run_helmholtz(args, rank, world, local_rank):
+    """The free-surface Helmholtz solve alone: the FP64 PCG-Jacobi solver (the
+    step's, bit-identical to NumPy) beside the FP32-inner / FP64-refined solver,
+    on seeded synthetic systems of growing size, both through oc_helm_solve with
+    the data on the device, timed by CUDA events on the call's stream."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from hydrostatic_ocean_core_benchmark_b200 import _lib
+
+    torch.cuda.set_device(local_rank)
+    lib = _lib.load()
+    stream = torch.cuda.Stream(device=local_rank)
+    peak, peak_kind = measured_hbm_peak()
+    rtol, reps = 1e-10, max(args.steps, 1)
+    sizes = [int(s) for s in args.helm_sizes.split(",")]
+    rows = []
+    for n in sizes:
+        dx, coef, ku, kv, mask, rhs = helmholtz_system(n, args.seed + n)
+        d_rhs = torch.from_numpy(rhs).to(f"cuda:{local_rank}")
+        row = {"n": n}
+        xs = {}
+        for name, kind in (("fp64_pcg_jacobi", 0), ("pcg_refined", 4)):
+            cfg = _lib.OcHelmConfig(nx=n, ny=n, dx=dx, dy=dx, coef=coef, solver=kind, rtol=rtol, max_iter=20000,
+                                    device=local_rank)
+            h = C.c_void_p()
+            rc = lib.oc_helm_create(C.byref(cfg), ku.ctypes.data, kv.ctypes.data, mask.ctypes.data, C.byref(h))
+            if rc:
+                row[name] = {"unavailable": f"{_lib.ERRORS.get(rc, rc)}: {lib.oc_helm_last_error(h).decode()}"
+                             if h else _lib.ERRORS.get(rc, rc)}
+                continue
+            x = torch.zeros_like(d_rhs)
+            its, conv = C.c_int32(), C.c_int32()
+
+            def solve():
+                _lib.check(lib.oc_helm_solve(h, C.c_void_p(d_rhs.data_ptr()), C.c_void_p(x.data_ptr()), 1,
+                                             C.byref(its), C.byref(conv), C.c_void_p(stream.cuda_stream)),
+                           None, name)
+
+            for _ in range(max(args.warmup, 3)):
+                solve()
+            times = []
+            for _ in range(reps):
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+                solve()
+                ev1.record(stream)
+                ev1.synchronize()
+                times.append(ev0.elapsed_time(ev1))
+            ms = statistics.median(times)
+            r = {"ms": ms, "iterations": its.value, "converged": bool(conv.value)}
+            if kind == 4:
+                outer, rel = C.c_int32(), C.c_double()
+                _lib.check(lib.oc_helm_refine_report(h, C.byref(outer), C.byref(rel)), None, name)
+                r["refinement_steps"], r["relative_residual_fp64"] = outer.value, rel.value
+                byt = refined_bytes_per_cell(its.value, outer.value) * n * n
+            else:
+                byt = helm_bytes_per_iteration(type("P", (), {"nx": n, "ny": n, "solver_kind": "pcg_jacobi"})) \
+                    * its.value
+            r["algorithmic_gbs"] = byt / (ms * 1e-3) / 1e9
+            r["frac"] = r["algorithmic_gbs"] / peak
+            xs[name] = x.cpu().numpy()
+            lib.oc_helm_destroy(h)
+            row[name] = r
+        if len(xs) == 2:
+            a, b = xs["fp64_pcg_jacobi"], xs["pcg_refined"]
+            row["rel_l2_refined_vs_fp64"] = float(np.linalg.norm(b - a) / np.linalg.norm(a))
+            row["speedup"] = row["fp64_pcg_jacobi"]["ms"] / row["pcg_refined"]["ms"]
+        rows.append(row)
+    top = rows[-1]["pcg_refined"]
+    line = {"metric": "helmholtz_solve_time", "value": top["ms"], "unit": "ms", "n_gpus": world,
+            "steps": reps, "warmup": max(args.warmup, 3), "ms_per_step": top["ms"], "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner, f64 refinement",
+            "data": "synthetic (seeded face coefficients, island, normal right-hand side)",
+            "config": {"workload": f"free-surface Helmholtz solve, {sizes[-1]}x{sizes[-1]}, rtol {rtol:g}",
+                       "sizes": sizes, "rtol": rtol,
+                       "l2": "working sets from 10 MB (512^2, L2-resident) to 2.6 GB (4096^2)"},
+            "roofline": {"bound": "hbm", "peak": peak, "peak_kind": peak_kind, "unit": "GB/s"},
+            "sizes": rows}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -577,10 +689,13 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-nx", type=int, default=128)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["seamount", "ensemble"], default="seamount",
+    ap.add_argument("--workload", choices=["seamount", "ensemble", "helmholtz"], default="seamount",
                     help="seamount: the 512x512x50 basin (the headline line); ensemble: the "
-                         "batched-ensemble form (its own line)")
+                         "batched-ensemble form (its own line); helmholtz: the FP64 and the "
+                         "FP32-inner/FP64-refined Helmholtz solvers alone (its own line)")
     ap.add_argument("--ens-members", type=int, default=64)
+    ap.add_argument("--helm-sizes", default="512,1024,2048,4096",
+                    help="grid sizes n of the n x n Helmholtz systems")
     args = ap.parse_args()
     rank = env_int("RANK", 0)
     world = env_int("WORLD_SIZE", 1)
@@ -589,6 +704,8 @@ def main():
         return run_reference_arm(args, rank)
     if args.workload == "ensemble":
         return run_ensemble(args, rank, world, local_rank)
+    if args.workload == "helmholtz":
+        return run_helmholtz(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

@@ -21,7 +21,12 @@
 // persistent cooperative launch over the bounded grid barrier of
 // grid_barrier.cuh: a barrier that waits past its bound sets OC_ERR_TIMEOUT
 // and every CTA leaves. Data written by another CTA in the same launch (the
-// search direction, the iterate, the partial sums) is read through L2 (ld.cg).
+// search directions, z, the iterate, the partial sums) is read through L2 (ld.cg).
+//
+// An inner iteration takes two barriers: the pass that forms A p also forms
+// the new direction p = z + beta p_old, each thread at its own cell and,
+// redundantly, at the four neighbours it needs, from z and the previous
+// direction, which lives in the other of two buffers.
 
 #include <cuda_runtime.h>
 
@@ -108,13 +113,23 @@ __device__ __forceinline__ double2 gather(const RefineParams& R, int slot, doubl
     return cta_sum2(a, b, sm);
 }
 
+// the search direction at cell k: z for the first iteration of an inner solve,
+// else z + beta p_old
+__device__ __forceinline__ float direction(const RefineParams& R, const float* pold, float beta, bool fresh, int k) {
+    const float zk = __ldcg(R.z + k);
+    return fresh ? zk : zk + beta * __ldcg(pold + k);
+}
+
 // FP32 operator on the search direction: diag p - (neighbour couplings); dry
-// cells are the identity, as in the FP64 operator
-__device__ __forceinline__ float apply32(const RefineParams& R, int e, const Nb& b) {
-    const float pc = __ldcg(R.p + e);
+// cells are the identity, as in the FP64 operator. Returns A p, with p at e in pc.
+__device__ __forceinline__ float apply32(const RefineParams& R, const float* pold, float beta, bool fresh, int e,
+                                         const Nb& b, float& pc) {
+    pc = direction(R, pold, beta, fresh, e);
     if (!R.wet[e]) return pc;
-    const float off = R.ax[e] * __ldcg(R.p + b.ie) + R.ax[b.iw] * __ldcg(R.p + b.iw) +
-                      R.ay[e] * __ldcg(R.p + b.jn) + R.ay[b.js] * __ldcg(R.p + b.js);
+    const float off = R.ax[e] * direction(R, pold, beta, fresh, b.ie) +
+                      R.ax[b.iw] * direction(R, pold, beta, fresh, b.iw) +
+                      R.ay[e] * direction(R, pold, beta, fresh, b.jn) +
+                      R.ay[b.js] * direction(R, pold, beta, fresh, b.js);
     return R.diag[e] * pc - off;
 }
 
@@ -133,13 +148,12 @@ __device__ __forceinline__ double apply64(const RefineParams& R, int e, const Nb
 }
 
 // a new residual r (FP64) starts an inner solve: rr = r in FP32, z = D^-1 rr,
-// p = z, d = 0; returns the terms of |r|^2 and rr.z
+// d = 0 (its first direction is z); returns the terms of |r|^2 and rr.z
 __device__ __forceinline__ void start_inner(const RefineParams& R, int e, double r, double& r2, double& rz) {
     const float r32 = (float)r;
     const float z32 = R.dinv[e] * r32;
     R.rr[e] = r32;
     R.z[e] = z32;
-    R.p[e] = z32;
     R.d[e] = 0.0f;
     r2 += r * r;
     rz += (double)r32 * (double)z32;
@@ -173,13 +187,18 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
         if (inner >= R.max_iter || outer >= R.max_outer) break;
         ++outer;
         const double inner_tol = R.inner_rtol * res;
+        bool fresh = true;
+        float beta = 0.0f;
+        float *pold = R.p2, *pnew = R.p;
         for (;;) {
-            // Ap = A p and p.Ap
+            // p = z + beta p_old, Ap = A p and p.Ap
             double pap = 0.0;
             for (int e = first; e < n; e += stride) {
-                const float ap = apply32(R, e, neighbours(e, nx, ny));
+                float pc;
+                const float ap = apply32(R, pold, beta, fresh, e, neighbours(e, nx, ny), pc);
+                pnew[e] = pc;
                 R.Ap[e] = ap;
-                pap += (double)R.p[e] * (double)ap;
+                pap += (double)pc * (double)ap;
             }
             publish(R, 0, pap, 0.0, sm);
             ok = grid_sync(R.bar_count, R.status);
@@ -190,7 +209,7 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
             // d += alpha p, rr -= alpha Ap, z = D^-1 rr, with |rr|^2 and rr.z
             double rr2 = 0.0, rzn = 0.0;
             for (int e = first; e < n; e += stride) {
-                const float pe = R.p[e];
+                const float pe = pnew[e];
                 R.d[e] += alpha * pe;
                 const float rre = R.rr[e] - alpha * R.Ap[e];
                 const float ze = R.dinv[e] * rre;
@@ -205,11 +224,12 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
             s = gather(R, 1, sm);
             ++inner;
             if (sqrt(s.x) <= inner_tol || inner >= R.max_iter) break;
-            const float beta = (float)(s.y / rz);
+            beta = (float)(s.y / rz);
             rz = s.y;
-            for (int e = first; e < n; e += stride) R.p[e] = R.z[e] + beta * R.p[e];
-            ok = grid_sync(R.bar_count, R.status);
-            if (!ok) break;
+            fresh = false;
+            float* t = pold;
+            pold = pnew;
+            pnew = t;
         }
         if (!ok) break;
         // the correction, in FP64
@@ -304,6 +324,7 @@ int RefinedHelm::init(int nx, int ny, double dx, double dy, double coef, double 
     float* dinv = (float*)dalloc(n4);
     unsigned char* wet = (unsigned char*)dalloc((size_t)n);
     R.p = (float*)dalloc(n4);
+    R.p2 = (float*)dalloc(n4);
     R.Ap = (float*)dalloc(n4);
     R.rr = (float*)dalloc(n4);
     R.z = (float*)dalloc(n4);
@@ -313,7 +334,7 @@ int RefinedHelm::init(int nx, int ny, double dx, double dy, double coef, double 
     R.status = (int*)dalloc(sizeof(int));
     R.report = (int*)dalloc(3 * sizeof(int));
     R.relres = (double*)dalloc(sizeof(double));
-    if (!mask || !ax || !ay || !diag || !dinv || !wet || !R.p || !R.Ap || !R.rr || !R.z || !R.d || !R.part ||
+    if (!mask || !ax || !ay || !diag || !dinv || !wet || !R.p || !R.p2 || !R.Ap || !R.rr || !R.z || !R.d || !R.part ||
         !R.bar_count || !R.status || !R.report || !R.relres) {
         err = "refined solver: device allocation failed";
         return OC_ERR_CUDA;

@@ -23,8 +23,9 @@ struct RefineParams {
     // (1 on dry cells) and the wet flag
     const float *ax, *ay, *diag, *dinv;
     const unsigned char* wet;
-    // FP32 inner work vectors
-    float *p, *Ap, *rr, *z, *d;
+    // FP32 inner work vectors; the search directions of consecutive iterations
+    // alternate between p and p2
+    float *p, *p2, *Ap, *rr, *z, *d;
     double* part;  // per-CTA partial sums: two slots of two values, 4 * gridDim.x
     unsigned long long* bar_count;
     int* status;
