@@ -122,15 +122,16 @@ __device__ __forceinline__ float direction(const RefineParams& R, const float* p
 
 // FP32 operator on the search direction: diag p - (neighbour couplings); dry
 // cells are the identity, as in the FP64 operator. Returns A p, with p at e in pc.
+// The wet test selects after the arithmetic, so no load waits for the flag.
 __device__ __forceinline__ float apply32(const RefineParams& R, const float* pold, float beta, bool fresh, int e,
                                          const Nb& b, float& pc) {
     pc = direction(R, pold, beta, fresh, e);
-    if (!R.wet[e]) return pc;
     const float off = R.ax[e] * direction(R, pold, beta, fresh, b.ie) +
                       R.ax[b.iw] * direction(R, pold, beta, fresh, b.iw) +
                       R.ay[e] * direction(R, pold, beta, fresh, b.jn) +
                       R.ay[b.js] * direction(R, pold, beta, fresh, b.js);
-    return R.diag[e] * pc - off;
+    const float full = R.diag[e] * pc - off;
+    return R.wet[e] ? full : pc;
 }
 
 // FP64 operator on the iterate, term by term as HelmOp.apply: the masked
@@ -191,14 +192,23 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
         float beta = 0.0f;
         float *pold = R.p2, *pnew = R.p;
         for (;;) {
-            // p = z + beta p_old, Ap = A p and p.Ap
+            // p = z + beta p_old, Ap = A p and p.Ap; two cells (e, e + stride) per
+            // turn, their loads ahead of their stores, added in the order of the cells
             double pap = 0.0;
-            for (int e = first; e < n; e += stride) {
-                float pc;
+            for (int e = first; e < n; e += 2 * stride) {
+                const int e2 = e + stride;
+                const bool two = e2 < n;
+                float pc, pc2 = 0.0f, ap2 = 0.0f;
                 const float ap = apply32(R, pold, beta, fresh, e, neighbours(e, nx, ny), pc);
+                if (two) ap2 = apply32(R, pold, beta, fresh, e2, neighbours(e2, nx, ny), pc2);
                 pnew[e] = pc;
                 R.Ap[e] = ap;
                 pap += (double)pc * (double)ap;
+                if (two) {
+                    pnew[e2] = pc2;
+                    R.Ap[e2] = ap2;
+                    pap += (double)pc2 * (double)ap2;
+                }
             }
             publish(R, 0, pap, 0.0, sm);
             ok = grid_sync(R.bar_count, R.status);
@@ -206,17 +216,33 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
             s = gather(R, 0, sm);
             if (!(s.x > 0.0)) break;  // p = 0: the FP32 residual vanished
             const float alpha = (float)(rz / s.x);
-            // d += alpha p, rr -= alpha Ap, z = D^-1 rr, with |rr|^2 and rr.z
+            // d += alpha p, rr -= alpha Ap, z = D^-1 rr, with |rr|^2 and rr.z; two
+            // cells per turn as above
             double rr2 = 0.0, rzn = 0.0;
-            for (int e = first; e < n; e += stride) {
-                const float pe = pnew[e];
-                R.d[e] += alpha * pe;
-                const float rre = R.rr[e] - alpha * R.Ap[e];
-                const float ze = R.dinv[e] * rre;
-                R.rr[e] = rre;
-                R.z[e] = ze;
-                rr2 += (double)rre * (double)rre;
-                rzn += (double)rre * (double)ze;
+            for (int e = first; e < n; e += 2 * stride) {
+                const int e2 = e + stride;
+                const bool two = e2 < n;
+                const float d1 = R.d[e] + alpha * pnew[e];
+                const float r1 = R.rr[e] - alpha * R.Ap[e];
+                const float z1 = R.dinv[e] * r1;
+                float d2 = 0.0f, r2v = 0.0f, z2 = 0.0f;
+                if (two) {
+                    d2 = R.d[e2] + alpha * pnew[e2];
+                    r2v = R.rr[e2] - alpha * R.Ap[e2];
+                    z2 = R.dinv[e2] * r2v;
+                }
+                R.d[e] = d1;
+                R.rr[e] = r1;
+                R.z[e] = z1;
+                rr2 += (double)r1 * (double)r1;
+                rzn += (double)r1 * (double)z1;
+                if (two) {
+                    R.d[e2] = d2;
+                    R.rr[e2] = r2v;
+                    R.z[e2] = z2;
+                    rr2 += (double)r2v * (double)r2v;
+                    rzn += (double)r2v * (double)z2;
+                }
             }
             publish(R, 1, rr2, rzn, sm);
             ok = grid_sync(R.bar_count, R.status);
