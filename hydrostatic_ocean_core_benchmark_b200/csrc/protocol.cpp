@@ -252,9 +252,6 @@ extern "C" int oc_run_namelist(const char* nml_path) {
     init.S = ts ? S0.data() : nullptr;
     cudaDeviceProp prop{};
     cudaGetDeviceProperties(&prop, 0);
-    std::vector<double> probe(n2);
-    oc_state_view eta_only{};
-    eta_only.eta = probe.data();
     auto diverged = [&]() -> bool {
         oc_stats st{};
         oc_get_stats(h, &st);
