@@ -16,7 +16,7 @@ state and the counters ``solver_iterations``, ``solver_failures``,
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass, replace
+from dataclasses import dataclass
 
 import numpy as np
 

@@ -28,8 +28,7 @@ planes, interface 0 being the surface.
 
 from __future__ import annotations
 
-import math
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 
