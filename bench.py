@@ -54,6 +54,12 @@ def env_int(name, default):
         return default
 
 
+def record_dir():
+    """Directory for the raw clock samples (OCEAN_B200_RECORD_DIR), if it names one."""
+    d = os.environ.get("OCEAN_B200_RECORD_DIR")
+    return Path(d) if d and Path(d).is_dir() else None
+
+
 def measured_hbm_peak():
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
@@ -152,8 +158,9 @@ def mg_level_cells(nx, ny, min_size=8):
 
 
 def helm_bytes_per_iteration(p):
-    """Survey accounting: PCG-Jacobi 15 arrays per column, MG V(2,2) 32 arrays per
-    cell of every level plus 4 fine arrays for the residual check."""
+    """Algorithmic bytes of one Helmholtz iteration: PCG-Jacobi 15 arrays per
+    column, MG V(2,2) 32 arrays per cell of every level plus 4 fine arrays for the
+    residual check."""
     n0 = p.nx * p.ny
     if p.solver_kind == "multigrid":
         return 8 * (32 * sum(mg_level_cells(p.nx, p.ny)) + 4 * n0)
@@ -288,8 +295,8 @@ def run_ours(args, rank, world, local_rank):
     launches0 = st.stats()["kernel_launches"]
     # timed region: device-resident state, events on the launching stream; the
     # steps replay the recorded two-step CUDA graphs (oc_step_graph)
-    out_dir = ROOT / "gpurun_out"
-    clocks = ClockSampler(local_rank, out_dir / f"clocks_rank{rank}.csv" if out_dir.is_dir() else None)
+    out_dir = record_dir()
+    clocks = ClockSampler(local_rank, out_dir / f"clocks_rank{rank}.csv" if out_dir else None)
     clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -511,8 +518,8 @@ def run_ensemble(args, rank, world, local_rank):
     ens.step(warm, stream=stream)
     ens.step(2, stream=stream)          # the graph of the timed region's starting buffers
     stream.synchronize()
-    out_dir = ROOT / "gpurun_out"
-    clocks = ClockSampler(local_rank, out_dir / f"clocks_ens_rank{rank}.csv" if out_dir.is_dir() else None)
+    out_dir = record_dir()
+    clocks = ClockSampler(local_rank, out_dir / f"clocks_ens_rank{rank}.csv" if out_dir else None)
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
