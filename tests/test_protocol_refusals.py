@@ -1,7 +1,8 @@
 """The binary protocol's refusals, on CPU: ``ocean3d5_b200 <prefix>.nml`` checks
 the namelist and the bundle files before it touches a GPU, and refuses what the
-step cannot run with ``FATAL: ...`` on stderr and exit code 1 (the reference
-binary's convention, libs/cuda/src/cfd_exp3d5_cuda.cu)."""
+step cannot run with ``FATAL: ...`` on stderr and exit code 1, the reference
+binary's convention (libs/cuda/src/cfd_exp3d5_cuda.cu:111-114,1117-1127 and
+libs/cuda/src/config.hpp:78,153-163)."""
 
 import subprocess
 from pathlib import Path
