@@ -42,3 +42,61 @@ def test_library_refuses_invalid_config_without_a_gpu():
     h = C.c_void_p()
     assert lib.oc_create(C.byref(cfg), C.byref(h)) == 1
     assert not h.value
+
+
+def test_entry_points_refuse_null_arguments_without_a_gpu():
+    """Every entry point answers a null handle or a missing required pointer
+    with OC_ERR_ARG before it touches a device; the error-string calls and
+    oc_destroy accept null."""
+    import ctypes as C
+    lib = _lib.load()
+    ARG = 1
+    i32, i64, dbl = C.c_int32(), C.c_int64(), C.c_double()
+    buf = (C.c_double * 8)()
+    calls = {
+        "oc_create": lambda: lib.oc_create(None, None),
+        "oc_set_domain": lambda: lib.oc_set_domain(None, buf, buf, None),
+        "oc_set_domain_slab": lambda: lib.oc_set_domain_slab(None, buf, buf, buf, buf, buf, 1.0, 1.0),
+        "oc_set_forcing": lambda: lib.oc_set_forcing(None, buf, buf),
+        "oc_set_state": lambda: lib.oc_set_state(None, None, 0),
+        "oc_set_state_async": lambda: lib.oc_set_state_async(None, None, 0, None),
+        "oc_reset_mixing": lambda: lib.oc_reset_mixing(None),
+        "oc_get_state": lambda: lib.oc_get_state(None, None, 0),
+        "oc_get_state_async": lambda: lib.oc_get_state_async(None, None, 0, None),
+        "oc_step": lambda: lib.oc_step(None, 1, None),
+        "oc_step_graph": lambda: lib.oc_step_graph(None, 1, None),
+        "oc_get_stats": lambda: lib.oc_get_stats(None, None),
+        "oc_set_profiling": lambda: lib.oc_set_profiling(None, 1),
+        "oc_get_kernel_times": lambda: lib.oc_get_kernel_times(None, None, 0, C.byref(i32)),
+        "oc_get_solve_log": lambda: lib.oc_get_solve_log(None, None, 0, C.byref(i32)),
+        "oc_reset_stats": lambda: lib.oc_reset_stats(None),
+        "oc_helmholtz_solve": lambda: lib.oc_helmholtz_solve(None, buf, buf, None, None),
+        "oc_thomas": lambda: lib.oc_thomas(None, buf, buf, buf, buf, 4, 2, None),
+        "oc_thomas_noalloc": lambda: lib.oc_thomas_noalloc(buf, buf, buf, buf, None, 4, 2, None),
+        "oc_buoyancy": lambda: lib.oc_buoyancy(None, buf, buf, buf, buf, 8, None),
+        "oc_helm_create": lambda: lib.oc_helm_create(None, buf, buf, buf, None),
+        "oc_helm_solve": lambda: lib.oc_helm_solve(None, buf, buf, 0, None, None, None),
+        "oc_helm_refine_report": lambda: lib.oc_helm_refine_report(None, C.byref(i32), C.byref(dbl)),
+        "oc_helm_set_inner_rtol": lambda: lib.oc_helm_set_inner_rtol(None, 1e-3),
+        "oc_helm_destroy": lambda: lib.oc_helm_destroy(None),
+        "oc_density": lambda: lib.oc_density(0, 1.0, 0.0, 0.0, 0.0, 0.0, None, buf, buf, buf, 8, None),
+        "oc_get_field": lambda: lib.oc_get_field(None, b"eta", buf, 8),
+        "oc_halo_values_per_row": lambda: lib.oc_halo_values_per_row(None, C.byref(i64)),
+        "oc_pack_rows": lambda: lib.oc_pack_rows(None, 0, 1, buf, None),
+        "oc_unpack_rows": lambda: lib.oc_unpack_rows(None, 0, 1, buf, None),
+        "oc_set_tiling": lambda: lib.oc_set_tiling(None, 1, 1),
+        "oc_autotune": lambda: lib.oc_autotune(None, C.byref(i32), C.byref(i32)),
+        "oc_ensemble_create": lambda: lib.oc_ensemble_create(None, 1, None),
+        "oc_ensemble_step": lambda: lib.oc_ensemble_step(None, 1, None),
+        "oc_ensemble_destroy": lambda: lib.oc_ensemble_destroy(None),
+    }
+    for name, call in calls.items():
+        assert call() == ARG, name
+    assert lib.oc_last_error(None) == b"null handle"
+    assert lib.oc_helm_last_error(None) == b"null handle"
+    assert lib.oc_ensemble_last_error(None) == b"null ensemble"
+    lib.oc_destroy(None)
+    # every header function is covered here, by the symbol tests or by the namelist protocol tests
+    covered = set(calls) | {"oc_version", "oc_last_error", "oc_helm_last_error", "oc_ensemble_last_error",
+                            "oc_destroy", "oc_run_namelist"}
+    assert header_functions() <= covered, header_functions() - covered
