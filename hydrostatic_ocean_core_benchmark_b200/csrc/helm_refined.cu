@@ -369,6 +369,7 @@ int RefinedHelm::init(int nx, int ny, double dx, double dy, double coef, double 
     cudaMemset(R.bar_count, 0, sizeof(unsigned long long));
     cudaMemset(R.status, 0, sizeof(int));
     cudaMemset(R.report, 0, 3 * sizeof(int));
+    cudaMemset(R.relres, 0, sizeof(double));  // a report before the first solve reads zeros
     R.mask = mask;
     R.ax = ax;
     R.ay = ay;
