@@ -20,9 +20,11 @@ through host memory) and unpacks the received rows into the halos
 (``oc_unpack_rows``, which also recomputes w for the new velocities).
 
     python -m torch.distributed.run --nproc-per-node N -m \\
-        hydrostatic_ocean_core_benchmark_b200.slab <prefix>.nml [--halo H]
+        hydrostatic_ocean_core_benchmark_b200.slab <prefix>.nml [--halo H] [--devices 0,1,..]
+    python -m hydrostatic_ocean_core_benchmark_b200.slab <prefix>.nml --ndev N [--halo H] [--devices ..]
 
-reads the reference's bundle, runs ``n_warmup`` + ``n_repeat`` repeats of
+(the second form starts the N ranks itself, as the reference binary's
+``--ndev``; ``--devices`` maps rank r to the r-th listed device) reads the reference's bundle, runs ``n_warmup`` + ``n_repeat`` repeats of
 ``n_steps`` and writes ``<out_prefix>_state3d5.bin`` and
 ``<out_prefix>_metrics.json`` as the reference's multi-device binary does.
 """
@@ -32,6 +34,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import socket
 import sys
 import statistics
 import time
@@ -269,9 +272,10 @@ def _read_bundle(p: OceanParams):
     return H, mask, state, dzr, taux, tauy
 
 
-def run_namelist(nml: str, halo: int = DEFAULT_HALO) -> int:
+def run_namelist(nml: str, halo: int = DEFAULT_HALO, devices: list[int] | None = None) -> int:
     """The multi-device binary's protocol (cfd_exp3d5_cuda_multi.cu:58-265) for the
-    rank this process is; rank 0 writes the state and metrics files."""
+    rank this process is; rank 0 writes the state and metrics files. ``devices``:
+    the device of each rank (default: the launcher's local rank)."""
     p = read_namelist(nml)
     dist = _dist()
     rank = dist.get_rank() if dist else 0
@@ -280,8 +284,15 @@ def run_namelist(nml: str, halo: int = DEFAULT_HALO) -> int:
     if p.scheme_name != "fb":
         raise ValueError(f"the multi-device run supports scheme fb only (got {p.scheme_name})")
     SlabLayout(p.ny, nranks, halo)
+    if devices is not None and len(devices) != nranks:
+        raise ValueError(f"--devices lists {len(devices)} devices for {nranks} ranks")
     import torch
-    device = int(os.environ.get("LOCAL_RANK", 0)) if torch.cuda.device_count() > 1 else 0
+    if devices is not None:
+        device = devices[rank]
+        if not 0 <= device < torch.cuda.device_count():
+            raise ValueError(f"device {device} does not exist ({torch.cuda.device_count()} visible)")
+    else:
+        device = int(os.environ.get("LOCAL_RANK", 0)) if torch.cuda.device_count() > 1 else 0
     torch.cuda.set_device(device)
     H, mask, state, dzr, taux, tauy = _read_bundle(p)
     run = FbSlabRun(p, H, mask, dzr, taux, tauy, halo=halo, device=device)
@@ -341,11 +352,68 @@ def run_namelist(nml: str, halo: int = DEFAULT_HALO) -> int:
     return 3 if diverged else 0
 
 
+def parse_devices(text: str) -> list[int]:
+    """``--devices 0,1,..`` (cfd_exp3d5_cuda_multi.cu:67): distinct non-negative ids."""
+    try:
+        ids = [int(t) for t in text.split(",")]
+    except ValueError:
+        raise ValueError(f"--devices takes a comma-separated list of device ids (got {text!r})") from None
+    if min(ids) < 0 or len(set(ids)) != len(ids):
+        raise ValueError(f"--devices must list distinct non-negative ids (got {text!r})")
+    return ids
+
+
+def _free_port() -> int:
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def _spawned_rank(rank: int, world: int, port: int, argv: list[str]) -> None:
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), LOCAL_WORLD_SIZE=str(world),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    rc = main(argv)
+    if rc:
+        sys.exit(rc)
+
+
+def _spawn(ndev: int, argv: list[str]) -> int:
+    """Start the ranks of one run on this node, as the reference binary does for --ndev."""
+    import torch.multiprocessing as mp
+    try:
+        mp.spawn(_spawned_rank, args=(ndev, _free_port(), argv), nprocs=ndev, join=True)
+    except mp.ProcessExitedException as e:
+        return e.exit_code if e.exit_code and e.exit_code > 0 else 1
+    except mp.ProcessRaisedException:
+        return 1
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description="y-slab multi-GPU run of the fb scheme (one rank per GPU)")
     ap.add_argument("namelist")
     ap.add_argument("--halo", type=int, default=DEFAULT_HALO)
+    ap.add_argument("--ndev", type=int, default=None,
+                    help="number of ranks; without a launcher, this process starts them")
+    ap.add_argument("--devices", default=None, help="device of each rank, e.g. 0,1,2,3")
     args = ap.parse_args(argv)
+    argv = list(sys.argv[1:] if argv is None else argv)
+    # the command line's refusals, before any rendezvous or device work
+    try:
+        devices = parse_devices(args.devices) if args.devices is not None else None
+        ndev = args.ndev if args.ndev is not None else (len(devices) if devices else None)
+        if ndev is not None and ndev < 1:
+            raise ValueError(f"--ndev must be >= 1 (got {ndev})")
+        if devices is not None and ndev != len(devices):
+            raise ValueError(f"--ndev {ndev} and --devices {args.devices} disagree")
+        launched = "WORLD_SIZE" in os.environ
+        if launched and ndev is not None and ndev != int(os.environ["WORLD_SIZE"]):
+            raise ValueError(f"--ndev {ndev}, but the launcher started {os.environ['WORLD_SIZE']} ranks")
+    except ValueError as e:
+        print(f"FATAL: {e}", file=sys.stderr, flush=True)
+        return 2
+    if not launched and ndev is not None and ndev > 1:
+        return _spawn(ndev, argv)
     import torch
     import torch.distributed as dist
     if "WORLD_SIZE" in os.environ and not dist.is_initialized():
@@ -354,7 +422,7 @@ def main(argv=None) -> int:
         # a rank that dies ends the others' next exchange with an error, not a hang
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     try:
-        rc = run_namelist(args.namelist, args.halo)
+        rc = run_namelist(args.namelist, args.halo, devices)
     except ValueError as e:
         print(f"FATAL: {e}", file=sys.stderr, flush=True)
         rc = 2

@@ -199,3 +199,38 @@ def test_front_end_refuses_before_any_device_work(tmp_path, scheme, ny, halo, wh
                        env={**env, "PYTHONPATH": str(root)})
     assert r.returncode == 2, r.stdout + r.stderr
     assert "FATAL" in r.stderr and what in r.stderr
+
+
+def _front_end(tmp_path, nml, *flags, env_extra=None):
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    env.update(PYTHONPATH=str(root), **(env_extra or {}))
+    return subprocess.run([sys.executable, "-m", "hydrostatic_ocean_core_benchmark_b200.slab", str(nml), *flags],
+                          capture_output=True, text=True, cwd=root, timeout=300, env=env)
+
+
+@pytest.mark.parametrize("flags,env_extra,what", [
+    (("--ndev", "0"), None, "--ndev must be >= 1"),
+    (("--devices", "0,x"), None, "comma-separated list"),
+    (("--devices", "1,1"), None, "distinct non-negative"),
+    (("--ndev", "3", "--devices", "0,1"), None, "disagree"),
+    (("--ndev", "3"), {"WORLD_SIZE": "2"}, "the launcher started 2 ranks"),
+    (("--devices", "5"), None, "device 5 does not exist"),
+])
+def test_front_end_command_line_refusals(tmp_path, flags, env_extra, what):
+    """--ndev and --devices as the reference binary takes them, refused before any
+    rendezvous or device work (a CPU box has no device 5)."""
+    r = _front_end(tmp_path, _bundle(tmp_path, "fb", 40), *flags, env_extra=env_extra)
+    assert r.returncode == 2, r.stdout + r.stderr
+    assert "FATAL" in r.stderr and what in r.stderr
+
+
+def test_front_end_starts_its_own_ranks(tmp_path):
+    """Without a launcher, --ndev 2 starts two ranks that meet over gloo on
+    127.0.0.1; here both refuse the theta scheme, and the exit code comes back."""
+    r = _front_end(tmp_path, _bundle(tmp_path, "theta", 40), "--ndev", "2")
+    assert r.returncode == 2, r.stdout + r.stderr
+    assert r.stderr.count("FATAL") >= 1 and "fb only" in r.stderr
