@@ -250,18 +250,13 @@ class FbSlabRun:
 
 # ---------------------------------------------------------------------- front end
 def _read_bundle(p: OceanParams):
-    from .bundle import read_domain
+    """The whole domain's inputs named by the namelist: H, mask, the initial state
+    (the init file has the state file's layout), levels and forcing if given."""
+    from .bundle import read_domain, read_state
     nx, ny, nz = p.nx, p.ny, p.nz
+    n2 = nx * ny
     H, mask = read_domain(p.domain_file, nx, ny)
-    raw = np.fromfile(p.init_file, dtype=np.float64)
-    n2, n3 = nx * ny, nx * ny * nz
-    ts = p.tracers == "TS"
-    names = ["u", "v", "b"] + (["T", "S"] if ts else [])
-    if raw.size != n2 + len(names) * n3:
-        raise ValueError(f"{p.init_file}: expected {n2 + len(names) * n3} doubles, got {raw.size}")
-    state = {"eta": raw[:n2].reshape(ny, nx)}
-    for q, name in enumerate(names):
-        state[name] = raw[n2 + q * n3:n2 + (q + 1) * n3].reshape(nz, ny, nx)
+    state = read_state(p.init_file, nx, ny, nz, p.tracers == "TS")
     dzr = None
     if getattr(p, "levels_file", ""):
         dzr = np.fromfile(p.levels_file, dtype=np.float64)
