@@ -216,6 +216,23 @@ def cpu_oracle_rate(args, steps: int, warmup: int):
     return cells * steps / dt, dt, p
 
 
+def host_cpu() -> dict:
+    """The host's logical core count and CPU model, recorded beside a CPU rate."""
+    model = "unknown"
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.lower().startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count()
+    return {"nproc": os.cpu_count(), "usable": usable, "cpu_model": model}
+
+
 def reference_sample_nx(args) -> int:
     """Largest sample (columns per side) whose W + K oracle steps fit ~150 s."""
     per_step_64 = 1.1 * args.nz / 50.0          # seconds per step at 64 x 64 columns
@@ -240,7 +257,7 @@ def run_reference_arm(args, rank):
             "config": {"workload": f"seamount_basin {args.nx}x{args.ny}x{args.nz}",
                        "sample": f"{p.nx}x{p.ny}x{p.nz}"},
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": sample},
+                             "sample": sample, "host": host_cpu()},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -444,7 +461,7 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, secs, cp = cpu_oracle_rate(args, args.cpu_steps, 1)
-        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port", "host": host_cpu(),
                "sample": f"CPU oracle (NumPy, bit-identical port of the reference stepper) on the "
                          f"same recipe at {cp.nx}x{cp.ny}x{cp.nz}, 1 warm-up + {args.cpu_steps} "
                          f"steps, {secs:.1f} s"}

@@ -4,9 +4,10 @@
 //   <prefix>.nml + <prefix>_domain.bin + <prefix>_init.bin
 //       -> <out_prefix>_state3d5.bin + <out_prefix>_metrics.json
 //
-// Namelist parsing follows the reference's rules (libs/cuda/src/config.hpp:
-// 62-93; missing keys take the defaults of its RunConfig, :18-50, and V05Config,
-// cfd_exp3d5_cuda.cu:72-86); the run loop, divergence guard, timing (median and
+// The namelist is read as the format the reference's bundle writer emits
+// (tools/toml2nml.py:27-34, 188-268); missing keys take the defaults of the
+// reference binary's RunConfig (libs/cuda/src/config.hpp:18-50) and V05Config
+// (cfd_exp3d5_cuda.cu:72-86); the run loop, divergence guard, timing (median and
 // MAD of wall time) and output layout follow cfd_exp3d5_cuda.cu:1104-1237.
 // Options the step cannot run are refused with "FATAL: ..." and a non-zero
 // status, never silently changed.
@@ -14,11 +15,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cctype>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <iterator>
 #include <map>
 #include <string>
 #include <vector>
@@ -27,49 +30,138 @@
 
 namespace {
 
-std::string trim(const std::string& s) {
-    const char* ws = " \t\r\n";
-    const size_t b = s.find_first_not_of(ws);
-    if (b == std::string::npos) return "";
-    return s.substr(b, s.find_last_not_of(ws) - b + 1);
-}
-
-bool read_namelist(const std::string& path, std::map<std::string, std::string>& kv) {
-    std::ifstream in(path);
-    if (!in) return false;
-    std::string line;
-    while (std::getline(in, line)) {
-        const size_t bang = line.find('!');
-        if (bang != std::string::npos) line = line.substr(0, bang);
-        line = trim(line);
-        if (line.empty() || line[0] == '&' || line[0] == '/') continue;
-        const size_t eq = line.find('=');
-        if (eq == std::string::npos) continue;
-        kv[trim(line.substr(0, eq))] = trim(line.substr(eq + 1));
+// A Fortran namelist file as the reference's v0.5 bundle writer emits it
+// (tools/toml2nml.py:188-268): `&group` opens a group and `/` closes it; inside,
+// `name = value` items are separated by newlines or commas; character values
+// are quoted ('...' or "...", a doubled quote standing for itself); reals carry
+// a Fortran exponent letter d/D (tools/toml2nml.py:27-34) or e/E; logicals are
+// .true./.false. (or T/F); `!` outside quotes starts a comment. Names are
+// case-insensitive. Values are kept as their raw text until asked for.
+class Namelist {
+  public:
+    bool load(const std::string& path) {
+        std::ifstream in(path, std::ios::binary);
+        if (!in) return false;
+        const std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+        scan(text);
+        return true;
     }
-    return true;
-}
-
-double to_double(std::string s) {
-    std::replace(s.begin(), s.end(), 'd', 'e');
-    std::replace(s.begin(), s.end(), 'D', 'e');
-    return std::strtod(s.c_str(), nullptr);
-}
-
-std::string unquote(const std::string& s) {
-    if (s.size() >= 2 && (s.front() == '\'' || s.front() == '"')) return s.substr(1, s.size() - 2);
-    return s;
-}
-
-struct Nml {
-    std::map<std::string, std::string> kv;
-    double num(const char* k, double d) const {
-        auto it = kv.find(k);
-        return it == kv.end() ? d : to_double(it->second);
+    double num(const char* name, double dflt) const {
+        const std::string* raw = find(name);
+        double v;
+        return (raw && fortran_real(*raw, v)) ? v : dflt;
     }
-    std::string str(const char* k, const std::string& d) const {
-        auto it = kv.find(k);
-        return it == kv.end() ? d : unquote(it->second);
+    std::string str(const char* name, const std::string& dflt) const {
+        const std::string* raw = find(name);
+        return raw ? *raw : dflt;
+    }
+    bool logical(const char* name, bool dflt) const {
+        const std::string* raw = find(name);
+        if (!raw || raw->empty()) return dflt;
+        size_t p = (*raw)[0] == '.' ? 1 : 0;
+        if (p >= raw->size()) return dflt;
+        const char c = (char)std::tolower((unsigned char)(*raw)[p]);
+        return c == 't' ? true : c == 'f' ? false : dflt;
+    }
+
+  private:
+    std::map<std::string, std::string> items_;
+
+    const std::string* find(const char* name) const {
+        const auto it = items_.find(lower(name));
+        return it == items_.end() ? nullptr : &it->second;
+    }
+    static std::string lower(std::string s) {
+        for (char& c : s) c = (char)std::tolower((unsigned char)c);
+        return s;
+    }
+    static bool name_char(char c) { return std::isalnum((unsigned char)c) || c == '_' || c == '%'; }
+
+    // one pass over the characters: outside a group everything is ignored; in a
+    // group, read a name, an '=' and one value (quoted or up to a separator)
+    void scan(const std::string& t) {
+        const size_t n = t.size();
+        size_t i = 0;
+        bool in_group = false;
+        auto skip_comment = [&]() {
+            while (i < n && t[i] != '\n') ++i;
+        };
+        while (i < n) {
+            const char c = t[i];
+            if (c == '!') {
+                skip_comment();
+                continue;
+            }
+            if (!in_group) {
+                if (c == '&' || c == '$') {  // group name follows; the name itself is not needed
+                    in_group = true;
+                    ++i;
+                    while (i < n && name_char(t[i])) ++i;
+                } else {
+                    ++i;
+                }
+                continue;
+            }
+            if (std::isspace((unsigned char)c) || c == ',') {
+                ++i;
+                continue;
+            }
+            if (c == '/' || c == '&' || c == '$') {  // end of the group (`/`, `&end`, `$end`)
+                in_group = false;
+                ++i;
+                while (i < n && name_char(t[i])) ++i;
+                continue;
+            }
+            // an item: name = value
+            const size_t n0 = i;
+            while (i < n && name_char(t[i])) ++i;
+            std::string name = lower(t.substr(n0, i - n0));
+            while (i < n && (t[i] == ' ' || t[i] == '\t')) ++i;
+            if (name.empty() || i >= n || t[i] != '=') {  // not an item: drop the rest of the line
+                skip_comment();
+                continue;
+            }
+            ++i;
+            while (i < n && (t[i] == ' ' || t[i] == '\t')) ++i;
+            std::string value;
+            if (i < n && (t[i] == '\'' || t[i] == '"')) {
+                const char q = t[i++];
+                while (i < n) {
+                    if (t[i] == q) {
+                        if (i + 1 < n && t[i + 1] == q) {  // doubled quote
+                            value += q;
+                            i += 2;
+                            continue;
+                        }
+                        ++i;
+                        break;
+                    }
+                    value += t[i++];
+                }
+            } else {
+                const size_t v0 = i;
+                while (i < n && !std::isspace((unsigned char)t[i]) && t[i] != ',' && t[i] != '/' && t[i] != '!') ++i;
+                value = t.substr(v0, i - v0);
+            }
+            items_[name] = value;
+        }
+    }
+
+    // a Fortran real or integer literal: the exponent letter d/D/q/Q after the
+    // mantissa is read as e; anything left unparsed makes the literal invalid
+    static bool fortran_real(const std::string& raw, double& out) {
+        std::string s;
+        s.reserve(raw.size());
+        bool mantissa = false;
+        for (char c : raw) {
+            if (mantissa && (c == 'd' || c == 'D' || c == 'q' || c == 'Q')) c = 'e';
+            if (std::isdigit((unsigned char)c) || c == '.') mantissa = true;
+            s += c;
+        }
+        if (s.empty()) return false;
+        char* end = nullptr;
+        out = std::strtod(s.c_str(), &end);
+        return end && *end == '\0';
     }
 };
 
@@ -113,8 +205,8 @@ int pick(const std::string& v, std::initializer_list<const char*> names, int& ou
 
 extern "C" int oc_run_namelist(const char* nml_path) {
     if (!nml_path) return fatal("usage: ocean3d5_b200 <namelist>");
-    Nml n;
-    if (!read_namelist(nml_path, n.kv)) return fatal(std::string("cannot open namelist ") + nml_path);
+    Namelist n;
+    if (!n.load(nml_path)) return fatal(std::string("cannot open namelist ") + nml_path);
     oc_config c{};
     c.nx = (int)n.num("nx", 100);
     c.ny = (int)n.num("ny", 100);
@@ -165,8 +257,7 @@ extern "C" int oc_run_namelist(const char* nml_path) {
     const std::string eos = n.str("eos", "linear");
     if (pick(eos, {"linear", "seos", "teos10"}, c.eos)) return fatal("eos must be linear|seos|teos10");
     if (pick(n.str("pgf", "remove"), {"remove", "keep"}, c.pgf)) return fatal("pgf must be remove|keep");
-    const std::string pc = n.str("pgf_correction", ".true.");
-    c.pgf_correction = (pc.find('t') != std::string::npos || pc.find('T') != std::string::npos) ? 1 : 0;
+    c.pgf_correction = n.logical("pgf_correction", true) ? 1 : 0;
     const std::string adv = n.str("advection", "none");
     if (pick(adv, {"none", "centered2", "upwind1", "up3", "up3_tvd"}, c.advection))
         return fatal("unknown advection " + adv);

@@ -9,14 +9,19 @@
 // array of this library instead.
 //
 // The scratch is a file-scope __device__ array of OC_THOMAS_NOALLOC_MAX_CELLS
-// doubles (8 MiB). Every GPU that loads the library holds it until the process
-// exits. Its device address is taken once per device, on the first call made
-// with that device current (cudaGetSymbolAddress); make that first call
-// before any stream capture. All calls share the one array and it keeps the
-// last call's contents: calls whose work can overlap on the GPU (different
-// streams, or several host threads) race on it and must be serialised by the
-// caller. Every scratch element a solve reads is written earlier by the same
-// solve, so nothing has to be cleared between calls.
+// doubles (8 MiB). CUDA loads a library's device code lazily, so the array is
+// committed on a device by the first call made with that device current, and
+// that device then holds it until the process exits. That first call also
+// takes the array's device address (cudaGetSymbolAddress) and keeps it for the
+// device. A host that fixes its device footprint at start-up therefore makes
+// one warm-up call per device at start-up; the same warm-up call has to come
+// before any stream capture. The kept address belongs to the device's current
+// context: after cudaDeviceReset the library must not be used again in the
+// process. All calls share the one array and it keeps the last call's
+// contents: calls whose work can overlap on the GPU (different streams, or
+// several host threads) race on it and must be serialised by the caller.
+// Every scratch element a solve reads is written earlier by the same solve,
+// so nothing has to be cleared between calls.
 
 #include <cuda_runtime.h>
 
@@ -68,6 +73,9 @@ extern "C" int oc_thomas_noalloc(const double* sub, const double* diag, const do
                      n, ncols, cells, OC_THOMAS_NOALLOC_MAX_CELLS);
         return OC_ERR_TOO_LARGE;
     }
+    // an error left pending by the caller's own earlier work is not this
+    // solve's: report it without consuming it, so the caller's check still sees it
+    if (cudaPeekAtLastError() != cudaSuccess) return OC_ERR_CUDA;
     double* scratch = nullptr;
     const int rc = scratch_for_current_device(&scratch);
     if (rc) return rc;

@@ -251,12 +251,16 @@ int oc_thomas(const double* sub, const double* diag, const double* sup, const do
  * device memory (a host that fixes its device footprint at start-up, or an
  * asynchronous pipeline that cannot afford the device-wide synchronisation of
  * cudaMalloc/cudaFree). No counterpart in the reference. Its scratch is a fixed
- * array of OC_THOMAS_NOALLOC_MAX_CELLS doubles (8 MiB) that every GPU loading
- * the library holds until exit; n * ncols above that returns OC_ERR_TOO_LARGE.
- * It calls no allocator. The first call on a device looks up the array's device
- * address, so make it before any stream capture. Work is enqueued on `stream`
- * and not waited for; calls that can overlap on the GPU share the array and
- * race, so the caller serialises them. */
+ * array of OC_THOMAS_NOALLOC_MAX_CELLS doubles (8 MiB); n * ncols above that
+ * returns OC_ERR_TOO_LARGE. It calls no allocator, but CUDA loads the array
+ * lazily: the first call on a device commits the 8 MiB there (held until exit)
+ * and looks up the array's device address, so a host with a fixed footprint
+ * makes one warm-up call per device at start-up, before any stream capture.
+ * The address is kept per device: do not use the library again after
+ * cudaDeviceReset. An error already pending on the calling thread is returned
+ * as OC_ERR_CUDA and left pending. Work is enqueued on `stream` and not waited
+ * for; calls that can overlap on the GPU share the array and race, so the
+ * caller serialises them. */
 #define OC_THOMAS_NOALLOC_MAX_CELLS 1048576
 int oc_thomas_noalloc(const double* sub, const double* diag, const double* sup, const double* rhs,
                       double* x, int32_t n, int32_t ncols, void* stream);

@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Generate the golden vectors that pin the CPU oracle to the unmodified reference.
 
-Run in a container that has the reference checked out (default
-``/root/reference``, override with ``OCEAN_REFERENCE``); the fixtures it writes
+Run in a container that has the reference checked out (``OCEAN_REFERENCE``, or a
+checkout named ``reference`` beside this repository); the fixtures it writes
 under ``tests/golden/*.npz`` are what travels. It imports the reference's own
 NumPy stepper (``libs/core/model3d_v05.py`` ``Stepper3DV05``), its bundle
 writer (``tools/toml2nml.py`` ``write_v05_bundle``), its case generators and
@@ -32,7 +32,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REF = Path(os.environ.get("OCEAN_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("OCEAN_REFERENCE", str(Path(__file__).resolve().parents[3] / "reference")))
 sys.path.insert(0, str(HERE))
 sys.path.insert(0, str(REPO))
 sys.path.insert(0, str(REF))

@@ -2,7 +2,8 @@
 """Generate the standalone-Helmholtz golden cases with the reference's own tool.
 
 Runs the reference's ``tools/write_helmholtz_case.py --reference`` (from the
-reference tree, default ``/root/reference``, override with ``OCEAN_REFERENCE``)
+reference tree: ``OCEAN_REFERENCE``, or a checkout named ``reference`` beside
+this repository)
 for a 64 x 64 and a 96 x 96 rough-topography case, and stores per case the
 face coefficients, mask, right-hand side, the reference's PCG solution at
 rtol 1e-13 (``eta_ref``) and its metadata, which carries NumPy's
@@ -23,7 +24,7 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("OCEAN_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("OCEAN_REFERENCE", str(Path(__file__).resolve().parents[3] / "reference")))
 CASES = {64: dict(nz=10, seed=20260911), 96: dict(nz=12, seed=20261203)}
 
 

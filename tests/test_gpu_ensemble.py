@@ -73,6 +73,28 @@ def test_ensemble_equals_members_stepped_alone():
         sa, sb = a.stats(), b.stats()
         assert all(sa[k] == sb[k] for k in keys), (m, {k: (sa[k], sb[k]) for k in keys})
         assert a.solve_log() == b.solve_log()
+    # the two smaller members directly against the oracle, field by field
+    for m in (1, 2):
+        _equal_to_oracle(MEMBERS[m], together[m], 9)
     ens.close()
     for st in together + alone:
         st.close()
+
+
+def _equal_to_oracle(member, st, steps):
+    from oracle import ocean_oracle as orc
+    nx, ny, nz, seed = member
+    s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=seed)
+    p = s.params
+    geo = orc.Geometry(p, s.H, s.mask, s.dzr)
+    b = orc.buoyancy(p.eos, s.T, s.S, geo.zc, p.g, p.rho0, p.alpha_t, p.beta_s, p.t0, p.s0) * geo.mask3
+    ref = orc.OracleStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    state = orc.OracleState(s.u, s.v, b, s.eta, s.T, s.S)
+    for _ in range(steps):
+        state = ref.step(state)
+    got = st.get_state()
+    for f in FIELDS:
+        want = {"km": ref.Km, "kh": ref.Kh}.get(f, None)
+        want = getattr(state, f) if want is None else want
+        assert np.array_equal(got[f], want), f"member {member[:3]}: {f} differs from the oracle"
+    assert st.solve_log() == ref.solve_log

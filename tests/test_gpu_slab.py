@@ -118,6 +118,37 @@ def test_slabs_on_ranks_equal_the_single_device_step(tmp_path, world):
     want = _single(_case(), steps)
     for f in FIELDS:
         assert np.array_equal(got[f], want[f]), f"{f} differs with {world} ranks"
+    # and directly against the oracle's whole-domain fb run
+    _equal_to_oracle(_case(), got, steps, f"{world} slabs")
+
+
+def _equal_to_oracle(s, got, steps, what):
+    from oracle import ocean_oracle as orc
+    p = s.params
+    geo = orc.Geometry(p, s.H, s.mask, s.dzr)
+    b = orc.buoyancy(p.eos, s.T, s.S, geo.zc, p.g, p.rho0, p.alpha_t, p.beta_s, p.t0, p.s0) * geo.mask3
+    ref = orc.OracleStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    state = orc.OracleState(s.u, s.v, b, s.eta, s.T, s.S)
+    for _ in range(steps):
+        state = ref.step(state)
+    for f in FIELDS:
+        want = {"km": ref.Km, "kh": ref.Kh}.get(f, None)
+        want = getattr(state, f) if want is None else want
+        assert np.array_equal(got[f], want), f"{what}: {f} differs from the oracle"
+
+
+@pytest.mark.parametrize("bc_y", ["closed", "periodic"])
+def test_one_slab_with_itself_equals_the_oracle(bc_y):
+    """The gathered slab run against the oracle's whole-domain fb step, bit for bit."""
+    from hydrostatic_ocean_core_benchmark_b200.slab import FbSlabRun
+    s = _case(bc_y)
+    steps = 6
+    run = FbSlabRun(s.params, s.H, s.mask, s.dzr, s.taux_c, s.tauy_c, rank=0, nranks=1)
+    run.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
+    run.step(steps)
+    got = run.gather_state()
+    run.close()
+    _equal_to_oracle(s, got, steps, f"one slab ({bc_y})")
 
 
 def test_namelist_front_end_matches_the_single_device_binary(tmp_path):

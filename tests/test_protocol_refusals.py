@@ -85,3 +85,39 @@ def test_missing_and_short_bundle_files(bundle, tmp_path):
     short_lv.write_bytes(np.ones(2).tobytes())
     r = _run(_mutated(bundle, tmp_path, "levels_file", f"'{short_lv}'"))
     assert r.returncode == 1 and "is shorter than nz doubles" in r.stderr
+
+
+@pytest.mark.parametrize("line,message", [
+    # a doubled quote inside a quoted value stands for one quote
+    ("  scheme_name = 'leap''frog'", "unknown scheme leap'frog"),
+    # names are case-insensitive and a comment may follow the value
+    ("  SCHEME_NAME = \"leapfrog\"   ! not a scheme", "unknown scheme leapfrog"),
+    # several items on one line, separated by commas; a D exponent
+    ("  theta = 0.0D0, n_picard = 2", "theta must lie in (0,1]"),
+    ("  theta = 1.5d+00", "theta must lie in (0,1]"),
+])
+def test_namelist_format_variants(bundle, tmp_path, line, message):
+    """The namelist reader follows the Fortran namelist format the bundle
+    writer emits (reference tools/toml2nml.py:27-34,188-268), including forms
+    the writer does not use but a hand-edited file may: doubled quotes, upper
+    case names, trailing comments and comma-separated items."""
+    key = line.split("=")[0].strip().lower()
+    lines = bundle.read_text().splitlines()
+    hits = [i for i, ln in enumerate(lines) if ln.strip().lower().startswith(f"{key} =")]
+    assert len(hits) == 1, key
+    lines[hits[0]] = line
+    nml = tmp_path / "case.nml"
+    nml.write_text("\n".join(lines) + "\n")
+    r = _run(nml)
+    assert r.returncode == 1, r.stdout + r.stderr
+    assert f"FATAL: {message}" in r.stderr
+
+
+def test_group_end_forms(bundle, tmp_path):
+    """`&end` closes a group as `/` does; items outside any group are ignored."""
+    text = bundle.read_text().replace("\n/\n", "\n&end\n")
+    text = "scheme_name = 'leapfrog'\n" + text
+    nml = tmp_path / "case.nml"
+    nml.write_text(text.replace("scheme_name = 'theta'", "scheme_name = 'split'"))
+    r = _run(nml)
+    assert r.returncode == 1 and "FATAL: unknown scheme split" in r.stderr, r.stderr

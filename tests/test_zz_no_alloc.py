@@ -40,6 +40,34 @@ def test_noalloc_thomas_matches_oc_thomas_on_two_calls():
         assert torch.equal(x_ref, x_new)
 
 
+def test_noalloc_thomas_allocates_nothing_after_its_warm_up_call():
+    """After the warm-up call that commits the fixed scratch, a call on a
+    non-default stream leaves the device's free memory unchanged."""
+    import torch
+
+    from hydrostatic_ocean_core_benchmark_b200 import _lib
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    rng = np.random.default_rng(7)
+    n, ncols = 32, 4096
+    sub, diag, sup, rhs = (torch.as_tensor(a, device="cuda") for a in _system(rng, n, ncols))
+    x_ref = torch.empty_like(rhs)
+    x_new = torch.empty_like(rhs)
+    ptrs = [a.data_ptr() for a in (sub, diag, sup, rhs)]
+    assert lib.oc_thomas(*ptrs, x_ref.data_ptr(), n, ncols, None) == 0
+    assert lib.oc_thomas_noalloc(*ptrs, x_new.data_ptr(), n, ncols, None) == 0  # warm-up
+    side = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    x_new.fill_(np.nan)
+    torch.cuda.synchronize()
+    assert lib.oc_thomas_noalloc(*ptrs, x_new.data_ptr(), n, ncols, side.cuda_stream) == 0
+    side.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    assert torch.equal(x_ref, x_new)
+
+
 def test_noalloc_thomas_rejects_sizes_beyond_its_scratch():
     import torch
 
