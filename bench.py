@@ -264,6 +264,91 @@ def run_reference_arm(args, rank):
     return 0
 
 
+# ------------------------------------------------------------------ mixed precision
+MIXED_FIELDS = ("eta", "u", "v", "b", "T", "S", "e", "km", "kh")
+
+
+def precision_leg(s, local_rank, steps, warmup, time_fp64=False):
+    """The mixed-precision step beside the fp64 one on the same initial state.
+
+    Both advance warmup + steps steps (two-step CUDA graphs) from the state of
+    the seeded recipe; the mixed path's last `steps` are timed with CUDA events
+    on the launching stream (and the fp64 path's too with time_fp64). Returns
+    the rates, the relative L2 error of every field against the fp64 path (which
+    is bit-identical to the reference), and the multigrid cycle counts."""
+    import torch
+
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    p = s.params
+    n3 = p.nx * p.ny * p.nz
+    out, rate, ms, logs = {}, {}, {}, {}
+    stream = torch.cuda.Stream(device=local_rank)
+    for prec in ("fp64", "mixed"):
+        st = OceanStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c, device=local_rank,
+                          precision=prec)
+        st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
+        st.step(warmup, stream=stream, graph=True)
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st.step(steps, stream=stream, graph=True)
+        e1.record(stream)
+        e1.synchronize()
+        ms[prec] = e0.elapsed_time(e1) / steps
+        rate[prec] = n3 / (ms[prec] / 1e3)
+        stats = st.stats()
+        if stats["solver_failures"] or stats["diverged"]:
+            raise RuntimeError(f"{prec} run failed: {stats}")
+        logs[prec] = st.solve_log()
+        shapes = {"eta": st.shape2, "e": st.shapei, "km": st.shapei, "kh": st.shapei}
+        o = {f: torch.empty(shapes.get(f, st.shape3), dtype=torch.float64, device=f"cuda:{local_rank}")
+             for f in MIXED_FIELDS}
+        st.get_state(out=o)
+        out[prec] = o
+        st.close()
+    rel = {}
+    for f in MIXED_FIELDS:
+        a, b = out["mixed"][f], out["fp64"][f]
+        den = float(torch.linalg.vector_norm(b))
+        rel[f] = float(torch.linalg.vector_norm(a - b)) / den if den > 0 else float(torch.linalg.vector_norm(a))
+    la, lb = logs["fp64"], logs["mixed"]
+    leg = {"steps": warmup + steps, "timed_steps": steps, "ms_per_step": ms["mixed"], "value": rate["mixed"],
+           "unit": UNIT, "rel_l2_vs_fp64": rel, "worst_field": max(rel, key=rel.get),
+           "multigrid_cycles": {"fp64": sum(la), "mixed": sum(lb), "solves": len(lb),
+                                "max_per_solve_difference": max((abs(x - y) for x, y in zip(la, lb)), default=0)}}
+    if time_fp64:
+        leg["fp64"] = {"ms_per_step": ms["fp64"], "value": rate["fp64"]}
+        leg["speedup_vs_fp64"] = ms["fp64"] / ms["mixed"]
+    del out
+    torch.cuda.empty_cache()
+    return leg
+
+
+def run_precision(args, rank, world, local_rank):
+    """--workload precision: the benchmark's precision form (the seamount recipe
+    at 1024 x 1024 x 64, 100 steps), fp64 beside mixed on one GPU."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    if rank != 0:
+        return 0
+    s = workload(args)
+    p = s.params
+    leg = precision_leg(s, local_rank, args.steps, args.warmup, time_fp64=True)
+    line = {"metric": "cell-steps/s, mixed FP32/FP64 step vs fp64 (rel L2 vs fp64 per field)",
+            "value": leg["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": leg["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (3D state and stencils) + f64 (b, pressure gradient, EOS, eta, Helmholtz)",
+            "data": "synthetic (seeded seamount-basin recipe)",
+            "config": {"workload": f"seamount_basin {p.nx}x{p.ny}x{p.nz}, TKE + TVD3 + polyTEOS10, "
+                                   f"theta={p.theta:g} + {p.solver_kind}, dt={p.dt:g} s",
+                       "cells": p.nx * p.ny * p.nz, "variant": "precision form (mixed vs fp64)"},
+            "fp64": leg["fp64"], "speedup_vs_fp64": leg["speedup_vs_fp64"],
+            "rel_l2_vs_fp64": leg["rel_l2_vs_fp64"], "multigrid_cycles": leg["multigrid_cycles"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args, rank, world, local_rank):
     import numpy as np
@@ -458,6 +543,14 @@ def run_ours(args, rank, world, local_rank):
     kernel_share = {k: {"launches": v[0], "ms": v[1], "share": v[1] / max(1e-12, sum(x[1] for x in ktimes.values()))}
                     for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1][1])}
 
+    # the mixed-precision step on the same recipe and grid, beside a fresh fp64
+    # run from the same initial state (errors per field against the fp64 path)
+    mixed = None
+    if args.mixed_steps > 0:
+        mixed = precision_leg(s, local_rank, args.mixed_steps, args.warmup)
+        mixed["speedup_vs_fp64"] = (ms_max / args.steps) / mixed["ms_per_step"]
+        mixed["fp64_ms_per_step"] = ms_max / args.steps
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, secs, cp = cpu_oracle_rate(args, args.cpu_steps, 1)
@@ -482,6 +575,7 @@ def run_ours(args, rank, world, local_rank):
                               "frac": step_gbs / peak, "algorithmic_bytes_per_step": bstep,
                               "solver_iterations_per_step": iters_per_step},
             "cpu_baseline": cpu,
+            "mixed": mixed,
             "e2e": e2e,
             "gpu_launches": launches,
             "launch_mode": "two-step CUDA graphs (oc_step_graph)" if graph else "one launch per kernel",
@@ -713,10 +807,13 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-nx", type=int, default=128)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["seamount", "ensemble", "helmholtz"], default="seamount",
+    ap.add_argument("--workload", choices=["seamount", "ensemble", "helmholtz", "precision"], default="seamount",
                     help="seamount: the 512x512x50 basin (the headline line); ensemble: the "
                          "batched-ensemble form (its own line); helmholtz: the FP64 and the "
-                         "FP32-inner/FP64-refined Helmholtz solvers alone (its own line)")
+                         "FP32-inner/FP64-refined Helmholtz solvers alone (its own line); precision: "
+                         "the mixed FP32/FP64 step beside the fp64 one (default grid 1024x1024x64)")
+    ap.add_argument("--mixed-steps", type=int, default=100,
+                    help="timed steps of the mixed-precision leg of the headline line (0: skip it)")
     ap.add_argument("--ens-members", type=int, default=64)
     ap.add_argument("--helm-sizes", default="512,1024,2048,4096",
                     help="grid sizes n of the n x n Helmholtz systems")
@@ -730,6 +827,10 @@ def main():
         return run_ensemble(args, rank, world, local_rank)
     if args.workload == "helmholtz":
         return run_helmholtz(args, rank, world, local_rank)
+    if args.workload == "precision":
+        if "--nx" not in sys.argv:
+            args.nx, args.ny, args.nz = 1024, 1024, 64
+        return run_precision(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

@@ -55,6 +55,7 @@ class OcConfig(C.Structure):
         ("c_k", C.c_double), ("c_eps", C.c_double), ("pr_t", C.c_double), ("z_0", C.c_double),
         ("e_min", C.c_double), ("l_min", C.c_double), ("e_bb", C.c_double), ("n2_min", C.c_double),
         ("device", C.c_int32),
+        ("precision", C.c_int32),
     ]
 
 
@@ -159,8 +160,13 @@ def exported_symbols() -> list[str]:
     return list(_SIGNATURES)
 
 
-def config_from_params(p: OceanParams, device: int = 0) -> OcConfig:
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
+def config_from_params(p: OceanParams, device: int = 0, precision: str = "fp64") -> OcConfig:
     p.validate()
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
     c = OcConfig()
     for name in ("nx", "ny", "nz", "n_picard", "n_split", "max_iter"):
         setattr(c, name, int(getattr(p, name)))
@@ -182,6 +188,7 @@ def config_from_params(p: OceanParams, device: int = 0) -> OcConfig:
     c.mxl = MXL[p.mxl]
     c.barotropic_average = BTAVG[p.barotropic_average]
     c.device = int(device)
+    c.precision = PRECISIONS[precision]
     return c
 
 

@@ -1,9 +1,10 @@
 """Build the sm_100a library ``lib/libocean_b200.so`` and the ``bin/ocean3d5_b200``
 executable in-tree with nvcc (cross-compiles without a GPU).
 
-FP contraction is disabled (``-fmad=false``, ``-ffp-contract=off``): the step is
-bit-for-bit equal to the reference's NumPy arithmetic only when every multiply
-and add rounds separately.
+FP contraction is disabled (``-fmad=false``, ``-ffp-contract=off``): the fp64
+step is bit-for-bit equal to the reference's NumPy arithmetic only when every
+multiply and add rounds separately. The 3D step kernels are compiled a second
+time for the mixed-precision path (``-DOC_MIXED``: FP32 fields, contraction on).
 """
 
 from __future__ import annotations
@@ -24,11 +25,14 @@ EXE = BIN_DIR / "ocean3d5_b200"
 # executables over the C ABI: (main source, binary)
 MAINS = [("ocean3d5_main.cpp", EXE), ("helmholtz_bench_main.cpp", BIN_DIR / "helmholtz_bench_b200"),
          ("eos_bench_main.cpp", BIN_DIR / "eos_bench_b200")]
-SOURCES = ["step_kernels.cu", "helmholtz.cu", "helm_refined.cu", "capi.cu", "thomas_noalloc.cu", "standalone.cu",
-           "protocol.cpp"]
+SOURCES = ["step_kernels.cu", "step2d_kernels.cu", "helmholtz.cu", "helm_refined.cu", "capi.cu", "mixed.cu",
+           "thomas_noalloc.cu", "standalone.cu", "protocol.cpp"]
+# (source, object, flags replacing the fp64 contraction flags): the mixed-precision build of the 3D kernels
+MIXED = [("step_kernels.cu", "step_kernels_mixed.o", ["-DOC_MIXED", "-Xcompiler", "-fPIC"])]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--extended-lambda",
-         "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{ROOT / 'include'}", f"-I{CSRC}"]
+COMMON = ["-Wno-deprecated-gpu-targets", "-O3", "-std=c++17", "-lineinfo", "--extended-lambda", f"-I{ROOT / 'include'}",
+          f"-I{CSRC}"]
+FLAGS = COMMON + ["-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off"]
 
 
 def nvcc() -> str:
@@ -61,6 +65,13 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         cmd = [cc, *ARCH, *FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
         if src.endswith(".cpp"):
             cmd = [cc, *FLAGS, "-x", "c++", "-c", str(CSRC / src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(str(obj))
+    for src, name, extra in MIXED:
+        obj = obj_dir / name
+        cmd = [cc, *ARCH, *COMMON, *extra, "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

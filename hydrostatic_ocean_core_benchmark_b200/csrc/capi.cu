@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "capi_internal.cuh"
 #include "helmholtz.cuh"
 #include "oc_internal.cuh"
 #include "ocean_b200.h"
@@ -27,21 +28,24 @@ __global__ void k_fill(double* a, double v, int64_t n) {
     if (t < n) a[t] = v;
 }
 
+// the larger of two magnitudes, NaN winning over every number (a NaN surface
+// elevation must reach the divergence check, as the reference's isnan test does)
+__host__ __device__ inline double nan_max(double a, double b) {
+    if (a != a) return a;
+    if (b != b) return b;
+    return b > a ? b : a;
+}
+
 __global__ void k_absmax_partial(const double* a, int64_t n, double* part) {
     __shared__ double sh[256];
     double m = 0.0;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const double x = fabs(a[t]);
-        if (!(x <= m)) m = x;
-    }
+         t += (int64_t)gridDim.x * blockDim.x)
+        m = nan_max(m, fabs(a[t]));
     sh[threadIdx.x] = m;
     __syncthreads();
     for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-        if (threadIdx.x < k) {
-            const double x = sh[threadIdx.x + k];
-            if (!(x <= sh[threadIdx.x])) sh[threadIdx.x] = x;
-        }
+        if (threadIdx.x < k) sh[threadIdx.x] = nan_max(sh[threadIdx.x], sh[threadIdx.x + k]);
         __syncthreads();
     }
     if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
@@ -55,66 +59,8 @@ static void fill(double* a, double v, int64_t n, cudaStream_t s) {
 
 using namespace oc;
 
-struct oc_handle {
-    oc_config cfg{};
-    std::string err;
-    bool has_domain = false, has_state = false;
-    KP P{};
-    int nx = 0, ny = 0, nz = 0;
-    size_t n2 = 0, n3 = 0, n3i = 0;
-    double h_max = 0.0;
-    int n_split = 0;
-    // host geometry (for oc_get_field and the stress fields)
-    std::vector<double> H, mask, mask_u, mask_v, dzr, dz3, mask3, mask3u, mask3v, dz3u, dz3v, zc;
-    std::vector<double> taux_c, tauy_c;
-    bool stress_field = false;
-    // device memory
-    std::vector<void*> allocs;
-    size_t bytes = 0;
-    double *d_H = nullptr, *d_mask = nullptr, *d_mask_u = nullptr, *d_mask_v = nullptr;
-    double *d_tau_u = nullptr, *d_tau_v = nullptr, *d_ustar2 = nullptr;
-    double *U[2] = {}, *V[2] = {}, *B[2] = {}, *Tt[2] = {}, *Ss[2] = {}, *ETA[2] = {};
-    int cur = 0;
-    double *e = nullptr, *km = nullptr, *kh = nullptr, *q = nullptr, *w = nullptr;
-    double *phi = nullptr, *pgx = nullptr, *pgy = nullptr, *avpv = nullptr, *avpu = nullptr;
-    double *dzu = nullptr, *dzv = nullptr, *stu = nullptr, *stv = nullptr;
-    double *ghu = nullptr, *ghv = nullptr, *uit = nullptr, *vit = nullptr;
-    double *Ku = nullptr, *Kv = nullptr, *gx2 = nullptr, *gy2 = nullptr, *Uold = nullptr,
-           *Vold = nullptr, *div_old = nullptr, *Ug = nullptr, *Vg = nullptr, *rhs2 = nullptr;
-    double *bt[12] = {};  // split-explicit 2D work
-    double* d_part = nullptr;
-    int* d_status = nullptr;
-    HelmSolver* solver = nullptr;
-    // host counters (model3d_v05.py:89-94)
-    long long steps = 0, tridiag = 0, rebuilds = 0, substeps = 0, solves = 0, launches = 0;
-    cudaStream_t last_stream = nullptr;
-    // optional per-kernel event timing
-    bool profiling = false;
-    std::vector<cudaEvent_t> ev_pool;
-    size_t ev_used = 0;
-    std::vector<std::pair<int, size_t>> ev_marks;  // (kernel class, index of the start event)
-    std::vector<std::string> prof_names;
-    std::vector<long long> prof_launches;
-    std::vector<double> prof_ms;
-    // CUDA graphs of two steps (one period of the ping-pong buffers), one per
-    // starting buffer, and the counter increments one launch stands for
-    struct Counters {
-        long long steps, tridiag, rebuilds, substeps, solves, launches;
-    };
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    // second stream for the old-state kernels that do not depend on the closure
-    cudaStream_t aux = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
-    Counters graph_delta[2] = {};
-    cudaStream_t capture_stream = nullptr;
-    long long graph_version = 0;  // bumped whenever recorded graphs go stale
-    // while an ensemble records its graph: every Helmholtz solve of every member
-    // waits on this event and records it, so the cooperative solves run one at a
-    // time and never compete for the SMs
-    cudaEvent_t solve_chain = nullptr;
-};
 
-namespace {
+namespace oc {
 
 // levels one CTA of k_mom_column / k_tracer_rhs marches unless tuned
 constexpr int kDefaultLevelsPerCta = 10;
@@ -166,6 +112,9 @@ int validate(const oc_config* c, std::string& err) {
     if (c->mxl < 0 || c->mxl > 1) return err = "mxl must be integral|recursive", OC_ERR_ARG;
     if (c->barotropic_average < 0 || c->barotropic_average > 1)
         return err = "barotropic_average must be none|mean", OC_ERR_ARG;
+    if (c->precision != OC_PRECISION_FP64 && c->precision != OC_PRECISION_MIXED)
+        return err = "precision must be fp64 or mixed", OC_ERR_ARG;
+    if (c->precision == OC_PRECISION_MIXED) return mixed_validate(c, err);
     return OC_OK;
 }
 
@@ -234,6 +183,14 @@ void fill_scalars(oc_handle* h) {
     P.one_p_kappa3 = 1.0 + kap;
     P.mom_kl = c.nz < kDefaultLevelsPerCta ? c.nz : kDefaultLevelsPerCta;
     P.tr_kl = P.mom_kl;
+    // the fp64 copies the kernels read for their fp64 quantities (equal to the
+    // fields above on this path; dx64, dy64 and the level table are set with the domain)
+    P.rho0_64 = c.rho0;
+    P.alpha_t64 = c.alpha_t;
+    P.beta_s64 = c.beta_s;
+    P.t0_64 = c.t0;
+    P.s0_64 = c.s0;
+    P.neg_g64 = -c.g;
 }
 
 double face_host(int rule, double a, double b) {
@@ -309,11 +266,21 @@ int upload_stress(oc_handle* h) {
     cudaMemcpy(h->d_tau_v, tv.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
     const cudaError_t e = cudaMemcpy(h->d_ustar2, us.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(h, e, "stress upload");
-    return OC_OK;
+    return h->mixed ? mixed_upload_stress(h) : OC_OK;
 }
 
 // q, Ku, Kv and the Helmholtz levels for the current K_m (model3d_v05.py:141-167)
 int build_coefficients(oc_handle* h, cudaStream_t s, bool count_rebuild) {
+    if (h->mixed) {
+        const int rc = mixed_build_coefficients(h, s);
+        if (rc) return rc;
+        h->tridiag += 1;
+        if (h->solver) {
+            h->solver->rebuild(s);
+            if (count_rebuild) h->rebuilds += 1;
+        }
+        return check_launch(h, "coefficients");
+    }
     launch_qsolve(h->P, h->km, h->q, s);
     h->tridiag += 1;
     launch_kukv(h->P, h->q, h->Ku, h->Kv, s);
@@ -354,38 +321,10 @@ int prof_class(oc_handle* h, const char* name) {
     return (int)h->prof_names.size() - 1;
 }
 
-// brackets one kernel (or one fixed group of kernels) with events
-struct Prof {
-    oc_handle* h;
-    cudaStream_t s;
-    int cls = -1;
-    size_t idx = 0;
-    Prof(oc_handle* h_, cudaStream_t s_, const char* name, int n_kernels = 1) : h(h_), s(s_) {
-        h->launches += n_kernels;
-        if (!h->profiling) return;
-        cls = prof_class(h, name);
-        h->prof_launches[cls] += n_kernels;
-        if (h->ev_used + 2 > h->ev_pool.size()) prof_harvest(h);
-        if (h->ev_pool.size() < h->ev_used + 2) {
-            cudaEvent_t a, b;
-            cudaEventCreate(&a);
-            cudaEventCreate(&b);
-            h->ev_pool.push_back(a);
-            h->ev_pool.push_back(b);
-        }
-        idx = h->ev_used;
-        h->ev_used += 2;
-        cudaEventRecord(h->ev_pool[idx], s);
-    }
-    ~Prof() {
-        if (cls < 0) return;
-        cudaEventRecord(h->ev_pool[idx + 1], s);
-        h->ev_marks.push_back({cls, idx});
-    }
-};
 
 // one step (model3d_v05.py:337-415)
 int step_once(oc_handle* h, cudaStream_t s) {
+    if (h->mixed) return step_once_mixed(h, s);
     const oc_config& c = h->cfg;
     const KP& P = h->P;
     const int cur = h->cur, nxt = 1 - cur;
@@ -510,7 +449,8 @@ int step_once(oc_handle* h, cudaStream_t s) {
     {
         // the explicit momentum terms are dead by now: their buffers hold the tracer right-hand sides
         Prof pr(h, s, "tracer_rhs");
-        launch_tracer_rhs(P, h->Tt[cur], h->Ss[cur], b, un, vn, h->w, h->kh, h->pgx, h->pgy, s);
+        launch_tracer_rhs(P, c.tracers == OC_TRACERS_TS ? h->Tt[cur] : b, h->Ss[cur], un, vn, h->w, h->kh, h->pgx,
+                          h->pgy, s);
     }
     {
         Prof pr(h, s, "tracer_solve");
@@ -570,11 +510,13 @@ int capture_graph(oc_handle* h) {
     return OC_OK;
 }
 
-}  // namespace
+}  // namespace oc
 
 extern "C" {
 
-const char* oc_version(void) { return "ocean_b200 1.0 (sm_100a, fp64, bit-parity with the NumPy reference)"; }
+const char* oc_version(void) {
+    return "ocean_b200 1.1 (sm_100a; fp64 path bit-identical to the NumPy reference; mixed FP32/FP64 path)";
+}
 
 int oc_create(const oc_config* cfg, oc_handle** out) {
     if (!cfg || !out) return OC_ERR_ARG;
@@ -605,6 +547,7 @@ int oc_create(const oc_config* cfg, oc_handle** out) {
     h->n2 = (size_t)cfg->nx * cfg->ny;
     h->n3 = h->n2 * cfg->nz;
     h->n3i = h->n2 * (cfg->nz + 1);
+    h->mixed = cfg->precision == OC_PRECISION_MIXED;
     fill_scalars(h);
     *out = h;
     return OC_OK;
@@ -667,6 +610,10 @@ static int set_domain_impl(oc_handle* h, const double* Hh, const double* maskh, 
         P.thin[k] = h->cfg.min_partial * h->dzr[k];
         P.dz_nom[k] = h->cfg.h0 / nz;  // the reference's nominal H/nz (model3d_v05.py:247)
     }
+    for (int k = 0; k <= nz; ++k) P.edge64[k] = P.edge[k];
+    for (int k = 0; k < nz; ++k) P.dzr64[k] = P.dzr[k];
+    P.dx64 = P.dx;
+    P.dy64 = P.dy;
     build_host_geometry(h);
     // compact per-column form of the z-level geometry (kfull, kb, two explicit
     // thicknesses), accepted only where it reproduces the formula exactly
@@ -717,21 +664,25 @@ static int set_domain_impl(oc_handle* h, const double* Hh, const double* maskh, 
     double* d_dzx = dalloc(h, 2 * n2);
     double* d_kface = dalloc(h, n2);
     const bool ts = h->cfg.tracers == OC_TRACERS_TS;
+    const bool f64 = !h->mixed;  // the mixed path keeps its 3D fields in FP32 buffers (mixed.cu)
     for (int t = 0; t < 2; ++t) {
-        h->U[t] = dalloc(h, n3);
-        h->V[t] = dalloc(h, n3);
+        h->U[t] = f64 ? dalloc(h, n3) : nullptr;
+        h->V[t] = f64 ? dalloc(h, n3) : nullptr;
         h->B[t] = dalloc(h, n3);
-        h->Tt[t] = ts ? dalloc(h, n3) : nullptr;
-        h->Ss[t] = ts ? dalloc(h, n3) : nullptr;
+        h->Tt[t] = (ts && f64) ? dalloc(h, n3) : nullptr;
+        h->Ss[t] = (ts && f64) ? dalloc(h, n3) : nullptr;
         h->ETA[t] = dalloc(h, n2);
     }
-    h->e = dalloc(h, n3i);
-    h->km = dalloc(h, n3i);
-    h->kh = dalloc(h, n3i);
-    h->w = dalloc(h, n3i);
-    for (double** p : {&h->q, &h->phi, &h->pgx, &h->pgy, &h->avpv, &h->avpu, &h->dzu, &h->dzv, &h->stu,
-                       &h->stv, &h->ghu, &h->ghv, &h->uit, &h->vit})
-        *p = dalloc(h, n3);
+    h->phi = dalloc(h, n3);
+    if (f64) {
+        h->e = dalloc(h, n3i);
+        h->km = dalloc(h, n3i);
+        h->kh = dalloc(h, n3i);
+        h->w = dalloc(h, n3i);
+        for (double** p : {&h->q, &h->pgx, &h->pgy, &h->avpv, &h->avpu, &h->dzu, &h->dzv, &h->stu, &h->stv,
+                           &h->ghu, &h->ghv, &h->uit, &h->vit})
+            *p = dalloc(h, n3);
+    }
     for (double** p : {&h->Ku, &h->Kv, &h->gx2, &h->gy2, &h->Uold, &h->Vold, &h->div_old, &h->Ug, &h->Vg,
                        &h->rhs2})
         *p = dalloc(h, n2);
@@ -746,7 +697,7 @@ static int set_domain_impl(oc_handle* h, const double* Hh, const double* maskh, 
     }
     for (void* p : h->allocs)
         if (!p) return fail(h, OC_ERR_CUDA, "device allocation failed");
-    if (!h->km || !h->ETA[1] || !h->rhs2) return fail(h, OC_ERR_CUDA, "device allocation failed");
+    if ((f64 && !h->km) || !h->ETA[1] || !h->rhs2) return fail(h, OC_ERR_CUDA, "device allocation failed");
     cudaMemcpy(h->d_H, h->H.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(h->d_mask, h->mask.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(h->d_mask_u, h->mask_u.data(), n2 * sizeof(double), cudaMemcpyHostToDevice);
@@ -764,11 +715,18 @@ static int set_domain_impl(oc_handle* h, const double* Hh, const double* maskh, 
     P.dzx = reinterpret_cast<const double2*>(d_dzx);
     cudaMemcpy(d_kface, kface.data(), n2 * sizeof(int2), cudaMemcpyHostToDevice);
     P.kface = reinterpret_cast<const int2*>(d_kface);
-    int rc = upload_stress(h);
+    P.dzx64 = P.dzx;
+    P.mask_u64 = P.mask_u;
+    P.mask_v64 = P.mask_v;
+    int rc = OC_OK;
+    if (h->mixed && (rc = mixed_alloc(h, kinfo, dzx))) return rc;
+    rc = upload_stress(h);
     if (rc) return rc;
-    fill(h->e, h->cfg.e_min, (int64_t)n3i, 0);
-    fill(h->km, h->cfg.nu, (int64_t)n3i, 0);
-    fill(h->kh, h->cfg.kappa, (int64_t)n3i, 0);
+    if (f64) {
+        fill(h->e, h->cfg.e_min, (int64_t)n3i, 0);
+        fill(h->km, h->cfg.nu, (int64_t)n3i, 0);
+        fill(h->kh, h->cfg.kappa, (int64_t)n3i, 0);
+    }
     if (h->cfg.scheme == OC_SCHEME_THETA) {
         h->solver = new HelmSolver();
         const double coef = h->cfg.g * std::pow(h->cfg.theta, 2.0) * std::pow(h->cfg.dt, 2.0);
@@ -796,6 +754,7 @@ int oc_set_domain_slab(oc_handle* h, const double* Hh, const double* maskh, cons
         return fail(h, OC_ERR_UNSUPPORTED,
                     "a slab of a larger domain steps with scheme fb only: theta needs a global elliptic solve "
                     "and split_explicit a halo exchange per substep");
+    if (h->mixed) return fail(h, OC_ERR_UNSUPPORTED, "slabs of a larger domain step in fp64 only");
     if (!dzrh || !mask_u || !mask_v)
         return fail(h, OC_ERR_ARG, "a slab needs the larger domain's level table and face masks");
     if (!(dx > 0.0) || !(dy > 0.0) || !std::isfinite(dx) || !std::isfinite(dy))
@@ -834,6 +793,7 @@ int halo_fields(oc_handle* h, HaloField* out) {
 
 int rows_check(oc_handle* h, int32_t j0, int32_t nrows, const void* buf) {
     if (!h || !buf) return OC_ERR_ARG;
+    if (h->mixed) return fail(h, OC_ERR_UNSUPPORTED, "row exchange serves the fp64 slabs only");
     if (!h->has_state) return fail(h, OC_ERR_STATE, "set the state before exchanging rows");
     if (j0 < 0 || nrows < 1 || (int64_t)j0 + nrows > h->ny) return fail(h, OC_ERR_ARG, "rows outside the domain");
     return OC_OK;
@@ -864,6 +824,7 @@ int copy_rows(oc_handle* h, int32_t j0, int32_t nrows, double* buf, bool pack, c
 
 int oc_halo_values_per_row(oc_handle* h, int64_t* count) {
     if (!h || !count) return OC_ERR_ARG;
+    if (h->mixed) return fail(h, OC_ERR_UNSUPPORTED, "row exchange serves the fp64 slabs only");
     if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain first");
     HaloField f[9];
     const int n = halo_fields(h, f);
@@ -898,6 +859,8 @@ int oc_set_tiling(oc_handle* h, int32_t mom_levels, int32_t tracer_levels) {
         return fail(h, OC_ERR_ARG, "levels per CTA must lie in 1..nz");
     h->P.mom_kl = mom_levels;
     h->P.tr_kl = tracer_levels;
+    h->P32.mom_kl = mom_levels;
+    h->P32.tr_kl = tracer_levels;
     drop_graphs(h);  // recorded launches carry the old values
     return OC_OK;
 }
@@ -905,6 +868,7 @@ int oc_set_tiling(oc_handle* h, int32_t mom_levels, int32_t tracer_levels) {
 int oc_autotune(oc_handle* h, int32_t* mom_levels, int32_t* tracer_levels) {
     if (!h) return OC_ERR_ARG;
     if (!h->has_state) return fail(h, OC_ERR_STATE, "set the state before tuning");
+    if (h->mixed) return fail(h, OC_ERR_UNSUPPORTED, "the autotuner times the fp64 kernels only");
     cudaSetDevice(h->cfg.device);
     KP P = h->P;
     const int c = h->cur, nz = h->nz;
@@ -929,7 +893,8 @@ int oc_autotune(oc_handle* h, int32_t* mom_levels, int32_t* tracer_levels) {
                     launch_mom_explicit(Q, h->U[c], h->V[c], h->B[c], h->phi, h->w, h->km, h->pgx, h->pgy, h->avpv,
                                         h->avpu, h->dzu, h->dzv, h->stu, h->stv, s);
                 else
-                    launch_tracer_rhs(Q, h->Tt[c], h->Ss[c], h->B[c], h->U[c], h->V[c], h->w, h->kh, h->pgx, h->pgy, s);
+                    launch_tracer_rhs(Q, h->cfg.tracers == OC_TRACERS_TS ? h->Tt[c] : h->B[c], h->Ss[c], h->U[c],
+                                      h->V[c], h->w, h->kh, h->pgx, h->pgy, s);
             };
             run();
             float ms = 1e30f;
@@ -995,6 +960,12 @@ static int set_state_on(oc_handle* h, const oc_state_view* s, int32_t on_device,
     if (ts && (!s->T || !s->S)) return fail(h, OC_ERR_ARG, "T and S are required with TS tracers");
     if (!ts && !s->b) return fail(h, OC_ERR_ARG, "b is required with buoyancy tracers");
     cudaSetDevice(h->cfg.device);
+    if (h->mixed) {
+        const int rc = mixed_set_state(h, s, on_device, st);
+        if (rc) return rc;
+        h->has_state = true;
+        return OC_OK;
+    }
     const int c = h->cur;
     int bad = 0;
     bad |= copy_in(h->ETA[c], s->eta, h->n2, on_device, st);
@@ -1043,6 +1014,13 @@ int oc_reset_mixing(oc_handle* h) {
     if (!h) return OC_ERR_ARG;
     if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain first");
     cudaSetDevice(h->cfg.device);
+    if (h->mixed) {
+        int rc = mixed_reset_mixing(h, 0);
+        if (rc) return rc;
+        if (h->solver) h->solver->rebuild(0);
+        const cudaError_t e = cudaDeviceSynchronize();
+        return e == cudaSuccess ? OC_OK : cuda_fail(h, e, "oc_reset_mixing");
+    }
     fill(h->km, h->cfg.nu, (int64_t)h->n3i, 0);
     fill(h->kh, h->cfg.kappa, (int64_t)h->n3i, 0);
     launch_qsolve(h->P, h->km, h->q, 0);
@@ -1060,6 +1038,7 @@ static int device_status(oc_handle* h) {
 
 // enqueue the copies of the current state on stream st
 static int get_state_on(oc_handle* h, const oc_state_view* s, int32_t on_device, cudaStream_t st) {
+    if (h->mixed) return mixed_get_state(h, s, on_device, st);
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     const int c = h->cur;
     const bool ts = h->cfg.tracers == OC_TRACERS_TS;
@@ -1403,8 +1382,7 @@ int oc_get_stats(oc_handle* h, oc_stats* out) {
         double part[64];
         cudaMemcpy(part, h->d_part, sizeof(part), cudaMemcpyDeviceToHost);
         double m = 0.0;
-        for (double x : part)
-            if (!(x <= m)) m = x;
+        for (double x : part) m = oc::nan_max(m, x);
         out->diverged = !(m < 1.0e6);
     }
     return out->device_status ? fail(h, out->device_status, "a device-side wait ran out its bound") : OC_OK;
@@ -1496,6 +1474,7 @@ int oc_get_field(oc_handle* h, const char* name, double* out, int64_t count) {
     }
     const double* d = nullptr;
     size_t cnt = 0;
+    if (n == "q" && h->mixed) return fail(h, OC_ERR_UNSUPPORTED, "q is an FP32 field on the mixed path");
     if (n == "q") d = h->q, cnt = h->n3;
     else if (n == "ku") d = h->Ku, cnt = h->n2;
     else if (n == "kv") d = h->Kv, cnt = h->n2;

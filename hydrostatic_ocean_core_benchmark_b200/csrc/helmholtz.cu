@@ -211,6 +211,53 @@ __device__ double tree_fold(const HelmParams& H, const FoldPlan& F, const double
     return r;
 }
 
+// The same fold for grids whose leaf sums do not fit one CTA's shared memory
+// (H.big_fold): the tree is cut below the nodes of at most a block's worth of
+// leaves. Each block subtree is folded by one CTA and its root written to
+// `broot`; after a grid barrier every CTA folds the top of the tree over the
+// block roots. Every addition is the one of the whole-tree fold, in the same
+// order, so the result is bit-identical; it costs one more grid barrier. Each
+// leaf buffer has its own root buffer, so folds that follow one another without
+// a barrier never overwrite roots another CTA is still reading.
+__device__ double fold_blocks(const HelmParams& H, const double* leaf, double* broot, double* sm, bool& ok) {
+    for (int j = blockIdx.x; j < H.n_blocks; j += gridDim.x) {
+        const int4 B = H.blocks[j];  // first leaf, leaves, offset of its height starts, heights
+        for (int t = threadIdx.x; t < B.y; t += blockDim.x) sm[t] = __ldcg(leaf + B.x + t);
+        __syncthreads();
+        for (int h = 0; h < B.w; ++h) {
+            for (int t = H.bh_start[B.z + h] + threadIdx.x; t < H.bh_start[B.z + h + 1]; t += blockDim.x) {
+                const int2 op = H.bops[t];
+                sm[op.x] = sm[op.x] + sm[op.y];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) broot[j] = sm[0];
+        __syncthreads();
+    }
+    ok = grid_sync(H);
+    if (!ok) return 0.0;
+    for (int t = threadIdx.x; t < H.n_blocks; t += blockDim.x) sm[t] = __ldcg(broot + t);
+    __syncthreads();
+    for (int h = 0; h < H.top_heights; ++h) {
+        for (int t = H.top_hstart[h] + threadIdx.x; t < H.top_hstart[h + 1]; t += blockDim.x) {
+            const int2 op = H.top_ops[t];
+            sm[op.x] = sm[op.x] + sm[op.y];
+        }
+        __syncthreads();
+    }
+    const double r = sm[0];
+    __syncthreads();
+    return r;
+}
+
+// the sum of one of the leaf buffers (leafA, leafB or leafC) in NumPy's order
+__device__ __forceinline__ double fold_sum(const HelmParams& H, const FoldPlan& F, const double* leaf, double* sm,
+                                           bool& ok) {
+    if (!H.big_fold) return tree_fold(H, F, leaf, sm);
+    double* broot = leaf == H.leafA ? H.broot : (leaf == H.leafB ? H.broot + H.n_blocks : H.broot + 2 * H.n_blocks);
+    return fold_blocks(H, leaf, broot, sm, ok);
+}
+
 // ------------------------------------------------------------------ tiled multigrid
 // A fine level is processed tile by tile in shared memory. The down phase loads
 // x, b and the coefficients of a tile plus a HALO-wide ring, runs the two
@@ -757,7 +804,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                },
                H.leafA, nullptr);
     ok = grid_sync(H);
-    const double norm_b = ok ? sqrt(tree_fold(H, fold, H.leafA, sm)) : 0.0;
+    const double norm_b = ok ? sqrt(fold_sum(H, fold, H.leafA, sm, ok)) : 0.0;
     if (persist) persist_level0(H, persist);  // the coefficients are fixed during the solve
     if (!ok || norm_b == 0.0) goto done;
     {
@@ -791,7 +838,8 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                     if (!ok) break;
                 }
                 iters = it;
-                const double res = sqrt(tree_fold(H, fold, H.leafA, sm));
+                const double res = sqrt(fold_sum(H, fold, H.leafA, sm, ok));
+                if (!ok) break;
                 if (res <= tol) {
                     conv = 1;
                     break;
@@ -838,7 +886,8 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                        H.leafB, nullptr);
             ok = grid_sync(H);
             if (!ok) goto done;
-            double rz = tree_fold(H, fold, H.leafB, sm);
+            double rz = fold_sum(H, fold, H.leafB, sm, ok);
+            if (!ok) goto done;
             conv = 0;
             for (int it = 1; it <= H.max_iter; ++it) {
                 leaf_phase(H,
@@ -850,7 +899,8 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                            H.leafC, nullptr);
                 ok = grid_sync(H);
                 if (!ok) break;
-                const double alpha = rz / tree_fold(H, fold, H.leafC, sm);
+                const double alpha = rz / fold_sum(H, fold, H.leafC, sm, ok);
+                if (!ok) break;
                 leaf_phase(H,
                            [&](int e) {
                                const double pe = __ldcg(p + e);
@@ -870,7 +920,8 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                 ok = grid_sync(H);
                 if (!ok) break;
                 iters = it;
-                const double res = sqrt(tree_fold(H, fold, H.leafA, sm));
+                const double res = sqrt(fold_sum(H, fold, H.leafA, sm, ok));
+                if (!ok) break;
                 if (res <= tol) {
                     conv = 1;
                     break;
@@ -887,7 +938,8 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
                     ok = grid_sync(H);
                     if (!ok) break;
                 }
-                const double rz_new = tree_fold(H, fold, H.leafB, sm);
+                const double rz_new = fold_sum(H, fold, H.leafB, sm, ok);
+                if (!ok) break;
                 const double beta = rz_new / rz;
                 for (int e = grid_team().first; e < L0.n; e += grid_team().stride)
                     p[e] = __ldcg(z + e) + beta * __ldcg(p + e);
@@ -963,6 +1015,57 @@ static PwNode pairwise_build(long start, long n, std::vector<int>& leaves,
     by_height[height - 1].push_back(make_int2(a.lo, b.lo));
     return {a.lo, height};
 }
+
+// leaves of NumPy's pairwise tree over n contiguous elements
+static long pairwise_leaves(long n) {
+    if (n <= 128) return 1;
+    long h = n / 2;
+    h -= h % 8;
+    return pairwise_leaves(h) + pairwise_leaves(n - h);
+}
+
+// The two-level form of the same tree: nodes of at most `block_leaves` leaves
+// become blocks, each with its own plan (leaf indices relative to its first
+// leaf; `hstart` gets heights + 1 offsets into `bops` per block), and the nodes
+// above them form the top plan over the block indices. `leaves` receives every
+// leaf in order, as pairwise_build gives them.
+struct TwoLevelPlan {
+    std::vector<int> leaves;
+    std::vector<int4> blocks;
+    std::vector<int2> bops;
+    std::vector<int> bh_start;
+    std::vector<std::vector<int2>> top_by_height;
+};
+
+static PwNode pairwise_build_two_level(long start, long n, long block_leaves, TwoLevelPlan& T) {
+    if (pairwise_leaves(n) <= block_leaves) {
+        std::vector<int> lv;
+        std::vector<std::vector<int2>> byh;
+        pairwise_build(start, n, lv, byh);
+        const int4 b = make_int4((int)T.leaves.size(), (int)lv.size(), (int)T.bh_start.size(), (int)byh.size());
+        T.leaves.insert(T.leaves.end(), lv.begin(), lv.end());
+        for (const auto& ops : byh) {
+            T.bh_start.push_back((int)T.bops.size());
+            T.bops.insert(T.bops.end(), ops.begin(), ops.end());
+        }
+        T.bh_start.push_back((int)T.bops.size());
+        T.blocks.push_back(b);
+        return {(int)T.blocks.size() - 1, 0};
+    }
+    long h = n / 2;
+    h -= h % 8;
+    const PwNode a = pairwise_build_two_level(start, h, block_leaves, T);
+    const PwNode b = pairwise_build_two_level(start + h, n - h, block_leaves, T);
+    const int height = std::max(a.height, b.height) + 1;
+    if ((int)T.top_by_height.size() < height) T.top_by_height.resize(height);
+    T.top_by_height[height - 1].push_back(make_int2(a.lo, b.lo));
+    return {a.lo, height};
+}
+
+// leaf sums beyond which the fold runs in two levels (their doubles would not
+// fit one CTA's shared memory beside the rest), and the leaves of one block
+static constexpr long kFoldOneLevelLeaves = 16384;
+static constexpr long kFoldBlockLeaves = 8192;
 
 void* HelmSolver::dalloc(size_t nbytes) {
     void* p = nullptr;
@@ -1053,10 +1156,17 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     H.z = (double*)dalloc(sizeof(double) * n);
     H.p = (double*)dalloc(sizeof(double) * n);
     H.Ap = (double*)dalloc(sizeof(double) * n);
-    // pairwise plan
+    // pairwise plan (two-level for grids whose leaf sums exceed shared memory)
     std::vector<int> leaves;
     std::vector<std::vector<int2>> by_height;
-    pairwise_build(0, (long)n, leaves, by_height);
+    TwoLevelPlan two;
+    H.big_fold = pairwise_leaves((long)n) > kFoldOneLevelLeaves ? 1 : 0;
+    if (H.big_fold) {
+        pairwise_build_two_level(0, (long)n, kFoldBlockLeaves, two);
+        leaves = two.leaves;
+    } else {
+        pairwise_build(0, (long)n, leaves, by_height);
+    }
     leaves.push_back((int)n);
     std::vector<int> hstart{0};
     std::vector<int2> ops;
@@ -1090,6 +1200,41 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     H.ops = d_ops;
     H.n_ops = (int)ops.size();
     H.bar_count = bar;
+    size_t fold_doubles = (size_t)H.n_leaves;  // shared memory the fold needs
+    if (H.big_fold) {
+        H.n_blocks = (int)two.blocks.size();
+        std::vector<int> top_hstart{0};
+        std::vector<int2> top_ops;
+        for (auto& v : two.top_by_height) {
+            top_ops.insert(top_ops.end(), v.begin(), v.end());
+            top_hstart.push_back((int)top_ops.size());
+        }
+        H.top_heights = (int)two.top_by_height.size();
+        int4* d_blocks = (int4*)dalloc(sizeof(int4) * two.blocks.size());
+        int2* d_bops = (int2*)dalloc(sizeof(int2) * std::max<size_t>(1, two.bops.size()));
+        int* d_bh = (int*)dalloc(sizeof(int) * two.bh_start.size());
+        int2* d_top = (int2*)dalloc(sizeof(int2) * std::max<size_t>(1, top_ops.size()));
+        int* d_top_h = (int*)dalloc(sizeof(int) * top_hstart.size());
+        H.broot = (double*)dalloc(sizeof(double) * 3 * (size_t)H.n_blocks);
+        if (!d_blocks || !d_bops || !d_bh || !d_top || !d_top_h || !H.broot) {
+            err = "cudaMalloc failed (Helmholtz reduction plan)";
+            return OC_ERR_CUDA;
+        }
+        cudaMemcpy(d_blocks, two.blocks.data(), sizeof(int4) * two.blocks.size(), cudaMemcpyHostToDevice);
+        if (!two.bops.empty())
+            cudaMemcpy(d_bops, two.bops.data(), sizeof(int2) * two.bops.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(d_bh, two.bh_start.data(), sizeof(int) * two.bh_start.size(), cudaMemcpyHostToDevice);
+        if (!top_ops.empty())
+            cudaMemcpy(d_top, top_ops.data(), sizeof(int2) * top_ops.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(d_top_h, top_hstart.data(), sizeof(int) * top_hstart.size(), cudaMemcpyHostToDevice);
+        H.blocks = d_blocks;
+        H.bops = d_bops;
+        H.bh_start = d_bh;
+        H.top_ops = d_top;
+        H.top_hstart = d_top_h;
+        fold_doubles = (size_t)H.n_blocks;
+        for (const int4& b : two.blocks) fold_doubles = std::max(fold_doubles, (size_t)b.y);
+    }
     // co-resident grid for the cooperative launch
     int dev = 0, sms = 0, coop = 0;
     cudaGetDevice(&dev);
@@ -1151,8 +1296,7 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     const size_t coarse_work = 6 * coarse_cells + (H.coarse_from < H.n_levels ? (size_t)H.lv[H.coarse_from].n : 0);
     const size_t mg_work = (kind == HK_MULTIGRID) ? std::max<size_t>(tile_work, coarse_work) : 0;
     // the tree fold and the V-cycle never run at the same time: one region serves both
-    smem_ = sizeof(double) * ((H.persist0 ? 4 * (size_t)TileWide::RN : 0) +
-                              std::max<size_t>((size_t)H.n_leaves, mg_work));
+    smem_ = sizeof(double) * ((H.persist0 ? 4 * (size_t)TileWide::RN : 0) + std::max<size_t>(fold_doubles, mg_work));
     int smem_optin = 0;
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncAttributes fa{};
@@ -1160,7 +1304,7 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     // the fold's plan joins shared memory when it fits beside the rest
     const size_t plan_doubles = (sizeof(int2) * ops.size() + sizeof(int) * hstart.size() + sizeof(double) - 1) / sizeof(double);
     H.ops_smem = 0;
-    if (smem_ + sizeof(double) * plan_doubles + fa.sharedSizeBytes <= (size_t)smem_optin) {
+    if (!H.big_fold && smem_ + sizeof(double) * plan_doubles + fa.sharedSizeBytes <= (size_t)smem_optin) {
         H.ops_smem = (int)plan_doubles;
         smem_ += sizeof(double) * plan_doubles;
     }

@@ -43,6 +43,16 @@ struct HelmParams {
     double* leafA;
     double* leafB;
     double* leafC;
+    // two-level fold when the leaf sums exceed shared memory (big_fold): block
+    // subtrees (first leaf, leaves, offset into bh_start, heights) with their ops
+    // relative to the block's first leaf, then the top of the tree over the roots
+    int big_fold, n_blocks, top_heights;
+    const int4* blocks;
+    const int2* bops;
+    const int* bh_start;
+    const int2* top_ops;
+    const int* top_hstart;
+    double* broot;  // 3 x n_blocks: one root buffer per leaf buffer
     // grid barrier and status
     unsigned long long* bar_count;  // grid barrier arrivals (only grows)
     int* status;

@@ -1,11 +1,17 @@
 // Internal definitions of the sm_100a ocean-core step.
 //
 // Bit-for-bit parity with the reference NumPy step (libs/core/model3d_v05.py)
-// is a design rule: every expression below performs the same IEEE-754 fp64
-// operations in the same order as the reference, the library is compiled with
-// -fmad=false (no contraction into FMA) and reductions follow the reference's
-// summation order (sequential over k for column sums; NumPy's pairwise tree
-// for the global dot products of the Helmholtz solver).
+// is a design rule of the fp64 path: every expression below performs the same
+// IEEE-754 fp64 operations in the same order as the reference, the fp64 build
+// is compiled with -fmad=false (no contraction into FMA) and reductions follow
+// the reference's summation order (sequential over k for column sums; NumPy's
+// pairwise tree for the global dot products of the Helmholtz solver).
+//
+// The helpers are templates on the floating type T of the step's 3D fields:
+// T = double is the fp64 path (every literal T(x) is then the same double, so
+// the operations are exactly the reference's); T = float is the mixed-precision
+// path, whose stencils and column solves run in FP32 (compiled separately, with
+// contraction).
 //
 // Static geometry is never stored as 3D arrays on the device: the z-level
 // thickness of a cell is a function of its column's depth H and the level
@@ -21,54 +27,71 @@
 
 namespace oc {
 
+template <class T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
 // Everything a step kernel needs, passed by value (lives in the kernel
-// parameter bank, constant-cached).
-struct KP {
+// parameter bank, constant-cached). T is the floating type of the 3D fields.
+// The fp64 copies (dx64, dy64, edge64, dzx64, eos constants) serve the few
+// quantities the mixed path keeps in FP64 (pressure-gradient depths, the EOS,
+// the surface-elevation gradient); in the fp64 path they equal the T fields.
+template <class T>
+struct KPT {
     int nx, ny, nz, n2, n3, n3i;
-    double dx, dy;
+    T dx, dy;
     // options
     int eos, pgf_remove, pgf_correction, advection, tracers_ts, closure_tke, mxl_recursive;
     int scheme;  // 0 fb, 1 theta, 2 split
     // physical constants
-    double dt, g, f0, rho0, N2, nu, kappa, bottom_drag, a_h, k_h;
-    double alpha_t, beta_s, t0, s0;
-    double c_k, c_eps, pr_t, z_0, e_min, l_min, e_bb, n2_min;
-    double theta, theta_cor, theta_v;
+    T dt, g, f0, rho0, N2, nu, kappa, bottom_drag, a_h, k_h;
+    T alpha_t, beta_s, t0, s0;
+    T c_k, c_eps, pr_t, z_0, e_min, l_min, e_bb, n2_min;
+    T theta, theta_cor, theta_v;
     // host-precomputed scalar products, formed in the reference's order
-    double thv_dt;        // theta_v * dt
-    double thv_dt_drag;   // (theta_v * dt) * bottom_drag
-    double thv_dt_zero;   // (theta_v * dt) * 0.0 (tracer rows have no drag)
-    double c1;            // (g * dt) * (1 - theta_eff)   explicit surface gradient
-    double c2;            // (g * dt) * theta_eff         back-substitution
-    double c3;            // (1 - theta_v) * dt           explicit vertical diffusion
-    double one_m_tc;      // 1 - theta_cor
-    double one_m_th;      // 1 - theta_eff
-    double neg_f0;        // -f0
-    double neg_g;         // -g
-    double neg_n2;        // -N2
-    double flux_t, flux_s;  // surface tracer fluxes
-    double one_m_kappa3, one_p_kappa3;  // 1 - 1/3, 1 + 1/3
+    T thv_dt;        // theta_v * dt
+    T thv_dt_drag;   // (theta_v * dt) * bottom_drag
+    T thv_dt_zero;   // (theta_v * dt) * 0.0 (tracer rows have no drag)
+    T c1;            // (g * dt) * (1 - theta_eff)   explicit surface gradient
+    T c2;            // (g * dt) * theta_eff         back-substitution
+    T c3;            // (1 - theta_v) * dt           explicit vertical diffusion
+    T one_m_tc;      // 1 - theta_cor
+    T one_m_th;      // 1 - theta_eff
+    T neg_f0;        // -f0
+    T neg_g;         // -g
+    T neg_n2;        // -N2
+    T flux_t, flux_s;  // surface tracer fluxes
+    T one_m_kappa3, one_p_kappa3;  // 1 - 1/3, 1 + 1/3
     // level table
-    double edge[OC_MAXNZ + 1];   // depth of level tops, cumsum of dzr
-    double dzr[OC_MAXNZ];
-    double thin[OC_MAXNZ];       // min_partial * dzr
-    double dz_nom[OC_MAXNZ];     // spacing of the momentum vertical advection per level
+    T edge[OC_MAXNZ + 1];   // depth of level tops, cumsum of dzr
+    T dzr[OC_MAXNZ];
+    T thin[OC_MAXNZ];       // min_partial * dzr
+    T dz_nom[OC_MAXNZ];     // spacing of the momentum vertical advection per level
     // static 2D fields
-    const double* H;
-    const double* mask;
-    const double* mask_u;
-    const double* mask_v;
-    const double* tau_u;   // surface stress / rho0 at u faces, masked
-    const double* tau_v;
-    const double* ustar2;  // closure surface u*^2
+    const T* H;
+    const T* mask;
+    const T* mask_u;
+    const T* mask_v;
+    const T* tau_u;   // surface stress / rho0 at u faces, masked
+    const T* tau_v;
+    const T* ustar2;  // closure surface u*^2
     const int2* kinfo;     // per column: (levels of exact thickness dzr, wet levels)
-    const double2* dzx;    // per column: thickness of wet levels kfull and kfull + 1
+    const typename Vec2<T>::type* dzx;  // per column: thickness of wet levels kfull and kfull + 1
     const int2* kface;     // per column: wet levels of its east (x) and north (y) face
     int face_rule;         // 0 min, 1 mean, 2 harmonic
     // levels one CTA marches in k_mom_column and k_tracer_rhs (1..nz); every
     // value gives the same results, only the speed depends on it
     int mom_kl, tr_kl;
+    // fp64 copies (see above)
+    double dx64, dy64;
+    double rho0_64, alpha_t64, beta_s64, t0_64, s0_64, neg_g64;
+    const double* mask_u64;
+    const double* mask_v64;
+    const double2* dzx64;
+    double edge64[OC_MAXNZ + 1];
+    double dzr64[OC_MAXNZ];
 };
+using KP = KPT<double>;
 
 __device__ __forceinline__ int wrapi(int i, int n) {
     if (i < 0) i += n;
@@ -80,7 +103,8 @@ __device__ __forceinline__ int wrapi(int i, int n) {
     return i;
 }
 
-__device__ __forceinline__ double inv_pos(double a) { return a > 0.0 ? 1.0 / a : 0.0; }
+template <class T>
+__device__ __forceinline__ T inv_pos(T a) { return a > T(0.0) ? T(1.0) / a : T(0.0); }
 
 // z-level partial-cell thickness of level k of column c and its wet mask
 // (reference domain.py:113-129: dz3_ref = clip(H - edge, 0, dzr) with thin
@@ -89,41 +113,43 @@ __device__ __forceinline__ double inv_pos(double a) { return a > 0.0 ? 1.0 / a :
 // exactly), levels kfull..kb-1 are wet with the explicit thicknesses dzx, levels
 // from kb on are dry -- after checking that it reproduces the formula bit for
 // bit, so no 3D geometry array is ever read.
-__device__ __forceinline__ double col_dz(const KP& P, int c, int k, double& m3) {
+template <class T>
+__device__ __forceinline__ T col_dz(const KPT<T>& P, int c, int k, T& m3) {
     const int2 ki = P.kinfo[c];
     if (k >= ki.y) {
-        m3 = 0.0;
-        return 0.0;
+        m3 = T(0.0);
+        return T(0.0);
     }
-    m3 = 1.0;
+    m3 = T(1.0);
     if (k < ki.x) return P.dzr[k];
-    const double2 dx = P.dzx[c];
+    const auto dx = P.dzx[c];
     return k == ki.x ? dx.x : dx.y;
 }
 
 // the compact geometry of one column held in registers; dz() equals col_dz()
-struct ColGeo {
+template <class T>
+struct ColGeoT {
     int kf, kb;
-    double d0, d1;
-    __device__ __forceinline__ static ColGeo load(const KP& P, int c) {
+    T d0, d1;
+    __device__ __forceinline__ static ColGeoT load(const KPT<T>& P, int c) {
         const int2 ki = P.kinfo[c];
-        const double2 dx = P.dzx[c];
-        return ColGeo{ki.x, ki.y, dx.x, dx.y};
+        const auto dx = P.dzx[c];
+        return ColGeoT{ki.x, ki.y, dx.x, dx.y};
     }
-    __device__ __forceinline__ double dz(const KP& P, int k, double& m3) const {
+    __device__ __forceinline__ T dz(const KPT<T>& P, int k, T& m3) const {
         if (k >= kb) {
-            m3 = 0.0;
-            return 0.0;
+            m3 = T(0.0);
+            return T(0.0);
         }
-        m3 = 1.0;
+        m3 = T(1.0);
         if (k < kf) return P.dzr[k];
         return k == kf ? d0 : d1;
     }
     // depth of the top of level k: the sequential sum of the thicknesses above
     // (col_above with the column's geometry in registers)
-    __device__ __forceinline__ double above(const KP& P, int k) const {
+    __device__ __forceinline__ T above(const KPT<T>& P, int k) const {
         const int m = k < kf ? k : kf;
-        double a = P.edge[m];
+        T a = P.edge[m];
         if (k > kf && kf < kb) {
             a = (m == 0) ? d0 : a + d0;
             if (k > kf + 1 && kf + 1 < kb) a = a + d1;
@@ -132,22 +158,57 @@ struct ColGeo {
     }
 };
 
-__device__ __forceinline__ double col_m3(const KP& P, int c, int k) { return k < P.kinfo[c].y ? 1.0 : 0.0; }
+using ColGeo = ColGeoT<double>;
+
+// the same column geometry in fp64 from the fp64 copies (the fp64 path's values
+// exactly): the depths the mixed path's pressure gradient and EOS are formed at
+struct ColGeo64 {
+    int kf, kb;
+    double d0, d1;
+    template <class T>
+    __device__ __forceinline__ static ColGeo64 load(const KPT<T>& P, int c) {
+        const int2 ki = P.kinfo[c];
+        const double2 dx = P.dzx64[c];
+        return ColGeo64{ki.x, ki.y, dx.x, dx.y};
+    }
+    template <class T>
+    __device__ __forceinline__ double dz(const KPT<T>& P, int k) const {
+        if (k >= kb) return 0.0;
+        if (k < kf) return P.dzr64[k];
+        return k == kf ? d0 : d1;
+    }
+    template <class T>
+    __device__ __forceinline__ double above(const KPT<T>& P, int k) const {
+        const int m = k < kf ? k : kf;
+        double a = P.edge64[m];
+        if (k > kf && kf < kb) {
+            a = (m == 0) ? d0 : a + d0;
+            if (k > kf + 1 && kf + 1 < kb) a = a + d1;
+        }
+        return a;
+    }
+};
+
+template <class T>
+__device__ __forceinline__ T col_m3(const KPT<T>& P, int c, int k) { return k < P.kinfo[c].y ? T(1.0) : T(0.0); }
 
 // 3D face masks m3 * m3(neighbour) * mask_face (domain.py:93-96): the wet levels
 // of a face are the top min(kb, kb of the neighbour) levels when the 2D face
 // is open, so one integer per face and column (checked on the host) gives them
-__device__ __forceinline__ double col_m3u(const KP& P, int c, int k) { return k < P.kface[c].x ? 1.0 : 0.0; }
-__device__ __forceinline__ double col_m3v(const KP& P, int c, int k) { return k < P.kface[c].y ? 1.0 : 0.0; }
+template <class T>
+__device__ __forceinline__ T col_m3u(const KPT<T>& P, int c, int k) { return k < P.kface[c].x ? T(1.0) : T(0.0); }
+template <class T>
+__device__ __forceinline__ T col_m3v(const KPT<T>& P, int c, int k) { return k < P.kface[c].y ? T(1.0) : T(0.0); }
 
 // depth of the top of level k (the sequential sum of dz3 above it) and of the
 // level centre (reference domain.py:148-154)
-__device__ __forceinline__ double col_above(const KP& P, int c, int k) {
+template <class T>
+__device__ __forceinline__ T col_above(const KPT<T>& P, int c, int k) {
     const int2 ki = P.kinfo[c];
     const int m = k < ki.x ? k : ki.x;
-    double above = P.edge[m];
+    T above = P.edge[m];
     if (k > ki.x && ki.x < ki.y) {
-        const double2 dx = P.dzx[c];
+        const auto dx = P.dzx[c];
         above = (m == 0) ? dx.x : above + dx.x;
         if (k > ki.x + 1 && ki.x + 1 < ki.y) above = above + dx.y;
     }
@@ -155,16 +216,18 @@ __device__ __forceinline__ double col_above(const KP& P, int c, int k) {
 }
 
 
-__device__ __forceinline__ double face_combine(const KP& P, double a, double b) {
+template <class T>
+__device__ __forceinline__ T face_combine(const KPT<T>& P, T a, T b) {
     if (P.face_rule == 0) return fmin(a, b);
-    if (P.face_rule == 1) return 0.5 * (a + b);
-    double tot = a + b;
-    return tot > 0.0 ? 2.0 * a * b / tot : 0.0;
+    if (P.face_rule == 1) return T(0.5) * (a + b);
+    T tot = a + b;
+    return tot > T(0.0) ? T(2.0) * a * b / tot : T(0.0);
 }
 
 // Superbee limiter of the TVD face (reference advection_v06.py:35-43)
-__device__ __forceinline__ double superbee(double r) {
-    return fmax(0.0, fmax(fmin(2.0 * r, 1.0), fmin(r, 2.0)));
+template <class T>
+__device__ __forceinline__ T superbee(T r) {
+    return fmax(T(0.0), fmax(fmin(T(2.0) * r, T(1.0)), fmin(r, T(2.0))));
 }
 
 // Upwind-biased value on the face between c0 and c1 (c_m = left of c0,
@@ -174,47 +237,46 @@ __device__ __forceinline__ double superbee(double r) {
 // are selected first and one value is formed: for vel <= 0 the reference's
 // c1 - t equals c1 + (-t) exactly, so the bits are the same, with one division
 // instead of two and no divergent branch.
-__device__ __forceinline__ double kappa_face(const KP& P, double cm, double c0, double c1, double cp,
-                                             double vel, double wm, double wp, bool limited) {
-    const bool pos = vel > 0.0;
-    const double base = pos ? c0 : c1;
-    const double far = pos ? (c0 - cm) : (cp - c1);
-    const double d = c1 - c0;
-    double t;
+template <class T>
+__device__ __forceinline__ T kappa_face(const KPT<T>& P, T cm, T c0, T c1, T cp, T vel, T wm, T wp, bool limited) {
+    const bool pos = vel > T(0.0);
+    const T base = pos ? c0 : c1;
+    const T far = pos ? (c0 - cm) : (cp - c1);
+    const T d = c1 - c0;
+    T t;
     if (limited) {
-        const double eps = d == 0.0 ? 1.0 : d;
-        const double r = d == 0.0 ? 0.0 : far / eps;
-        t = 0.5 * superbee(r) * d;
+        const T eps = d == T(0.0) ? T(1.0) : d;
+        const T r = d == T(0.0) ? T(0.0) : far / eps;
+        t = T(0.5) * superbee(r) * d;
     } else {
-        t = 0.25 * (P.one_m_kappa3 * far + P.one_p_kappa3 * d);
+        t = T(0.25) * (P.one_m_kappa3 * far + P.one_p_kappa3 * d);
     }
-    const double f = base + (pos ? t : -t);
-    return ((pos ? wm : wp) > 0.0) ? f : base;
+    const T f = base + (pos ? t : -t);
+    return ((pos ? wm : wp) > T(0.0)) ? f : base;
 }
 
 // Interior vertical face value at an interface with `above` (layer k-1),
 // `below` (layer k), far_up (k-2, 0 when absent), far_dn (k+1, 0 when absent)
 // and wet flags of the far cells; w positive upward. advection_v06.py:50-74,
 // selected before forming as in kappa_face.
-__device__ __forceinline__ double kappa_face_z(const KP& P, double far_up, double above, double below,
-                                               double far_dn, double w, bool has_up, bool has_dn,
-                                               bool limited) {
-    const bool up = w > 0.0;
-    const double base = up ? below : above;
-    const double far = up ? (below - far_dn) : (far_up - above);
-    const double d = above - below;
-    double t;
+template <class T>
+__device__ __forceinline__ T kappa_face_z(const KPT<T>& P, T far_up, T above, T below, T far_dn, T w, bool has_up,
+                                          bool has_dn, bool limited) {
+    const bool up = w > T(0.0);
+    const T base = up ? below : above;
+    const T far = up ? (below - far_dn) : (far_up - above);
+    const T d = above - below;
+    T t;
     if (limited) {
-        const double eps = d == 0.0 ? 1.0 : d;
-        const double r = d == 0.0 ? 0.0 : far / eps;
-        t = 0.5 * superbee(r) * d;
+        const T eps = d == T(0.0) ? T(1.0) : d;
+        const T r = d == T(0.0) ? T(0.0) : far / eps;
+        t = T(0.5) * superbee(r) * d;
     } else {
-        t = 0.25 * (P.one_m_kappa3 * far + P.one_p_kappa3 * d);
+        t = T(0.25) * (P.one_m_kappa3 * far + P.one_p_kappa3 * d);
     }
-    const double f = base + (up ? t : -t);
+    const T f = base + (up ? t : -t);
     return (up ? has_dn : has_up) ? f : base;
 }
-
 // ---------------------------------------------------------------- EOS
 // polyTEOS10-bsq (Roquet et al. 2015, Table 4) and the S-EOS of their eq. (25):
 // the published coefficients, in the Horner form of reference eos.py:68-111.
@@ -267,12 +329,17 @@ __device__ __forceinline__ double rho_anomaly_of(int eos, double rho0, double al
     return rho_teos10(T, S, z) - rho0;
 }
 
-__device__ __forceinline__ double rho_anomaly(const KP& P, double T, double S, double z) {
-    return rho_anomaly_of(P.eos, P.rho0, P.alpha_t, P.beta_s, P.t0, P.s0, T, S, z);
+// The EOS is evaluated in fp64 on both paths, with the fp64 copies of the
+// constants (in the fp64 path they are the constants themselves): in FP32 the
+// anomaly rho - rho0 of a ~1027 kg m-3 density would keep only ~3 digits.
+template <class T>
+__device__ __forceinline__ double rho_anomaly(const KPT<T>& P, double Tc, double Sa, double z) {
+    return rho_anomaly_of(P.eos, P.rho0_64, P.alpha_t64, P.beta_s64, P.t0_64, P.s0_64, Tc, Sa, z);
 }
 
-__device__ __forceinline__ double buoyancy_of(const KP& P, double T, double S, double z) {
-    return P.neg_g * rho_anomaly(P, T, S, z) / P.rho0;
+template <class T>
+__device__ __forceinline__ double buoyancy_of(const KPT<T>& P, double Tc, double Sa, double z) {
+    return P.neg_g64 * rho_anomaly(P, Tc, Sa, z) / P.rho0_64;
 }
 
 // ---------------------------------------------------------------- launch helpers

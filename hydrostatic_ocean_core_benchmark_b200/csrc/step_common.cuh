@@ -1,0 +1,52 @@
+// Helpers shared by the step's 3D kernels (step_kernels.cu, compiled for the
+// fp64 and the mixed-precision path) and its 2D kernels (step2d_kernels.cu).
+#pragma once
+
+#include "oc_internal.cuh"
+
+namespace oc {
+
+// neighbour offsets of one column, wrapped once (periodic index layout, up to
+// three cells away)
+struct Nbr {
+    int i, j, c;
+    int nx, ny;
+    int ix[7], jy[7];  // i-3..i+3 and (j-3..j+3) * nx, wrapped
+    __device__ __forceinline__ void init(int i_, int j_, int nx_, int ny_) {
+        i = i_;
+        j = j_;
+        nx = nx_;
+        ny = ny_;
+        c = j * nx + i;
+#pragma unroll
+        for (int d = -3; d <= 3; ++d) {
+            ix[d + 3] = wrapi(i + d, nx);
+            jy[d + 3] = wrapi(j + d, ny) * nx;
+        }
+    }
+    __device__ __forceinline__ int at(int dj, int di) const { return jy[dj + 3] + ix[di + 3]; }
+};
+
+#define COLUMN_PROLOGUE                                  \
+    const int i = blockIdx.x * blockDim.x + threadIdx.x; \
+    const int j = blockIdx.y * blockDim.y + threadIdx.y; \
+    if (i >= P.nx || j >= P.ny) return;                  \
+    Nbr nb;                                              \
+    nb.init(i, j, P.nx, P.ny);                           \
+    const size_t n2 = (size_t)P.n2;                      \
+    (void)n2;
+
+// face thickness at level k of a face whose wet levels are the top kf ones,
+// between cells of thickness dza and dzb: mask3_face x face_combine(dza, dzb)
+// (reference domain.py:93-96, 142-146)
+template <class T>
+__device__ __forceinline__ T face_dz(const KPT<T>& P, int kf, int k, T dza, T dzb) {
+    return (k < kf ? T(1.0) : T(0.0)) * face_combine(P, dza, dzb);
+}
+
+// one thread per column, 32 x 4 columns per CTA
+static inline dim3 col_block() { return dim3(32, 4); }
+template <class T>
+static inline dim3 col_grid(const KPT<T>& P) { return dim3((P.nx + 31) / 32, (P.ny + 3) / 4); }
+
+}  // namespace oc

@@ -35,14 +35,19 @@ class OceanStepper:
     """One model instance on one GPU."""
 
     def __init__(self, params: OceanParams, H, mask, dzr=None, taux_c=None, tauy_c=None,
-                 device: int = 0, slab=None):
+                 device: int = 0, slab=None, precision: str = "fp64"):
         """``slab``: for one y-slab of a larger domain (fb scheme, multi-GPU), the
         tuple (mask_u, mask_v, dx, dy) of the larger domain -- its face masks at
         this handle's rows and its spacing (oc_set_domain_slab); dzr is then
-        required and is the larger domain's level table."""
+        required and is the larger domain's level table.
+
+        ``precision``: "fp64" (bit-identical to the reference) or "mixed" (the 3D
+        state and stencils in FP32; b, the pressure gradient, the EOS, eta and the
+        Helmholtz solve in fp64). States go in and come out as float64 either way."""
         self.lib = _lib.load()
         self.p = params
-        cfg = _lib.config_from_params(params, device)
+        self.precision = precision
+        cfg = _lib.config_from_params(params, device, precision)
         h = C.c_void_p()
         _lib.check(self.lib.oc_create(C.byref(cfg), C.byref(h)), None, "oc_create")
         self.h = h

@@ -61,6 +61,15 @@ enum { OC_TRACERS_BUOYANCY = 0, OC_TRACERS_TS = 1 };
 enum { OC_CLOSURE_NONE = 0, OC_CLOSURE_TKE = 1 };
 enum { OC_MXL_INTEGRAL = 0, OC_MXL_RECURSIVE = 1 };
 enum { OC_BTAVG_NONE = 0, OC_BTAVG_MEAN = 1 };
+/* precision of the step (no reference counterpart: the reference's precision
+ * variants are whole-program fp32 builds, libs/cuda/Makefile:77-113).
+ * OC_PRECISION_FP64: every field fp64, bit-identical to the reference.
+ * OC_PRECISION_MIXED: the 3D state (u, v, T, S, e, K_m, K_h) and the 3D
+ * stencils and column solves in FP32; the buoyancy, its potential, the
+ * pressure-gradient and EOS arithmetic, the surface elevation and every 2D
+ * field (transports, the Helmholtz system and its solve) in fp64. Schemes theta
+ * and fb with TS tracers. */
+enum { OC_PRECISION_FP64 = 0, OC_PRECISION_MIXED = 1 };
 
 /* Every scalar of the step; field meaning and units as the reference namelist keys. */
 typedef struct oc_config {
@@ -81,6 +90,7 @@ typedef struct oc_config {
     int32_t closure, mxl;
     double c_k, c_eps, pr_t, z_0, e_min, l_min, e_bb, n2_min;
     int32_t device;
+    int32_t precision;  /* OC_PRECISION_*; 0 (fp64) when zero-initialised */
 } oc_config;
 
 /* Pointers to one model state. eta [ny][nx]; u, v, b, T, S [nz][ny][nx];

@@ -212,3 +212,32 @@ def test_graph_steps_match_plain_steps(case):
               "barotropic_substeps", "solves"):
         assert sa[k] == sb[k], k
     assert la == lb
+
+
+@pytest.mark.parametrize("n,solver", [(2048, "pcg_jacobi"), (2048, "multigrid"), (2000, "pcg_jacobi")])
+def test_grids_above_one_ctas_fold_match_oracle(n, solver):
+    """Above 16,384 NumPy leaves (about 2.1 M columns) the solver folds the
+    pairwise tree in two levels (block subtrees, then the top over their roots).
+    The sums are NumPy's all the same: iteration counts and solutions equal the
+    oracle's bit for bit, on the grid of the reference's largest published runs
+    (2000 x 2000, docs/32_hardware_ladder.md) and at 2048 x 2048."""
+    from types import SimpleNamespace
+
+    from hydrostatic_ocean_core_benchmark_b200.solvers_var import HelmholtzVar
+    rng = np.random.default_rng(n)
+    dx = 4.0e6 / n
+    mask = np.ones((n, n))
+    mask[n // 4:n // 3, n // 5:n // 2] = 0.0
+    ku = (0.5 + 0.5 * rng.random((n, n))) * mask * np.roll(mask, -1, 1)
+    kv = (0.5 + 0.5 * rng.random((n, n))) * mask * np.roll(mask, -1, 0)
+    rhs = rng.standard_normal((n, n)) * mask
+    coef = 0.5 * dx * dx
+    grid = SimpleNamespace(nx=n, ny=n, dx=dx, dy=dx)
+    solver_gpu = HelmholtzVar(grid, coef, ku, kv, mask, kind=solver, rtol=1e-10)
+    x, rep = solver_gpu.solve(rhs)
+    ref = orc.Helmholtz(n, n, 4.0e6, 4.0e6, coef, ku, kv, mask, solver, 1e-10, 2000)
+    xr, itr, ok = ref.solve(rhs)
+    assert ok and rep.converged
+    assert rep.iterations == itr
+    assert np.array_equal(x, xr)
+    solver_gpu.close()
