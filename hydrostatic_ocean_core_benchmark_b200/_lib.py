@@ -95,6 +95,10 @@ _SIGNATURES = {
     "oc_get_state": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.c_int32]),
     "oc_get_state_async": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.c_int32, C.c_void_p]),
     "oc_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "oc_adjoint_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]),
+    "oc_adjoint_eos": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p]),
     "oc_step_graph": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "oc_get_stats": (C.c_int, [C.c_void_p, C.POINTER(OcStats)]),
     "oc_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),

@@ -25,7 +25,7 @@ EXE = BIN_DIR / "ocean3d5_b200"
 # executables over the C ABI: (main source, binary)
 MAINS = [("ocean3d5_main.cpp", EXE), ("helmholtz_bench_main.cpp", BIN_DIR / "helmholtz_bench_b200"),
          ("eos_bench_main.cpp", BIN_DIR / "eos_bench_b200")]
-SOURCES = ["step_kernels.cu", "step2d_kernels.cu", "helmholtz.cu", "helm_refined.cu", "capi.cu", "mixed.cu",
+SOURCES = ["step_kernels.cu", "step2d_kernels.cu", "helmholtz.cu", "helm_refined.cu", "capi.cu", "mixed.cu", "adjoint.cu",
            "thomas_noalloc.cu", "standalone.cu", "protocol.cpp"]
 # (source, object, flags replacing the fp64 contraction flags): the mixed-precision build of the 3D kernels
 MIXED = [("step_kernels.cu", "step_kernels_mixed.o", ["-DOC_MIXED", "-Xcompiler", "-fPIC"])]

@@ -1515,6 +1515,22 @@ int oc_get_kernel_times(oc_handle* h, oc_kernel_time* out, int32_t capacity, int
 
 const char* oc_last_error(const oc_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
+int oc_adjoint_step(oc_handle* h, const oc_state_view* x0, const oc_state_view* x1, const oc_state_view* x1_b,
+                    oc_state_view* x0_b, double* taux_b, double* tauy_b, void* stream) {
+    if (!h) return OC_ERR_ARG;
+    if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain first");
+    cudaSetDevice(h->cfg.device);
+    return adjoint_step(h, x0, x1, x1_b, x0_b, taux_b, tauy_b, (cudaStream_t)stream);
+}
+
+int oc_adjoint_eos(oc_handle* h, const double* T, const double* S, const double* b_b, double* T_b, double* S_b,
+                   void* stream) {
+    if (!h) return OC_ERR_ARG;
+    if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain first");
+    cudaSetDevice(h->cfg.device);
+    return adjoint_eos(h, T, S, b_b, T_b, S_b, (cudaStream_t)stream);
+}
+
 void oc_destroy(oc_handle* h) {
     if (!h) return;
     cudaSetDevice(h->cfg.device);
@@ -1524,6 +1540,7 @@ void oc_destroy(oc_handle* h) {
     if (h->aux) cudaStreamDestroy(h->aux);
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join) cudaEventDestroy(h->join);
+    adjoint_free(h);
     delete h->solver;
     for (void* p : h->allocs) cudaFree(p);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);

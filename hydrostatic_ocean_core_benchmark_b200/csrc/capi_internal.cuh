@@ -12,6 +12,10 @@
 #include "oc_internal.cuh"
 #include "ocean_b200.h"
 
+namespace oc {
+struct AdjointWork;
+}
+
 using oc::HelmSolver;
 using oc::KP;
 using oc::KPT;
@@ -86,6 +90,8 @@ struct oc_handle {
     float *H32 = nullptr, *mask32 = nullptr, *mask_u32 = nullptr, *mask_v32 = nullptr;
     float *tau_u32 = nullptr, *tau_v32 = nullptr, *ustar2_32 = nullptr, *dzx32 = nullptr;
     double* stage = nullptr;  // (nz+1) n2 doubles: a state field on its way in or out
+    // work of the adjoint step (adjoint.cu), made on its first call
+    oc::AdjointWork* adj = nullptr;
 };
 
 
@@ -100,6 +106,13 @@ int mixed_set_state(oc_handle* h, const oc_state_view* s, int32_t on_device, cud
 int mixed_get_state(oc_handle* h, const oc_state_view* s, int32_t on_device, cudaStream_t st);
 int mixed_reset_mixing(oc_handle* h, cudaStream_t s);
 int step_once_mixed(oc_handle* h, cudaStream_t s);
+
+// adjoint.cu: the adjoint of the fp64 step
+int adjoint_step(oc_handle* h, const oc_state_view* x0, const oc_state_view* x1, const oc_state_view* x1_b,
+                 const oc_state_view* x0_b, double* taux_b, double* tauy_b, cudaStream_t s);
+int adjoint_eos(oc_handle* h, const double* T, const double* S, const double* b_b, double* T_b, double* S_b,
+                cudaStream_t s);
+void adjoint_free(oc_handle* h);
 
 // capi.cu helpers the mixed path shares
 int fail(oc_handle* h, int code, const std::string& msg);

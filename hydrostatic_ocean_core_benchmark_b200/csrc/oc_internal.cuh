@@ -280,23 +280,26 @@ __device__ __forceinline__ T kappa_face_z(const KPT<T>& P, T far_up, T above, T 
 // ---------------------------------------------------------------- EOS
 // polyTEOS10-bsq (Roquet et al. 2015, Table 4) and the S-EOS of their eq. (25):
 // the published coefficients, in the Horner form of reference eos.py:68-111.
-__device__ __forceinline__ double rho_teos10(double CT, double SA, double z) {
-    const double zh = z * 1.0e-4;
-    const double ss = sqrt((SA + 32.0) * (0.875 / 35.16504));
-    const double tt = CT * (1.0 / 40.0);
-    const double r0 = (((((-1.7243708991e-03 * zh + 1.5616995503e-02) * zh + 6.4326772569e-02) * zh
+// N is double for the step; the adjoint evaluates the same expressions on a
+// dual number (value and derivative) to get the exact partial derivatives
+template <class N>
+__device__ __forceinline__ N rho_teos10_n(N CT, N SA, N z) {
+    const N zh = z * 1.0e-4;
+    const N ss = sqrt((SA + 32.0) * (0.875 / 35.16504));
+    const N tt = CT * (1.0 / 40.0);
+    const N r0 = (((((-1.7243708991e-03 * zh + 1.5616995503e-02) * zh + 6.4326772569e-02) * zh
                          + 2.2601900708e-01) * zh + -5.2099962525e+00) * zh + 4.6494977072e+01) * zh;
-    const double rz3 = 3.7969820455e-01 * tt + -1.8507636718e-02 * ss + -2.3342758797e-02;
-    const double rz2 = ((-1.2419983026e+00 * tt + -2.1311365518e-01 * ss + 2.0564311499e+00) * tt
+    const N rz3 = 3.7969820455e-01 * tt + -1.8507636718e-02 * ss + -2.3342758797e-02;
+    const N rz2 = ((-1.2419983026e+00 * tt + -2.1311365518e-01 * ss + 2.0564311499e+00) * tt
                         + (2.5019633803e+00 * ss + -4.9527603989e+00) * ss + 2.0660924175e+00);
-    const double rz1 = ((((5.5927935970e-01 * tt + -5.5077101279e-01 * ss + -2.4649669534e+00) * tt
+    const N rz1 = ((((5.5927935970e-01 * tt + -5.5077101279e-01 * ss + -2.4649669534e+00) * tt
                           + (-1.8795372996e+00 * ss + 3.5063081279e+00) * ss + 6.7080479603e+00) * tt
                          + ((-6.5399043664e-01 * ss + 5.0042598061e+00) * ss + -4.4870114575e+00) * ss
                          + -1.3336301113e+01) * tt
                         + (((6.6051753097e+00 * ss + -3.0938076334e+01) * ss + 5.0774768218e+01) * ss
                            + -4.2549998214e+01) * ss
                         + 1.9681925209e+01);
-    const double rz0 = ((((((-1.9098268277e-01 * tt + 4.5111434961e-01 * ss + 5.4048723791e-01) * tt
+    const N rz0 = ((((((-1.9098268277e-01 * tt + 4.5111434961e-01 * ss + 5.4048723791e-01) * tt
                             + (-5.3563304045e+00 * ss + 1.1311538584e+01) * ss + -8.3627885467e+00) * tt
                            + ((-3.1742946532e+00 * ss + 1.9717078466e+01) * ss + -3.3449108469e+01) * ss
                            + 2.1661789529e+01) * tt
@@ -315,18 +318,26 @@ __device__ __forceinline__ double rho_teos10(double CT, double SA, double z) {
     return ((rz3 * zh + rz2) * zh + rz1) * zh + rz0 + r0;
 }
 
+__device__ __forceinline__ double rho_teos10(double CT, double SA, double z) { return rho_teos10_n<double>(CT, SA, z); }
+
 // density anomaly rho' (eos.py:103-127): linear with the given constants, the
 // simplified EOS, or polyTEOS10-bsq about rho0
-__device__ __forceinline__ double rho_anomaly_of(int eos, double rho0, double alpha_t, double beta_s,
-                                                 double t0, double s0, double T, double S, double z) {
+template <class N>
+__device__ __forceinline__ N rho_anomaly_n(int eos, double rho0, double alpha_t, double beta_s, double t0, double s0,
+                                           N T, N S, N z) {
     if (eos == 0) return rho0 * (-alpha_t * (T - t0) + beta_s * (S - s0));
     if (eos == 1) {
-        const double Ta = T - 10.0, Sa = S - 35.0;
+        const N Ta = T - 10.0, Sa = S - 35.0;
         return (-1.6550e-1 * (1.0 + (0.5 * 5.9520e-2) * Ta + 1.4970e-4 * z) * Ta
                 + 7.6554e-1 * (1.0 - (0.5 * 7.4914e-4) * Sa - 1.1090e-5 * z) * Sa
                 - 2.4341e-3 * Ta * Sa);
     }
-    return rho_teos10(T, S, z) - rho0;
+    return rho_teos10_n<N>(T, S, z) - rho0;
+}
+
+__device__ __forceinline__ double rho_anomaly_of(int eos, double rho0, double alpha_t, double beta_s,
+                                                 double t0, double s0, double T, double S, double z) {
+    return rho_anomaly_n<double>(eos, rho0, alpha_t, beta_s, t0, s0, T, S, z);
 }
 
 // The EOS is evaluated in fp64 on both paths, with the fp64 copies of the

@@ -43,32 +43,6 @@ using ColGeoR = ColGeoT<real>;
 
 // ------------------------------------------------------------------ helpers
 
-// Row k of A = I - thv dt Dz for a column (reference vertical_var.py:35-77).
-__device__ __forceinline__ void implicit_row(const KPR& P, int k, real dzk, real m3k, real m3k1,
-                                             real dzi_k, real dzi_k1, real Kk, real Kk1,
-                                             real thv_dt_drag, real& sub, real& diag,
-                                             real& sup) {
-    const real inv_dz = inv_pos(dzk);
-    const real fac = P.thv_dt * inv_dz;
-    const real at = fac * Kk * inv_pos(dzi_k);
-    const real ab = fac * Kk1 * inv_pos(dzi_k1);
-    sub = -at;
-    sup = -ab;
-    diag = real(1.0) + at + ab;
-    if (k == 0) {
-        diag = real(1.0) + ab;
-        sub = real(0.0);
-    }
-    if (m3k > real(0.0) && m3k1 == real(0.0)) {
-        diag = real(1.0) + at + thv_dt_drag * inv_dz;
-        sup = real(0.0);
-    }
-    if (m3k == real(0.0)) {
-        diag = real(1.0);
-        sub = real(0.0);
-        sup = real(0.0);
-    }
-}
 
 
 __device__ __forceinline__ real m3u_at(const KPR& P, const Nbr& n, int dj, int di, int k) {

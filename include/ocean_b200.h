@@ -339,6 +339,26 @@ int oc_get_field(oc_handle* h, const char* name, double* host_out, int64_t count
  * <out_prefix>_state3d5.bin and <out_prefix>_metrics.json. */
 int oc_run_namelist(const char* nml_path);
 
+/* Adjoint of one fp64 step (no reference counterpart: the reference has no
+ * adjoint). Given the state before the step (x0: eta, u, v, b, T, S), the
+ * state after it (x1: u, v, T, S; the step's output from x0) and the
+ * cotangents of the step's outputs (x1_b: eta, u, v, b, T, S), it writes the
+ * cotangents of the step's inputs into x0_b (eta, u, v, b, T, S; overwritten)
+ * and adds the cotangent of the surface x-stress field at cell centres to
+ * taux_b (and of the y-stress to tauy_b, when not NULL), all [ny][nx] or
+ * [nz][ny][nx] fp64 device arrays. It is the transpose of the step's Jacobian:
+ * the transposed column solves, a second Helmholtz solve with the same
+ * (symmetric) operator, and the advection with the limiter branches the
+ * forward values select. Covered: the theta scheme with TS tracers, the
+ * closure off and pgf keep (OC_ERR_UNSUPPORTED otherwise). Asynchronous on
+ * `stream`; its first call makes its work buffers and solver. */
+int oc_adjoint_step(oc_handle* h, const oc_state_view* x0, const oc_state_view* x1, const oc_state_view* x1_b,
+                    oc_state_view* x0_b, double* taux_b, double* tauy_b, void* stream);
+/* The EOS's part of an initial state whose b is diagnosed from T and S:
+ * T_b += b_b m3 db/dT, S_b += b_b m3 db/dS (device arrays [nz][ny][nx]). */
+int oc_adjoint_eos(oc_handle* h, const double* T, const double* S, const double* b_b, double* T_b, double* S_b,
+                   void* stream);
+
 const char* oc_last_error(const oc_handle* h);
 
 void oc_destroy(oc_handle* h);

@@ -1,0 +1,102 @@
+"""The hand-written adjoint of the step (oc_adjoint_step) on the GPU.
+
+Pins, as the north star of the differentiation form asks: a float64 torch
+restatement of the step (tests/torch_step.py, whose forward matches the
+oracle) differentiated by torch.autograd, and centred finite differences of
+the GPU forward (epsilon = 1e-6, seeded random directions). The objective is
+the volume-weighted mean temperature of the top three levels after the run;
+the inputs are the initial temperature and the surface x-stress field.
+The configuration is the benchmark recipe with the closure off (the adjoint's
+scope): stretched levels, double-gyre wind field, TVD3, polyTEOS10,
+theta = 0.6 + multigrid.
+"""
+
+import numpy as np
+import pytest
+
+from hydrostatic_ocean_core_benchmark_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    import torch
+    assert torch.cuda.is_available()
+    torch.cuda.set_device(0)
+
+
+def _setup(nx, ny, nz, seed, steps, every):
+    import torch
+    from hydrostatic_ocean_core_benchmark_b200.adjoint import OceanRollout
+    s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=seed, closure="none")
+    ro = OceanRollout(s.params, s.H, s.mask, dzr=s.dzr, n_steps=steps, every=every)
+    dev = "cuda:0"
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)  # noqa: E731
+    fixed = {"eta": T(s.eta), "u": T(s.u), "v": T(s.v), "S": T(s.S)}
+    from oracle import ocean_oracle as orc
+    geo = orc.Geometry(s.params, s.H, s.mask, s.dzr)
+    vol = geo.dz3 * geo.dx * geo.dy * geo.mask3
+    w = np.zeros_like(vol)
+    w[:3] = vol[:3] / np.sum(vol[:3])
+    return s, ro, fixed, T(s.T), T(s.taux_c), T(w)
+
+
+def _grad(ro, fixed, T0, taux, w):
+    from hydrostatic_ocean_core_benchmark_b200.adjoint import rollout_apply
+    T0 = T0.clone().requires_grad_(True)
+    tx = taux.clone().requires_grad_(True)
+    out = rollout_apply(ro, T0, tx, fixed)
+    J = (w * out["T"]).sum()
+    J.backward()
+    return T0.grad.detach(), tx.grad.detach(), float(J)
+
+
+def _final_T(ro, fixed, T0, taux):
+    state0 = {"eta": fixed["eta"], "u": fixed["u"], "v": fixed["v"], "T": T0, "S": fixed["S"]}
+    return ro.forward(state0, taux)["T"]
+
+
+def test_adjoint_matches_torch_autograd_of_the_restated_step():
+    import torch
+    from torch_step import TorchStep
+    s, ro, fixed, T0, taux, w = _setup(40, 32, 10, 3, steps=4, every=2)
+    gT, gtau, J = _grad(ro, fixed, T0, taux, w)
+    ts = TorchStep(s.params, s.H, s.mask, s.dzr, device="cuda:0")
+    T0r = T0.clone().requires_grad_(True)
+    txr = taux.clone().requires_grad_(True)
+    st = {"eta": fixed["eta"], "u": fixed["u"], "v": fixed["v"], "S": fixed["S"], "T": T0r,
+          "b": ts.buoyancy(T0r, fixed["S"])}
+    for _ in range(4):
+        st = ts.step(st, txr)
+    Jr = (w * st["T"]).sum()
+    Jr.backward()
+    assert abs(J - float(Jr)) <= 1e-12 * abs(float(Jr))
+    rel_T = float(torch.linalg.vector_norm(gT - T0r.grad) / torch.linalg.vector_norm(T0r.grad))
+    rel_tau = float(torch.linalg.vector_norm(gtau - txr.grad) / torch.linalg.vector_norm(txr.grad))
+    assert rel_T < 1e-9 and rel_tau < 1e-8, (rel_T, rel_tau)
+    ro.close()
+
+
+@pytest.mark.parametrize("nx,ny,nz,steps,every,ndir", [(40, 32, 10, 6, 3, 8), (256, 256, 32, 20, 5, 32)])
+def test_adjoint_agrees_with_centred_finite_differences(nx, ny, nz, steps, every, ndir):
+    """eps = 1e-6 along seeded random directions in (T0, tau_x); the
+    directional derivative from the final states' weighted difference."""
+    import torch
+    s, ro, fixed, T0, taux, w = _setup(nx, ny, nz, 11, steps=steps, every=every)
+    gT, gtau, _ = _grad(ro, fixed, T0, taux, w)
+    gen = torch.Generator(device="cuda:0").manual_seed(2026)
+    eps = 1e-6
+    m3 = (w >= 0).double()
+    worst = 0.0
+    for _ in range(ndir):
+        dT = torch.randn(T0.shape, generator=gen, device="cuda:0", dtype=torch.float64) * (T0 != 0)
+        dtau = 0.1 * torch.randn(taux.shape, generator=gen, device="cuda:0", dtype=torch.float64)
+        Tp = _final_T(ro, fixed, T0 + eps * dT, taux + eps * dtau).clone()
+        Tm = _final_T(ro, fixed, T0 - eps * dT, taux - eps * dtau).clone()
+        fd = float((w * (Tp - Tm)).sum()) / (2 * eps)
+        ad = float((gT * dT).sum() + (gtau * dtau).sum())
+        worst = max(worst, abs(fd - ad) / abs(ad))
+    del m3
+    assert worst < 1e-6, worst
+    ro.close()
