@@ -89,6 +89,8 @@ def test_entry_points_refuse_null_arguments_without_a_gpu():
         "oc_ensemble_create": lambda: lib.oc_ensemble_create(None, 1, None),
         "oc_ensemble_step": lambda: lib.oc_ensemble_step(None, 1, None),
         "oc_ensemble_destroy": lambda: lib.oc_ensemble_destroy(None),
+        "oc_adjoint_step": lambda: lib.oc_adjoint_step(None, buf, buf, buf, buf, buf, None, None),
+        "oc_adjoint_eos": lambda: lib.oc_adjoint_eos(None, buf, buf, buf, buf, buf, None),
     }
     for name, call in calls.items():
         assert call() == ARG, name
