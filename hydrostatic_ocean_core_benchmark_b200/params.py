@@ -205,7 +205,7 @@ def params_from_reference(domain, physics, scheme, dt) -> OceanParams:
 
 
 # ----------------------------------------------------------------------------
-# namelist I/O (reference tools/toml2nml.py:27-34,188-268; config.hpp:62-93)
+# namelist I/O (the format of reference tools/toml2nml.py:27-34,188-268)
 
 _GROUPS = {
     "grid_nml": ("nx", "ny", "nz", "lx", "ly"),
@@ -251,30 +251,96 @@ def write_namelist(path: str | Path, p: OceanParams) -> Path:
 
 
 def parse_namelist_text(text: str) -> dict[str, str]:
-    """key -> raw value, by the reference parser's rules (config.hpp:75-93)."""
-    kv: dict[str, str] = {}
-    for line in text.splitlines():
-        bang = line.find("!")
-        if bang >= 0:
-            line = line[:bang]
-        line = line.strip()
-        if not line or line[0] in "&/":
+    """name -> raw value of a Fortran namelist file as the bundle writer emits it
+    (reference tools/toml2nml.py:27-34, 188-268): ``&group`` opens a group and
+    ``/`` (or ``&end``) closes it; items are ``name = value`` separated by
+    newlines or commas; character values are quoted, a doubled quote standing
+    for itself; ``!`` outside quotes starts a comment; names are
+    case-insensitive. Quoted values come back without their quotes. The same
+    scanner as the compiled protocol's (csrc/protocol.cpp)."""
+    items: dict[str, str] = {}
+    i, n = 0, len(text)
+    in_group = False
+
+    def name_char(ch):
+        return ch.isalnum() or ch in "_%"
+
+    def skip_line():
+        nonlocal i
+        while i < n and text[i] != "\n":
+            i += 1
+
+    while i < n:
+        ch = text[i]
+        if ch == "!":
+            skip_line()
             continue
-        eq = line.find("=")
-        if eq < 0:
+        if not in_group:
+            i += 1
+            if ch in "&$":
+                in_group = True
+                while i < n and name_char(text[i]):
+                    i += 1
             continue
-        kv[line[:eq].strip()] = line[eq + 1:].strip()
-    return kv
+        if ch.isspace() or ch == ",":
+            i += 1
+            continue
+        if ch in "/&$":
+            in_group = False
+            i += 1
+            while i < n and name_char(text[i]):
+                i += 1
+            continue
+        n0 = i
+        while i < n and name_char(text[i]):
+            i += 1
+        name = text[n0:i].lower()
+        while i < n and text[i] in " \t":
+            i += 1
+        if not name or i >= n or text[i] != "=":
+            skip_line()
+            continue
+        i += 1
+        while i < n and text[i] in " \t":
+            i += 1
+        if i < n and text[i] in "'\"":
+            q = text[i]
+            i += 1
+            out = []
+            while i < n:
+                if text[i] == q:
+                    if i + 1 < n and text[i + 1] == q:
+                        out.append(q)
+                        i += 2
+                        continue
+                    i += 1
+                    break
+                out.append(text[i])
+                i += 1
+            items[name] = "".join(out)
+        else:
+            v0 = i
+            while i < n and not text[i].isspace() and text[i] not in ",/!":
+                i += 1
+            items[name] = text[v0:i]
+    return items
 
 
 def _to_double(raw: str) -> float:
-    return float(raw.replace("d", "e").replace("D", "e"))
+    """A Fortran real literal: the exponent letter d/D/q/Q read as e."""
+    out, mantissa = [], False
+    for ch in raw:
+        if mantissa and ch in "dDqQ":
+            ch = "e"
+        if ch.isdigit() or ch == ".":
+            mantissa = True
+        out.append(ch)
+    return float("".join(out))
 
 
-def _unquote(raw: str) -> str:
-    if len(raw) >= 2 and raw[0] in "'\"":
-        return raw[1:-1]
-    return raw
+def _logical(raw: str) -> bool:
+    r = raw[1:] if raw.startswith(".") else raw
+    return r[:1].lower() == "t"
 
 
 def read_namelist(path: str | Path) -> OceanParams:
@@ -293,9 +359,9 @@ def read_namelist(path: str | Path) -> OceanParams:
         elif f.type in ("float", float):
             setattr(p, f.name, _to_double(raw))
         elif f.type in ("bool", bool):
-            setattr(p, f.name, ("t" in raw) or ("T" in raw))
+            setattr(p, f.name, _logical(raw))
         else:
-            setattr(p, f.name, _unquote(raw))
+            setattr(p, f.name, raw)
     return p
 
 
