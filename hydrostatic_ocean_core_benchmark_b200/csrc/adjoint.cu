@@ -29,6 +29,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -964,7 +965,9 @@ static int adjoint_setup(oc_handle* h) {
     a->solver = new HelmSolver();
     const oc_config& c = h->cfg;
     const double coef = c.g * std::pow(c.theta, 2.0) * std::pow(c.dt, 2.0);
-    const int rc = a->solver->init(h->nx, h->ny, c.lx / h->nx, c.ly / h->ny, coef, c.solver, c.rtol, c.max_iter,
+    // its systems solved to a tighter tolerance than the forward's (at most 1e-13)
+    const double rtol = std::min(c.rtol, 1.0e-13);
+    const int rc = a->solver->init(h->nx, h->ny, c.lx / h->nx, c.ly / h->ny, coef, c.solver, rtol, c.max_iter,
                                    h->mask.data(), h->Ku, h->Kv, 1 << 20, h->d_status, h->err);
     if (rc) {
         delete a;

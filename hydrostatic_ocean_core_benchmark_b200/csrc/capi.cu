@@ -389,12 +389,18 @@ int step_once(oc_handle* h, cudaStream_t s) {
             { Prof pr(h, s, "helm_rhs"); launch_helm_rhs(P, eta, h->div_old, h->Ug, h->Vg, h->rhs2, s); }
             int rc = ensure_log(h, h->solves + 1, s);  // graphs reserve the log before recording
             if (rc) return rc;
-            if (h->solve_chain) cudaStreamWaitEvent(s, h->solve_chain, 0);
-            {
-                Prof pr(h, s, "helm_solve");
-                rc = h->solver->solve(h->rhs2, etan, s, h->err);
+            if (h->batch_rec) {
+                // an ensemble recording its batched graph: the solve becomes a pair of
+                // placeholder nodes the batched solve is later wired between
+                rc = batch_defer(h, s, h->rhs2, etan);
+            } else {
+                if (h->solve_chain) cudaStreamWaitEvent(s, h->solve_chain, 0);
+                {
+                    Prof pr(h, s, "helm_solve");
+                    rc = h->solver->solve(h->rhs2, etan, s, h->err);
+                }
+                if (h->solve_chain) cudaEventRecord(h->solve_chain, s);
             }
-            if (h->solve_chain) cudaEventRecord(h->solve_chain, s);
             if (rc) return rc;
             h->solves += 1;
             double* ou = last ? un : h->uit;
@@ -510,6 +516,38 @@ int capture_graph(oc_handle* h) {
     return OC_OK;
 }
 
+}  // namespace oc
+
+namespace oc {
+// the solves of the steps an ensemble records with batched solves: per member,
+// in recording order, the placeholder nodes each solve was replaced by
+struct BatchRecorder {
+    struct Deferred {
+        const double* rhs;
+        double* x;
+        cudaGraphNode_t pre, post;
+    };
+    std::vector<std::vector<Deferred>> per_member;
+    int member = 0;
+};
+
+int batch_defer(oc_handle* h, cudaStream_t s, const double* rhs, double* x) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd);
+    if (e != cudaSuccess || st != cudaStreamCaptureStatusActive)
+        return fail(h, OC_ERR_CUDA, "a deferred solve outside a recording");
+    cudaGraphNode_t pre = nullptr, post = nullptr;
+    e = cudaGraphAddEmptyNode(&pre, g, deps, nd);
+    if (e == cudaSuccess) e = cudaGraphAddEmptyNode(&post, g, &pre, 1);
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &post, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return cuda_fail(h, e, "deferred solve");
+    BatchRecorder* r = h->batch_rec;
+    r->per_member[r->member].push_back({rhs, x, pre, post});
+    return OC_OK;
+}
 }  // namespace oc
 
 extern "C" {
@@ -1149,7 +1187,12 @@ struct oc_ensemble {
     std::vector<oc_handle::Counters> delta;     // each member's counter increments per replay
     int device = 0;
     std::string err;
+    // one cooperative launch per solve of the recorded steps, every member's system
+    // at once, when all members run the theta scheme with the same Picard count
+    bool batched = false;
+    std::vector<oc::HelmBatch> plans;
     ~oc_ensemble() {
+        for (auto& b : plans) oc::helm_batch_free(b);
         if (exec) cudaGraphExecDestroy(exec);
         for (auto st : streams) cudaStreamDestroy(st);
         for (auto ev : joins) cudaEventDestroy(ev);
@@ -1195,8 +1238,43 @@ int ensemble_record(oc_ensemble* e) {
         before[m] = counters_of(h);
         cur[m] = h->cur;
     }
-    cudaGraph_t g = nullptr;
+    // batched solves: the members' systems and solution buffers of each solve of
+    // the two recorded steps are known before recording (rhs2; eta of the other
+    // buffer in the first step, of the current one in the second), so the plans
+    // (device parameter arrays, CTA shares) are made here, outside the capture
+    for (auto& b : e->plans) helm_batch_free(b);
+    e->plans.clear();
+    bool batched = n > 0;
+    for (size_t m = 0; m < n && batched; ++m) {
+        const oc_handle* h = e->members[m];
+        batched = h->solver && h->cfg.scheme == OC_SCHEME_THETA && h->cfg.n_picard == e->members[0]->cfg.n_picard;
+    }
     std::string why;
+    if (batched) {
+        const int np = e->members[0]->cfg.n_picard;
+        std::vector<HelmSolver*> sv(n);
+        std::vector<const double*> rh(n);
+        std::vector<double*> xs(n);
+        for (int q = 0; q < 2 * np && batched; ++q) {
+            for (size_t m = 0; m < n; ++m) {
+                oc_handle* h = e->members[m];
+                sv[m] = h->solver;
+                rh[m] = h->rhs2;
+                xs[m] = h->ETA[q < np ? 1 - h->cur : h->cur];
+            }
+            e->plans.emplace_back();
+            std::string perr;
+            if (helm_batch_plan(sv.data(), rh.data(), xs.data(), (int)n, e->plans.back(), perr) != OC_OK) {
+                batched = false;  // e.g. more members than co-resident CTAs: chained solves instead
+                for (auto& b : e->plans) helm_batch_free(b);
+                e->plans.clear();
+            }
+        }
+    }
+    e->batched = batched;
+    BatchRecorder rec;
+    rec.per_member.resize(n);
+    cudaGraph_t g = nullptr;
     cudaError_t ce = cudaStreamBeginCapture(e->capture, cudaStreamCaptureModeThreadLocal);
     int rc = ce == cudaSuccess ? OC_OK : OC_ERR_CUDA;
     if (rc) why = std::string("begin capture: ") + cudaGetErrorString(ce);
@@ -1209,18 +1287,71 @@ int ensemble_record(oc_ensemble* e) {
                 oc_handle* h = e->members[m];
                 const bool prof = h->profiling;
                 h->profiling = false;
-                h->solve_chain = e->chain;
+                h->solve_chain = batched ? nullptr : e->chain;
+                h->batch_rec = batched ? &rec : nullptr;
+                rec.member = (int)m;
                 rc = step_once(h, e->streams[m]);
+                h->batch_rec = nullptr;
                 h->solve_chain = nullptr;
                 h->profiling = prof;
                 if (rc) why = "member " + std::to_string(m) + ": " + h->err;
             }
+        // the batched solves: solve q waits for every member's placeholder before it
+        std::vector<cudaGraphNode_t> solve_nodes;
+        if (batched && rc == OC_OK) {
+            for (size_t q = 0; q < e->plans.size() && rc == OC_OK; ++q) {
+                std::vector<cudaGraphNode_t> pre(n);
+                for (size_t m = 0; m < n && rc == OC_OK; ++m) {
+                    if (rec.per_member[m].size() != e->plans.size() || rec.per_member[m][q].rhs != e->members[m]->rhs2 ||
+                        rec.per_member[m][q].x != e->members[m]->ETA[q < e->plans.size() / 2 ? 1 - cur[m] : cur[m]]) {
+                        rc = OC_ERR_STATE;
+                        why = "member " + std::to_string(m) + ": its solves differ from the batched plan";
+                    }
+                    pre[m] = rc == OC_OK ? rec.per_member[m][q].pre : nullptr;
+                }
+                if (rc) break;
+                ce = cudaStreamUpdateCaptureDependencies(e->capture, pre.data(), n, cudaStreamSetCaptureDependencies);
+                if (ce == cudaSuccess) {
+                    std::string lerr;
+                    if (helm_batch_launch(e->plans[q], e->capture, lerr) != OC_OK) {
+                        rc = OC_ERR_CUDA;
+                        why = lerr;
+                    }
+                } else {
+                    rc = OC_ERR_CUDA;
+                    why = std::string("batched solve dependencies: ") + cudaGetErrorString(ce);
+                }
+                if (rc == OC_OK) {
+                    cudaStreamCaptureStatus cs;
+                    const cudaGraphNode_t* d = nullptr;
+                    size_t nd = 0;
+                    ce = cudaStreamGetCaptureInfo(e->capture, &cs, nullptr, nullptr, &d, &nd);
+                    if (ce != cudaSuccess || nd != 1) {
+                        rc = OC_ERR_CUDA;
+                        why = "batched solve node not found in the recording";
+                    } else {
+                        solve_nodes.push_back(d[0]);
+                    }
+                }
+            }
+        }
         for (size_t m = 0; m < n; ++m) {
             cudaEventRecord(e->joins[m], e->streams[m]);
             cudaStreamWaitEvent(e->capture, e->joins[m], 0);
         }
+        ce = cudaStreamEndCapture(e->capture, &g);
+        // each member's work after solve q waits for the batched solve q
+        for (size_t q = 0; q < solve_nodes.size() && rc == OC_OK && ce == cudaSuccess; ++q)
+            for (size_t m = 0; m < n && rc == OC_OK; ++m) {
+                const cudaError_t ae = cudaGraphAddDependencies(g, &solve_nodes[q], &rec.per_member[m][q].post, 1);
+                if (ae != cudaSuccess) {
+                    rc = OC_ERR_CUDA;
+                    why = std::string("batched solve edges: ") + cudaGetErrorString(ae);
+                }
+            }
+    } else {
+        ce = cudaStreamEndCapture(e->capture, &g);
     }
-    ce = cudaStreamEndCapture(e->capture, &g);
     if (rc == OC_OK && ce != cudaSuccess) {
         rc = OC_ERR_CUDA;
         why = std::string("end capture: ") + cudaGetErrorString(ce);

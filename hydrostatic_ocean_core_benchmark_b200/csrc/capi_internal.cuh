@@ -14,6 +14,7 @@
 
 namespace oc {
 struct AdjointWork;
+struct BatchRecorder;
 }
 
 using oc::HelmSolver;
@@ -92,6 +93,8 @@ struct oc_handle {
     double* stage = nullptr;  // (nz+1) n2 doubles: a state field on its way in or out
     // work of the adjoint step (adjoint.cu), made on its first call
     oc::AdjointWork* adj = nullptr;
+    // while an ensemble records with batched solves: where the step's solves are deferred to
+    oc::BatchRecorder* batch_rec = nullptr;
 };
 
 
@@ -113,6 +116,9 @@ int adjoint_step(oc_handle* h, const oc_state_view* x0, const oc_state_view* x1,
 int adjoint_eos(oc_handle* h, const double* T, const double* S, const double* b_b, double* T_b, double* S_b,
                 cudaStream_t s);
 void adjoint_free(oc_handle* h);
+
+// capi.cu: a solve deferred to the ensemble's batched solve while it records
+int batch_defer(oc_handle* h, cudaStream_t s, const double* rhs, double* x);
 
 // capi.cu helpers the mixed path shares
 int fail(oc_handle* h, int code, const std::string& msg);

@@ -32,17 +32,18 @@ static __device__ __forceinline__ void grid_sync_begin(const int* status) {
     }
 }
 
-// thread 0's arrival and wait, out of line: the solve calls the barrier from many places
-static __device__ __noinline__ void grid_arrive_wait(unsigned long long* cnt, int* status) {
+// thread 0's arrival and wait, out of line: the solve calls the barrier from many places.
+// ncta: the CTAs taking part (the launch's grid, or one member's share of it)
+static __device__ __noinline__ void grid_arrive_wait(unsigned long long* cnt, int* status, unsigned ncta) {
     unsigned long long target = s_gbar.next;
     if (target == 0) {
         unsigned long long old;
         asm volatile("atom.add.release.gpu.u64 %0, [%1], 1;" : "=l"(old) : "l"(cnt) : "memory");
-        target = old - old % gridDim.x + gridDim.x;
+        target = old - old % ncta + ncta;
     } else {
         asm volatile("red.add.release.gpu.u64 [%0], 1;" ::"l"(cnt) : "memory");
     }
-    s_gbar.next = target + gridDim.x;
+    s_gbar.next = target + ncta;
     const long long t0 = clock64();
     for (unsigned spin = 1;; ++spin) {
         unsigned long long v;
@@ -62,11 +63,15 @@ static __device__ __noinline__ void grid_arrive_wait(unsigned long long* cnt, in
     }
 }
 
-static __device__ __forceinline__ bool grid_sync(unsigned long long* cnt, int* status) {
+static __device__ __forceinline__ bool grid_sync(unsigned long long* cnt, int* status, unsigned ncta) {
     __syncthreads();
-    if (threadIdx.x == 0 && s_gbar.ok) grid_arrive_wait(cnt, status);
+    if (threadIdx.x == 0 && s_gbar.ok) grid_arrive_wait(cnt, status, ncta);
     __syncthreads();
     return s_gbar.ok != 0;
+}
+
+static __device__ __forceinline__ bool grid_sync(unsigned long long* cnt, int* status) {
+    return grid_sync(cnt, status, gridDim.x);
 }
 
 }  // namespace oc

@@ -49,11 +49,23 @@ using TileWide = TileShape<128, 16>;  // level 0 of large grids: one tile per CT
 // per-level tile shape codes (HLevel::shape)
 enum { SHAPE_32 = 0, SHAPE_3216 = 1, SHAPE_16 = 2, SHAPE_8 = 3, SHAPE_WIDE = 4 };
 
+// ------------------------------------------------------------------ the solve's CTAs
+// A solve runs on the CTAs of its launch, or, in a batched launch that solves
+// several systems at once, on one system's share of them: s_grid.cta is the
+// CTA's index among the solve's CTAs and s_grid.ncta their number. Every
+// work-distribution loop and the barrier use these instead of the launch's grid.
+struct SolveGrid {
+    int cta, ncta;
+};
+static __shared__ SolveGrid s_grid;
+
 // ------------------------------------------------------------------ barrier
 // the bounded grid barrier of grid_barrier.cuh on the solver's counter and status
 __device__ __forceinline__ void grid_sync_begin(const HelmParams& H) { grid_sync_begin(H.status); }
 
-__device__ __forceinline__ bool grid_sync(const HelmParams& H) { return grid_sync(H.bar_count, H.status); }
+__device__ __forceinline__ bool grid_sync(const HelmParams& H) {
+    return grid_sync(H.bar_count, H.status, (unsigned)s_grid.ncta);
+}
 
 // ------------------------------------------------------------------ level operators
 struct Cell {
@@ -109,8 +121,8 @@ struct Team {
 
 __device__ __forceinline__ Team grid_team() {
     Team t;
-    t.first = blockIdx.x * blockDim.x + threadIdx.x;
-    t.stride = gridDim.x * blockDim.x;
+    t.first = s_grid.cta * blockDim.x + threadIdx.x;
+    t.stride = s_grid.ncta * blockDim.x;
     return t;
 }
 
@@ -164,8 +176,8 @@ __device__ __forceinline__ double leaf_sum_warp(const double* va, int len) {
 template <class F>
 __device__ void leaf_phase(const HelmParams& H, F f, double* outA, double* outB) {
     const int lane = threadIdx.x & 31;
-    const int nwarps = gridDim.x * (blockDim.x >> 5);
-    const int my = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;  // leaf L runs on CTA L mod grid
+    const int nwarps = s_grid.ncta * (blockDim.x >> 5);
+    const int my = (threadIdx.x >> 5) * s_grid.ncta + s_grid.cta;  // leaf L runs on CTA L mod grid
     for (int L = my; L < H.n_leaves; L += nwarps) {
         const int s = H.leaf_start[L];
         const int len = H.leaf_start[L + 1] - s;
@@ -220,7 +232,7 @@ __device__ double tree_fold(const HelmParams& H, const FoldPlan& F, const double
 // leaf buffer has its own root buffer, so folds that follow one another without
 // a barrier never overwrite roots another CTA is still reading.
 __device__ double fold_blocks(const HelmParams& H, const double* leaf, double* broot, double* sm, bool& ok) {
-    for (int j = blockIdx.x; j < H.n_blocks; j += gridDim.x) {
+    for (int j = s_grid.cta; j < H.n_blocks; j += s_grid.ncta) {
         const int4 B = H.blocks[j];  // first leaf, leaves, offset of its height starts, heights
         for (int t = threadIdx.x; t < B.y; t += blockDim.x) sm[t] = __ldcg(leaf + B.x + t);
         __syncthreads();
@@ -374,7 +386,7 @@ __device__ void persist_level0(const HelmParams& H, double* persist) {
     using S = TileWide;
     const HLevel& L = H.lv[0];
     const int tx = (L.nx + S::TX - 1) / S::TX;
-    const int tile = blockIdx.x;
+    const int tile = s_grid.cta;
     if (tile >= tx * ((L.ny + S::TY - 1) / S::TY)) return;
     const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
     for (int r = threadIdx.x; r < S::RN; r += blockDim.x) {
@@ -470,7 +482,7 @@ __device__ void mg_down(const HelmParams& H, int l, const double* xin, double* x
     const int tx = (L.nx + S::TX - 1) / S::TX, ty = (L.ny + S::TY - 1) / S::TY;
     const bool keep = persist != nullptr;
     TileRefs t = keep ? tile_refs_persist<S>(persist, smem) : tile_refs<S>(smem);
-    for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
+    for (int tile = s_grid.cta; tile < tx * ty; tile += s_grid.ncta) {
         const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
         tile_load<S>(L, i0, j0, xin, nullptr, t, !keep);
         tile_four_half_sweeps<S>(L, i0, j0, t, 0);
@@ -521,7 +533,7 @@ __device__ void mg_up(const HelmParams& H, int l, const double* xin, const HLeve
     const int tx = (L.nx + S::TX - 1) / S::TX, ty = (L.ny + S::TY - 1) / S::TY;
     const bool keep = persist != nullptr;
     TileRefs t = keep ? tile_refs_persist<S>(persist, smem) : tile_refs<S>(smem);
-    for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
+    for (int tile = s_grid.cta; tile < tx * ty; tile += s_grid.ncta) {
         const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
         tile_load<S>(L, i0, j0, xin, &C, t, !keep);
         tile_four_half_sweeps<S>(L, i0, j0, t, 1);
@@ -700,7 +712,7 @@ __device__ void mg_smooth(const HelmParams& H, int l, const double* xin, double*
     const HLevel& L = H.lv[l];
     const int tx = (L.nx + Tile32::TX - 1) / Tile32::TX, ty = (L.ny + Tile32::TY - 1) / Tile32::TY;
     TileRefs t = tile_refs<Tile32>(smem);
-    for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
+    for (int tile = s_grid.cta; tile < tx * ty; tile += s_grid.ncta) {
         const int i0 = (tile % tx) * Tile32::TX, j0 = (tile / tx) * Tile32::TY;
         tile_load<Tile32>(L, i0, j0, xin, nullptr, t);
         tile_four_half_sweeps<Tile32>(L, i0, j0, t, reverse ? 1 : 0);
@@ -717,7 +729,7 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, d
     const int cf = H.coarse_from, nl = H.n_levels;
     double* x0b = (x0 == H.lv[0].x) ? H.lv[0].x2 : H.lv[0].x;
     if (cf == 0) {
-        if (blockIdx.x == 0) mg_coarse(H, smem, x0, x0b);
+        if (s_grid.cta == 0) mg_coarse(H, smem, x0, x0b);
         ok = grid_sync(H);
         return x0b;
     }
@@ -736,7 +748,7 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, d
     }
     if (!ok) return x0;
     if (cf < nl) {
-        if (blockIdx.x == 0) mg_coarse(H, smem, nullptr, H.lv[cf].x2);
+        if (s_grid.cta == 0) mg_coarse(H, smem, nullptr, H.lv[cf].x2);
         ok = grid_sync(H);
     } else {
         const int l = nl - 1;
@@ -770,8 +782,9 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, d
 }
 
 // ------------------------------------------------------------------ the solve kernel
-__global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
-    extern __shared__ double smem_all[];
+// A whole solve on the CTAs s_grid names (set by the kernel, followed by a CTA
+// barrier, before the call).
+__device__ __forceinline__ void helm_solve_body(const HelmParams& H, double* smem_all) {
     // with H.persist0 the first 4 RN doubles hold level 0's coefficient tile for the
     // whole solve; every other use of shared memory works above them
     double* persist = H.persist0 ? smem_all : nullptr;
@@ -950,7 +963,7 @@ __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
         }
     }
 done:
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (s_grid.cta == 0 && threadIdx.x == 0) {
         const int idx = *H.log_count;
         if (idx < H.log_cap) {
             H.log_iters[idx] = ok ? iters : -1;
@@ -958,6 +971,36 @@ done:
         }
         *H.log_count = idx + 1;
     }
+}
+
+__global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
+    extern __shared__ double smem_all[];
+    if (threadIdx.x == 0) s_grid = SolveGrid{(int)blockIdx.x, (int)gridDim.x};
+    __syncthreads();
+    helm_solve_body(H, smem_all);
+}
+
+// Several systems in one cooperative launch: system m runs on CTAs
+// [cta_start[m], cta_start[m + 1]) with its own parameters (copied into shared
+// memory), its own barrier counter, status word and solve log; the systems
+// never wait on one another.
+__global__ void __launch_bounds__(512) k_helm_solve_batched(const HelmParams* __restrict__ systems,
+                                                            const int* __restrict__ cta_start, int n) {
+    extern __shared__ double smem_all[];
+    __shared__ HelmParams sH;
+    __shared__ int s_m;
+    if (threadIdx.x == 0) {
+        int m = 0;
+        while (m + 1 < n && (int)blockIdx.x >= cta_start[m + 1]) ++m;
+        s_m = m;
+        s_grid = SolveGrid{(int)blockIdx.x - cta_start[m], cta_start[m + 1] - cta_start[m]};
+    }
+    __syncthreads();
+    const int* src = reinterpret_cast<const int*>(systems + s_m);
+    int* dst = reinterpret_cast<int*>(&sH);
+    for (int t = threadIdx.x; t < (int)(sizeof(HelmParams) / sizeof(int)); t += blockDim.x) dst[t] = src[t];
+    __syncthreads();
+    helm_solve_body(sH, smem_all);
 }
 
 // ------------------------------------------------------------------ level rebuild
@@ -1295,6 +1338,15 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     }
     const size_t coarse_work = 6 * coarse_cells + (H.coarse_from < H.n_levels ? (size_t)H.lv[H.coarse_from].n : 0);
     const size_t mg_work = (kind == HK_MULTIGRID) ? std::max<size_t>(tile_work, coarse_work) : 0;
+    // in a batched launch a system has fewer CTAs than tiles: no persistent level-0
+    // tile (its six arrays are loaded per tile instead) and no shared copy of the plan
+    size_t tile_work_b = 0;
+    if (kind == HK_MULTIGRID) {
+        for (int l = 0; l < n_grid; ++l) tile_work_b = std::max<size_t>(tile_work_b, 6 * (size_t)rn_of(H.lv[l].shape));
+        if (H.coarse_from >= H.n_levels) tile_work_b = std::max<size_t>(tile_work_b, 6 * (size_t)Tile32::RN);
+    }
+    const size_t mg_work_b = (kind == HK_MULTIGRID) ? std::max<size_t>(tile_work_b, coarse_work) : 0;
+    smem_batched_ = sizeof(double) * std::max<size_t>(fold_doubles, mg_work_b);
     // the tree fold and the V-cycle never run at the same time: one region serves both
     smem_ = sizeof(double) * ((H.persist0 ? 4 * (size_t)TileWide::RN : 0) + std::max<size_t>(fold_doubles, mg_work));
     int smem_optin = 0;
@@ -1369,6 +1421,122 @@ void HelmSolver::rebuild(cudaStream_t s) {
         const HLevel& F = hp_.lv[l > 0 ? l - 1 : 0];
         k_helm_level<<<(L.n + 255) / 256, 256, 0, s>>>(F, L, l > 0 ? 1 : 0);
     }
+}
+
+HelmParams HelmSolver::batched_params(const double* rhs, double* x) const {
+    HelmParams H = hp_;
+    H.rhs = rhs;
+    H.lv[0].x = x;
+    H.persist0 = 0;
+    H.ops_smem = 0;
+    return H;
+}
+
+int helm_batch_plan(HelmSolver* const* solvers, const double* const* rhs, double* const* x, int n, HelmBatch& b,
+                    std::string& err) {
+    helm_batch_free(b);
+    if (n < 1) {
+        err = "a batched solve needs at least one system";
+        return OC_ERR_ARG;
+    }
+    size_t smem = 0;
+    double total = 0.0;
+    std::vector<HelmParams> hp(n);
+    for (int m = 0; m < n; ++m) {
+        hp[m] = solvers[m]->batched_params(rhs[m], x[m]);
+        smem = std::max(smem, solvers[m]->batched_smem());
+        total += solvers[m]->work_weight();
+    }
+    int dev = 0, sms = 0, smem_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k_helm_solve_batched);
+    if (smem + fa.sharedSizeBytes > (size_t)smem_optin) {
+        err = "batched Helmholtz solve: a system needs more shared memory than a CTA has";
+        return OC_ERR_UNSUPPORTED;
+    }
+    if (smem > 48 * 1024) {
+        static std::mutex mu;
+        static std::map<int, size_t> allowance;
+        std::lock_guard<std::mutex> lock(mu);
+        size_t& a = allowance[dev];
+        if (smem > a) {
+            cudaFuncSetAttribute(k_helm_solve_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            a = smem;
+        }
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_helm_solve_batched, 512, smem);
+    if (per_sm < 1) {
+        err = "batched Helmholtz solve kernel cannot be resident";
+        return OC_ERR_CUDA;
+    }
+    const int grid = sms * std::min(per_sm, 2);
+    if (n > grid) {
+        err = "more systems than co-resident CTAs";
+        return OC_ERR_UNSUPPORTED;
+    }
+    // CTAs in proportion to the cells, at least one each, the remainder to the largest shares
+    std::vector<int> share(n, 1);
+    int left = grid - n;
+    std::vector<double> want(n);
+    for (int m = 0; m < n; ++m) want[m] = (grid - n) * solvers[m]->work_weight() / total;
+    for (int m = 0; m < n; ++m) {
+        const int add = std::min(left, (int)want[m]);
+        share[m] += add;
+        left -= add;
+        want[m] -= add;
+    }
+    while (left > 0) {
+        int best = 0;
+        for (int m = 1; m < n; ++m)
+            if (want[m] > want[best]) best = m;
+        share[best] += 1;
+        want[best] -= 1.0;
+        --left;
+    }
+    b.cta_start.assign(n + 1, 0);
+    for (int m = 0; m < n; ++m) b.cta_start[m + 1] = b.cta_start[m] + share[m];
+    if (cudaMalloc(&b.d_params, sizeof(HelmParams) * n) != cudaSuccess ||
+        cudaMalloc(&b.d_cta_start, sizeof(int) * (n + 1)) != cudaSuccess) {
+        helm_batch_free(b);
+        err = "cudaMalloc failed (batched solve plan)";
+        return OC_ERR_CUDA;
+    }
+    cudaMemcpy(b.d_params, hp.data(), sizeof(HelmParams) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(b.d_cta_start, b.cta_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice);
+    b.n = n;
+    b.grid = b.cta_start[n];
+    b.smem = smem;
+    return OC_OK;
+}
+
+int helm_batch_launch(const HelmBatch& b, cudaStream_t s, std::string& err) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(b.grid);
+    cfg.blockDim = dim3(512);
+    cfg.dynamicSmemBytes = b.smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_helm_solve_batched, (const HelmParams*)b.d_params,
+                                             (const int*)b.d_cta_start, b.n);
+    if (e != cudaSuccess) {
+        err = std::string("batched Helmholtz solve launch: ") + cudaGetErrorString(e);
+        return OC_ERR_CUDA;
+    }
+    return OC_OK;
+}
+
+void helm_batch_free(HelmBatch& b) {
+    if (b.d_params) cudaFree(b.d_params);
+    if (b.d_cta_start) cudaFree(b.d_cta_start);
+    b = HelmBatch{};
 }
 
 int HelmSolver::solve(const double* rhs, double* x, cudaStream_t s, std::string& err) {

@@ -81,15 +81,36 @@ class HelmSolver {
     int* d_log_conv() const { return hp_.log_conv; }
     int* d_log_count() const { return hp_.log_count; }
     int grow_log(int cap, cudaStream_t s, std::string& err);
+    // this solver's system for a batched launch (helm_batch_*): the parameters
+    // of x = A^-1 rhs without the one-CTA-per-tile assumptions, and the dynamic
+    // shared memory it needs
+    HelmParams batched_params(const double* rhs, double* x) const;
+    size_t batched_smem() const { return smem_batched_; }
+    double work_weight() const { return (double)hp_.lv[0].n; }
     size_t bytes() const { return bytes_; }
 
    private:
     HelmParams hp_{};
     std::vector<void*> allocs_;
     int grid_ = 0, block_ = 512;
-    size_t smem_ = 0;
+    size_t smem_ = 0, smem_batched_ = 0;
     size_t bytes_ = 0;
     void* dalloc(size_t nbytes);
 };
+
+// Several solvers' systems solved by one cooperative launch (k_helm_solve_batched):
+// system m on its own share of the CTAs, proportional to its cells. The plan's
+// device arrays hold the systems' parameters, so a recorded launch replays them.
+struct HelmBatch {
+    int n = 0, grid = 0;
+    size_t smem = 0;
+    HelmParams* d_params = nullptr;
+    int* d_cta_start = nullptr;
+    std::vector<int> cta_start;
+};
+int helm_batch_plan(HelmSolver* const* solvers, const double* const* rhs, double* const* x, int n, HelmBatch& b,
+                    std::string& err);
+int helm_batch_launch(const HelmBatch& b, cudaStream_t s, std::string& err);
+void helm_batch_free(HelmBatch& b);
 
 }  // namespace oc

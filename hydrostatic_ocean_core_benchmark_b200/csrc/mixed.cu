@@ -331,12 +331,18 @@ int step_once_mixed(oc_handle* h, cudaStream_t s) {
             { Prof pr(h, s, "helm_rhs"); launch_helm_rhs(P, eta, h->div_old, h->Ug, h->Vg, h->rhs2, s); }
             int rc = ensure_log(h, h->solves + 1, s);
             if (rc) return rc;
-            if (h->solve_chain) cudaStreamWaitEvent(s, h->solve_chain, 0);
-            {
-                Prof pr(h, s, "helm_solve");
-                rc = h->solver->solve(h->rhs2, etan, s, h->err);
+            if (h->batch_rec) {
+                // an ensemble recording its batched graph: the solve becomes a pair of
+                // placeholder nodes the batched solve is later wired between
+                rc = batch_defer(h, s, h->rhs2, etan);
+            } else {
+                if (h->solve_chain) cudaStreamWaitEvent(s, h->solve_chain, 0);
+                {
+                    Prof pr(h, s, "helm_solve");
+                    rc = h->solver->solve(h->rhs2, etan, s, h->err);
+                }
+                if (h->solve_chain) cudaEventRecord(h->solve_chain, s);
             }
-            if (h->solve_chain) cudaEventRecord(h->solve_chain, s);
             if (rc) return rc;
             h->solves += 1;
             float* ou = last ? un : h->uit32;

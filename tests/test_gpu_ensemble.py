@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 FIELDS = ("eta", "u", "v", "b", "T", "S", "e", "km", "kh")
 # nx, ny, nz, seed: the solvers of the two larger grids need different amounts of
 # shared memory, created largest first
-MEMBERS = [(512, 512, 6, 3), (256, 256, 6, 4), (40, 36, 12, 5)]
+MEMBERS = [(512, 512, 6, 3), (256, 256, 6, 4), (40, 36, 12, 5), (136, 200, 8, 6)]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -26,10 +26,10 @@ def _cuda():
     torch.cuda.set_device(0)
 
 
-def _member(nx, ny, nz, seed):
+def _member(nx, ny, nz, seed, precision="fp64"):
     from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
     s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=seed)
-    st = OceanStepper(s.params, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    st = OceanStepper(s.params, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c, precision=precision)
     st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
     return st
 
@@ -76,6 +76,25 @@ def test_ensemble_equals_members_stepped_alone():
     # the two smaller members directly against the oracle, field by field
     for m in (1, 2):
         _equal_to_oracle(MEMBERS[m], together[m], 9)
+    ens.close()
+    for st in together + alone:
+        st.close()
+
+
+def test_mixed_precision_ensemble_equals_members_stepped_alone():
+    """Members of the mixed-precision step in one ensemble (batched solves) give
+    the bits of the same members stepped alone."""
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanEnsemble
+    grids = [(96, 64, 8, 21), (136, 120, 6, 22), (48, 40, 10, 23)]
+    together = [_member(*m, precision="mixed") for m in grids]
+    alone = [_member(*m, precision="mixed") for m in grids]
+    ens = OceanEnsemble(together)
+    ens.step(6)
+    for st in alone:
+        st.step(6)
+    for m, (a, b) in enumerate(zip(together, alone)):
+        _same(a, b, f"mixed member {grids[m][:3]}")
+        assert a.solve_log() == b.solve_log()
     ens.close()
     for st in together + alone:
         st.close()
