@@ -92,6 +92,8 @@ _SIGNATURES = {
     "oc_set_state": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.c_int32]),
     "oc_set_state_async": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.c_int32, C.c_void_p]),
     "oc_reset_mixing": (C.c_int, [C.c_void_p]),
+    "oc_bind_state": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.POINTER(OcStateView)]),
+    "oc_state_parity": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "oc_get_state": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.c_int32]),
     "oc_get_state_async": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.c_int32, C.c_void_p]),
     "oc_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),

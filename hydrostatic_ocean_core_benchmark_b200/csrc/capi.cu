@@ -703,6 +703,7 @@ static int set_domain_impl(oc_handle* h, const double* Hh, const double* maskh, 
     double* d_kface = dalloc(h, n2);
     const bool ts = h->cfg.tracers == OC_TRACERS_TS;
     const bool f64 = !h->mixed;  // the mixed path keeps its 3D fields in FP32 buffers (mixed.cu)
+    h->bound = false;            // a new domain drops caller-owned state buffers
     for (int t = 0; t < 2; ++t) {
         h->U[t] = f64 ? dalloc(h, n3) : nullptr;
         h->V[t] = f64 ? dalloc(h, n3) : nullptr;
@@ -768,7 +769,10 @@ static int set_domain_impl(oc_handle* h, const double* Hh, const double* maskh, 
     if (h->cfg.scheme == OC_SCHEME_THETA) {
         h->solver = new HelmSolver();
         const double coef = h->cfg.g * std::pow(h->cfg.theta, 2.0) * std::pow(h->cfg.dt, 2.0);
-        rc = h->solver->init(nx, ny, h->cfg.lx / nx, h->cfg.ly / ny, coef, h->cfg.solver, h->cfg.rtol,
+        // the mixed-precision step needs no reference iteration counts: where the
+        // configuration names the stationary multigrid it solves by MG-preconditioned CG
+        const int kind = (h->mixed && h->cfg.solver == OC_SOLVER_MULTIGRID) ? OC_SOLVER_PCG_MG : h->cfg.solver;
+        rc = h->solver->init(nx, ny, h->cfg.lx / nx, h->cfg.ly / ny, coef, kind, h->cfg.rtol,
                              h->cfg.max_iter, h->mask.data(), h->Ku, h->Kv, 4096, h->d_status, h->err);
         if (rc) return rc;
     }
@@ -1046,6 +1050,105 @@ int oc_set_state(oc_handle* h, const oc_state_view* s, int32_t on_device) {
 
 int oc_set_state_async(oc_handle* h, const oc_state_view* s, int32_t on_device, void* stream) {
     return set_state_on(h, s, on_device, (cudaStream_t)stream);
+}
+
+// the handle's state pointers in one array: ETA, U, V, B, Tt, Ss of parity 0,
+// the same of parity 1, then e, km, kh
+static void state_slots(oc_handle* h, double** slot[15]) {
+    double** per[6] = {h->ETA, h->U, h->V, h->B, h->Tt, h->Ss};
+    for (int p = 0; p < 2; ++p)
+        for (int f = 0; f < 6; ++f) slot[6 * p + f] = &per[f][p];
+    slot[12] = &h->e;
+    slot[13] = &h->km;
+    slot[14] = &h->kh;
+}
+
+int oc_bind_state(oc_handle* h, const oc_state_view* a, const oc_state_view* b) {
+    if (!h) return OC_ERR_ARG;
+    if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain before binding a state");
+    if (h->mixed)
+        return fail(h, OC_ERR_UNSUPPORTED, "the mixed-precision step keeps FP32 state fields; bind needs fp64 ones");
+    if ((a == nullptr) != (b == nullptr)) return fail(h, OC_ERR_ARG, "give both buffer sets, or neither");
+    cudaSetDevice(h->cfg.device);
+    // the step may still be writing the buffers about to be replaced
+    cudaError_t err = cudaDeviceSynchronize();
+    if (err != cudaSuccess) return cuda_fail(h, err, "oc_bind_state");
+    double** slot[15];
+    state_slots(h, slot);
+    if (!a) {
+        if (h->bound)
+            for (int i = 0; i < 15; ++i) *slot[i] = h->own_state[i];
+        h->bound = false;
+        h->has_state = false;
+        drop_graphs(h);
+        return OC_OK;
+    }
+    const bool ts = h->cfg.tracers == OC_TRACERS_TS;
+    const size_t fsize[6] = {h->n2, h->n3, h->n3, h->n3, h->n3, h->n3};
+    struct Buf {
+        double* p;
+        size_t n;
+        int slot;  // index into slot[] for the current parity's set (parity 0 numbering)
+    };
+    std::vector<Buf> bufs;
+    const oc_state_view* sets[2] = {a, b};
+    for (int which = 0; which < 2; ++which) {
+        const oc_state_view* s = sets[which];
+        double* f[6] = {s->eta, s->u, s->v, s->b, s->T, s->S};
+        const int nf = ts ? 6 : 4;
+        for (int i = 0; i < nf; ++i) {
+            if (!f[i]) return fail(h, OC_ERR_ARG, "eta, u, v, b (and T, S with TS tracers) are required in both sets");
+            bufs.push_back({f[i], fsize[i], 6 * which + i});
+        }
+    }
+    double* opt[3] = {a->e, a->km, a->kh};
+    for (int i = 0; i < 3; ++i)
+        if (opt[i]) bufs.push_back({opt[i], h->n3i, 12 + i});
+    for (const Buf& x : bufs) {
+        if (reinterpret_cast<uintptr_t>(x.p) % alignof(double))
+            return fail(h, OC_ERR_ARG, "a bound buffer is not 8-byte aligned");
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, x.p) != cudaSuccess ||
+            (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != h->cfg.device) {
+            cudaGetLastError();
+            return fail(h, OC_ERR_ARG, "a bound buffer is not device memory of the handle's device");
+        }
+    }
+    for (size_t i = 0; i < bufs.size(); ++i)
+        for (size_t j = i + 1; j < bufs.size(); ++j) {
+            const char *p0 = reinterpret_cast<const char*>(bufs[i].p), *p1 = reinterpret_cast<const char*>(bufs[j].p);
+            if (p0 < p1 + bufs[j].n * sizeof(double) && p1 < p0 + bufs[i].n * sizeof(double))
+                return fail(h, OC_ERR_ARG, "two bound buffers overlap");
+        }
+    if (!h->bound)
+        for (int i = 0; i < 15; ++i) h->own_state[i] = *slot[i];
+    // set a becomes the current parity, set b the other one
+    const int c = h->cur;
+    for (int i = 0; i < 15; ++i) *slot[i] = h->own_state[i];
+    for (const Buf& x : bufs) {
+        int idx = x.slot;
+        if (idx < 12) idx = 6 * ((idx / 6) ^ c) + idx % 6;
+        *slot[idx] = x.p;
+    }
+    h->bound = true;
+    h->bound_base = c;
+    if (!a->e) fill(h->e, h->cfg.e_min, (int64_t)h->n3i, 0);
+    launch_wcol(h->P, h->U[c], h->V[c], h->w, 0);
+    if (a->km) {
+        launch_qsolve(h->P, h->km, h->q, 0);
+        launch_kukv(h->P, h->q, h->Ku, h->Kv, 0);
+        if (h->solver) h->solver->rebuild(0);
+    }
+    drop_graphs(h);
+    h->has_state = true;
+    err = cudaDeviceSynchronize();
+    return err == cudaSuccess ? check_launch(h, "oc_bind_state") : cuda_fail(h, err, "oc_bind_state");
+}
+
+int oc_state_parity(oc_handle* h, int32_t* which) {
+    if (!h || !which) return OC_ERR_ARG;
+    *which = h->bound ? (h->cur ^ h->bound_base) : 0;
+    return OC_OK;
 }
 
 int oc_reset_mixing(oc_handle* h) {

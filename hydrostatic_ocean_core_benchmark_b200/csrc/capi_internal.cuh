@@ -41,6 +41,11 @@ struct oc_handle {
     double *d_tau_u = nullptr, *d_tau_v = nullptr, *d_ustar2 = nullptr;
     double *U[2] = {}, *V[2] = {}, *B[2] = {}, *Tt[2] = {}, *Ss[2] = {}, *ETA[2] = {};
     int cur = 0;
+    // the handle's own state buffers while caller-owned ones are bound
+    // (oc_bind_state): ETA, U, V, B, Tt, Ss for both parities, then e, km, kh
+    bool bound = false;
+    int bound_base = 0;  // the parity that was current when the buffers were bound
+    double* own_state[15] = {};
     double *e = nullptr, *km = nullptr, *kh = nullptr, *q = nullptr, *w = nullptr;
     double *phi = nullptr, *pgx = nullptr, *pgy = nullptr, *avpv = nullptr, *avpu = nullptr;
     double *dzu = nullptr, *dzv = nullptr, *stu = nullptr, *stv = nullptr;

@@ -725,9 +725,9 @@ __device__ void mg_smooth(const HelmParams& H, int l, const double* xin, double*
 // new x (x0 or level 0's second buffer). Levels below coarse_from have a grid
 // down and up phase; the rest run in CTA 0, or, when every level is too large
 // for it, the coarsest level is smoothed on the grid.
-__device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* smem, double* persist, bool& ok) {
+__device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* x0b, double* smem, double* persist,
+                                bool& ok) {
     const int cf = H.coarse_from, nl = H.n_levels;
-    double* x0b = (x0 == H.lv[0].x) ? H.lv[0].x2 : H.lv[0].x;
     if (cf == 0) {
         if (s_grid.cta == 0) mg_coarse(H, smem, x0, x0b);
         ok = grid_sync(H);
@@ -811,7 +811,7 @@ __device__ __forceinline__ void helm_solve_body(const HelmParams& H, double* sme
                [&](int e) {
                    const double r = rhs[e] * L0.mask[e];
                    b0[e] = r;
-                   if (H.kind <= HK_PCG_RBGS) H.r[e] = r;
+                   if (H.kind <= HK_PCG_RBGS || H.kind == HK_PCG_MG) H.r[e] = r;
                    x[e] = 0.0;
                    return make_double2(r * r, 0.0);
                },
@@ -828,7 +828,7 @@ __device__ __forceinline__ void helm_solve_body(const HelmParams& H, double* sme
             double* xc = x;  // the level-0 buffer holding the current iterate
             for (int it = 1; it <= H.max_iter && ok; ++it) {
                 if (H.kind == HK_MULTIGRID) {
-                    xc = vcycle_tiled(H, xc, sm, persist, ok);
+                    xc = vcycle_tiled(H, xc, xc == H.lv[0].x ? H.lv[0].x2 : H.lv[0].x, sm, persist, ok);
                 } else {
                     colour_phase(L0, x, b0, 0, grid_team());
                     ok = grid_sync(H);
@@ -877,6 +877,21 @@ __device__ __forceinline__ void helm_solve_body(const HelmParams& H, double* sme
             // z = M^-1 r
             auto precondition = [&](bool& okp) {
                 if (jac) return;
+                if (H.kind == HK_PCG_MG) {
+                    // one V(2,2) cycle on level 0's rhs r from a zero iterate (symmetric:
+                    // red-black pre-smoothing, black-red post-smoothing)
+                    for (int e = grid_team().first; e < L0.n; e += grid_team().stride) {
+                        b0[e] = __ldcg(r + e);
+                        z[e] = 0.0;
+                    }
+                    okp = grid_sync(H);
+                    if (!okp) return;
+                    double* zr = vcycle_tiled(H, z, L0.x2, sm, persist, okp);
+                    if (!okp || zr == z) return;
+                    for (int e = grid_team().first; e < L0.n; e += grid_team().stride) z[e] = __ldcg(zr + e);
+                    okp = grid_sync(H);
+                    return;
+                }
                 for (int e = grid_team().first; e < L0.n; e += grid_team().stride) z[e] = 0.0;
                 okp = grid_sync(H);
                 if (!okp) return;
@@ -1137,7 +1152,8 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     masks.push_back(std::vector<double>(mask_host, mask_host + (size_t)nx * ny));
     int lnx = nx, lny = ny;
     std::vector<std::pair<int, int>> dims{{nx, ny}};
-    if (kind == HK_MULTIGRID) {
+    const bool mg_levels = kind == HK_MULTIGRID || kind == HK_PCG_MG;
+    if (mg_levels) {
         while (lnx % 2 == 0 && lny % 2 == 0 && lnx / 2 >= 8 && lny / 2 >= 8 &&
                (int)dims.size() < OC_MAX_LEVELS) {
             const int cnx = lnx / 2, cny = lny / 2;
@@ -1292,7 +1308,7 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     // Level 0 of a grid whose 32 x 32 tiles need more than one round over the SMs
     // runs 128 x 16 tiles instead. When NumPy's leaves are then exactly the tiles'
     // 128-cell rows, the last up phase forms the residual's leaf sums itself.
-    const bool grid_levels = kind == HK_MULTIGRID && H.n_levels >= 2 && H.coarse_from >= 1;
+    const bool grid_levels = mg_levels && H.n_levels >= 2 && H.coarse_from >= 1;
     const long long tiles32 = (long long)((nx + 31) / 32) * ((ny + 31) / 32);
     H.wide0 = (grid_levels && nx % TileWide::TX == 0 && tiles32 > sms) ? 1 : 0;
     // every other grid level takes the smallest tile whose count fits one round
@@ -1301,7 +1317,7 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     for (int l = 0; l < H.n_levels; ++l) {
         HLevel& L = H.lv[l];
         L.shape = SHAPE_32;
-        if (kind != HK_MULTIGRID) continue;
+        if (!mg_levels) continue;
         if (l == 0 && H.wide0) {
             L.shape = SHAPE_WIDE;
             continue;
@@ -1317,7 +1333,7 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     bool aligned = H.n_leaves > 0;
     for (int q = 0; q < H.n_leaves && aligned; ++q)
         aligned = leaves[q] == 128 * q && leaves[q + 1] - leaves[q] == 128;
-    H.fused_res = (H.wide0 && aligned) ? 1 : 0;
+    H.fused_res = (kind == HK_MULTIGRID && H.wide0 && aligned) ? 1 : 0;
     // shared memory: the persistent tile (if any), then the largest of the tree
     // fold, the grid levels' tiles and the coarse levels of CTA 0
     size_t tile_work = 0;
@@ -1331,21 +1347,21 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
             default: return Tile32::RN;
         }
     };
-    if (kind == HK_MULTIGRID) {
+    if (mg_levels) {
         for (int l = 0; l < n_grid; ++l)
             tile_work = std::max<size_t>(tile_work, (l == 0 && H.persist0 ? 2 : 6) * (size_t)rn_of(H.lv[l].shape));
         if (H.coarse_from >= H.n_levels) tile_work = std::max<size_t>(tile_work, 6 * (size_t)Tile32::RN);
     }
     const size_t coarse_work = 6 * coarse_cells + (H.coarse_from < H.n_levels ? (size_t)H.lv[H.coarse_from].n : 0);
-    const size_t mg_work = (kind == HK_MULTIGRID) ? std::max<size_t>(tile_work, coarse_work) : 0;
+    const size_t mg_work = mg_levels ? std::max<size_t>(tile_work, coarse_work) : 0;
     // in a batched launch a system has fewer CTAs than tiles: no persistent level-0
     // tile (its six arrays are loaded per tile instead) and no shared copy of the plan
     size_t tile_work_b = 0;
-    if (kind == HK_MULTIGRID) {
+    if (mg_levels) {
         for (int l = 0; l < n_grid; ++l) tile_work_b = std::max<size_t>(tile_work_b, 6 * (size_t)rn_of(H.lv[l].shape));
         if (H.coarse_from >= H.n_levels) tile_work_b = std::max<size_t>(tile_work_b, 6 * (size_t)Tile32::RN);
     }
-    const size_t mg_work_b = (kind == HK_MULTIGRID) ? std::max<size_t>(tile_work_b, coarse_work) : 0;
+    const size_t mg_work_b = mg_levels ? std::max<size_t>(tile_work_b, coarse_work) : 0;
     smem_batched_ = sizeof(double) * std::max<size_t>(fold_doubles, mg_work_b);
     // the tree fold and the V-cycle never run at the same time: one region serves both
     smem_ = sizeof(double) * ((H.persist0 ? 4 * (size_t)TileWide::RN : 0) + std::max<size_t>(fold_doubles, mg_work));

@@ -7,7 +7,9 @@
 
 namespace oc {
 
-enum { HK_PCG_JACOBI = 0, HK_PCG_RBGS = 1, HK_RBGS = 2, HK_MULTIGRID = 3 };
+// HK_PCG_MG (no reference counterpart): CG preconditioned by one symmetric
+// V(2,2) cycle of the multigrid hierarchy; the mixed-precision step's solver
+enum { HK_PCG_JACOBI = 0, HK_PCG_RBGS = 1, HK_RBGS = 2, HK_MULTIGRID = 3, HK_PCG_MG = 5 };
 
 struct HLevel {
     int nx, ny, n;

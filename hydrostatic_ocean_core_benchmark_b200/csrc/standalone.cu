@@ -64,7 +64,7 @@ extern "C" int oc_helm_create(const oc_helm_config* cfg, const double* ku, const
     *out = nullptr;
     if (cfg->nx < 2 || cfg->ny < 2 || !(cfg->dx > 0.0) || !(cfg->dy > 0.0) || !(cfg->coef >= 0.0) ||
         !(cfg->rtol > 0.0) || cfg->max_iter < 1 || cfg->solver < OC_SOLVER_PCG_JACOBI ||
-        cfg->solver > OC_SOLVER_PCG_REFINED)
+        cfg->solver > OC_SOLVER_PCG_MG)
         return OC_ERR_ARG;
     if (cudaSetDevice(cfg->device) != cudaSuccess) return OC_ERR_CUDA;
     oc_helm* h = new oc_helm();

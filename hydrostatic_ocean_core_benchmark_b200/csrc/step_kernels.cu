@@ -38,6 +38,20 @@ typedef float real;
 typedef double real;
 #endif
 typedef double wide;
+
+// Minimum resident CTAs per SM the register allocation of the three largest
+// stencil/column kernels is bounded for (__launch_bounds__): k_closure runs
+// 128 threads, k_mom_column 512 and k_tracer_rhs 256 per CTA. The bits of the
+// results do not depend on them.
+#ifndef OC_MINB_CLOSURE
+#define OC_MINB_CLOSURE 8
+#endif
+#ifndef OC_MINB_MOM
+#define OC_MINB_MOM 2
+#endif
+#ifndef OC_MINB_TRACER
+#define OC_MINB_TRACER 4
+#endif
 using KPR = KPT<real>;
 using ColGeoR = ColGeoT<real>;
 
@@ -133,7 +147,7 @@ __global__ void __launch_bounds__(128) k_qsolve(KPR P, const real* __restrict__ 
 // at a level is read just before) and q. With the Gaspar lengths, the lengths
 // of interface k are formed inside the forward sweep.
 template <int NZM>
-__global__ void __launch_bounds__(128, 8) k_closure(KPR P, const real* __restrict__ u,
+__global__ void __launch_bounds__(128, OC_MINB_CLOSURE) k_closure(KPR P, const real* __restrict__ u,
                                                  const real* __restrict__ v,
                                                  const wide* __restrict__ b,
                                                  real* __restrict__ e, real* __restrict__ km,
@@ -642,7 +656,7 @@ struct TileLevel {
     __device__ __forceinline__ real MV(int dj, int di) const { return k < skv[rc + dj * MOM_RX + di] ? real(1.0) : real(0.0); }
 };
 
-__global__ void __launch_bounds__(MOM_TX * MOM_TY * 2, 2) k_mom_column(
+__global__ void __launch_bounds__(MOM_TX * MOM_TY * 2, OC_MINB_MOM) k_mom_column(
     KPR P, const real* __restrict__ u, const real* __restrict__ v, const wide* __restrict__ b,
     const wide* __restrict__ phi, const real* __restrict__ w, const real* __restrict__ km,
     real* __restrict__ pgx, real* __restrict__ pgy, real* __restrict__ avpv,
@@ -1009,7 +1023,7 @@ __device__ __forceinline__ real tracer_vface(const KPR& P, const ColGeoR& g, int
     return real(0.5) * (f_m1 + f_0);
 }
 
-__global__ void __launch_bounds__(TRX * TRY, 4) k_tracer_rhs(KPR P, const real* __restrict__ C0,
+__global__ void __launch_bounds__(TRX * TRY, OC_MINB_TRACER) k_tracer_rhs(KPR P, const real* __restrict__ C0,
                                                              const real* __restrict__ S,
                                                              const real* __restrict__ u,
                                                              const real* __restrict__ v,

@@ -29,7 +29,7 @@ import numpy as np
 
 from . import _lib
 
-KINDS = {"pcg_jacobi": 0, "pcg_rbgs": 1, "rbgs": 2, "multigrid": 3, "pcg_refined": 4}
+KINDS = {"pcg_jacobi": 0, "pcg_rbgs": 1, "rbgs": 2, "multigrid": 3, "pcg_refined": 4, "pcg_mg": 5}
 
 
 @dataclass
@@ -49,7 +49,7 @@ class HelmholtzVar:
                  min_size: int = 8, device: int = 0) -> None:
         if kind not in KINDS:
             raise ValueError(f"unknown variable-coefficient solver '{kind}' "
-                             "(expected pcg_jacobi|pcg_rbgs|rbgs|multigrid|pcg_refined)")
+                             "(expected pcg_jacobi|pcg_rbgs|rbgs|multigrid|pcg_refined|pcg_mg)")
         if (n_pre, n_post, min_size) != (2, 2, 8):
             raise ValueError("the B200 multigrid is V(2,2) coarsened down to 8 cells "
                              "(n_pre=2, n_post=2, min_size=8)")

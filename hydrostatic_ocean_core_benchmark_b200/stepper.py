@@ -155,6 +155,51 @@ class OceanStepper:
         sp = getattr(stream, "cuda_stream", stream)
         self._call("oc_set_state_async", self.lib.oc_set_state_async, self.h, C.byref(view), dev, sp)
 
+    def bind_state(self, current: dict | None, other: dict | None = None):
+        """Make caller-owned CUDA tensors the state, without a copy (oc_bind_state).
+
+        ``current`` holds the state to start from (eta, u, v, b and, with TS
+        tracers, T and S; optionally e, km, kh, used in place); ``other`` names
+        tensors of the same fields (without e, km, kh) that the step writes
+        into. The state alternates between the two sets, one step each:
+        ``state_parity()`` says which holds it. The stepper keeps both sets
+        alive until the next bind_state; ``bind_state(None)`` returns to the
+        handle's own buffers (set the state again after it)."""
+        if current is None:
+            if other is not None:
+                raise ValueError("give both sets, or neither")
+            self._call("oc_bind_state", self.lib.oc_bind_state, self.h, None, None)
+            self._bound = None
+            return
+        if other is None:
+            raise ValueError("bind_state needs the second set the step writes into")
+        for name, a in list(current.items()) + list(other.items()):
+            if a is not None and not (_is_tensor(a) and a.is_cuda):
+                raise ValueError(f"{name}: bound buffers must be CUDA tensors")
+        if any(other.get(k) is not None for k in FIELDSI):
+            raise ValueError("e, km and kh are bound once, in the current set")
+        va, _, _ = self._view(current, self._shapes(), writable=True)
+        vb, _, _ = self._view(other, self._shapes(), writable=True)
+        self._call("oc_bind_state", self.lib.oc_bind_state, self.h, C.byref(va), C.byref(vb))
+        self._bound = (dict(current), dict(other))
+
+    def state_parity(self) -> int:
+        """0 when the bound ``current`` set holds the state, 1 when ``other`` does."""
+        w = C.c_int32()
+        self._call("oc_state_parity", self.lib.oc_state_parity, self.h, C.byref(w))
+        return int(w.value)
+
+    def bound_state(self) -> dict:
+        """The bound tensors that hold the current state (no copy; read after the
+        stream has passed the steps)."""
+        if not getattr(self, "_bound", None):
+            raise RuntimeError("no state is bound")
+        cur, oth = self._bound
+        src = oth if self.state_parity() else cur
+        out = {k: v for k, v in src.items() if v is not None and k not in FIELDSI}
+        out.update({k: v for k, v in cur.items() if v is not None and k in FIELDSI})
+        return out
+
     def get_state_async(self, stream, out: dict):
         """Enqueue the copies of the current state into ``out`` on `stream` without
         waiting (oc_get_state_async); ``out`` is complete once the stream passes them."""

@@ -52,6 +52,10 @@ enum { OC_SOLVER_PCG_JACOBI = 0, OC_SOLVER_PCG_RBGS = 1, OC_SOLVER_RBGS = 2, OC_
 /* standalone Helmholtz solver only (oc_helm_*), no reference counterpart: FP32
  * inner PCG-Jacobi inside FP64 iterative refinement */
 enum { OC_SOLVER_PCG_REFINED = 4 };
+/* no reference counterpart: CG preconditioned by one symmetric V(2,2) cycle of
+ * the multigrid hierarchy, fp64. The mixed-precision step solves with it where
+ * the configuration names multigrid; the standalone solver offers it too. */
+enum { OC_SOLVER_PCG_MG = 5 };
 enum { OC_BC_PERIODIC = 0, OC_BC_CLOSED = 1 };
 enum { OC_FACE_MIN = 0, OC_FACE_MEAN = 1, OC_FACE_HARMONIC = 2 };
 enum { OC_EOS_LINEAR = 0, OC_EOS_SEOS = 1, OC_EOS_TEOS10 = 2 };
@@ -204,6 +208,24 @@ int oc_set_state(oc_handle* h, const oc_state_view* s, int32_t on_device);
  * other work. A following oc_step on the same stream sees the state. No
  * reference counterpart: the reference steps host arrays synchronously. */
 int oc_set_state_async(oc_handle* h, const oc_state_view* s, int32_t on_device, void* stream);
+
+/* Take caller-owned device buffers as the state, without a copy (fp64
+ * handles; the mixed-precision step keeps FP32 fields and refuses). `a` holds
+ * the state to start from: eta, u, v, b and, with TS tracers, T and S are
+ * required; e, km and kh are optional (NULL keeps the handle's own arrays, e
+ * then reset to e_min as oc_set_state does). `b` names a second set of eta, u,
+ * v, b (and T, S) that the step writes into: the state alternates between the
+ * two sets, one step each (oc_state_parity says which holds it). Every buffer
+ * is device memory of this handle's device, 8-byte aligned, of the size
+ * oc_set_state reads, and no two of them overlap. The handle never frees
+ * them; they must outlive the handle or the next oc_bind_state. Recorded
+ * graphs are dropped. Both NULL: back to the handle's own buffers (the state
+ * must then be set again). Synchronises. No reference counterpart: the
+ * reference's stepper returns new arrays from every step. */
+int oc_bind_state(oc_handle* h, const oc_state_view* a, const oc_state_view* b);
+
+/* Which bound set holds the current state: 0 = a, 1 = b (0 when unbound). */
+int oc_state_parity(oc_handle* h, int32_t* which);
 
 /* Restore the constant viscosity nu and diffusivity kappa of the
  * configuration (the stepper's state at construction). */
