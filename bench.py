@@ -40,8 +40,7 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = json.loads((ROOT / "BASELINE.json").read_text())["metric"] if (ROOT / "BASELINE.json").exists() \
-    else "cell-steps/s"
+METRIC = "cell-steps/s fp64 vs mixed (≤1e-6 rel L2 vs fp64); adjoint/forward time ratio"
 UNIT = "cell-steps/s"
 HBM_FALLBACK_GBS = 6650.0
 
@@ -190,7 +189,7 @@ def dram_traffic_from_profiles(kernel: str):
 # ------------------------------------------------------------------ workloads
 def workload(args):
     from hydrostatic_ocean_core_benchmark_b200 import cases
-    return cases.seamount_basin(nx=args.nx, ny=args.ny, nz=args.nz, seed=args.seed)
+    return cases.seamount_basin(nx=args.nx, ny=args.ny, nz=args.nz, seed=args.seed, dt=args.dt)
 
 
 def cpu_oracle_rate(args, steps: int, warmup: int):
@@ -609,16 +608,30 @@ def run_ensemble(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     rng = np.random.default_rng(args.seed + 5)
-    members, shapes = [], []
+    members, shapes, solvers, twins = [], [], [], []
+    prec = args.ens_precision
     for m in range(args.ens_members):
-        nx, ny = (32 * int(x) for x in rng.integers(4, 13, 2))
+        if args.ens_sizes == "any":
+            nx, ny = (int(x) for x in rng.integers(128, 385, 2))
+        else:
+            nx, ny = (32 * int(x) for x in rng.integers(4, 13, 2))
         nz = int(rng.choice([24, 32, 48]))
-        s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=args.seed + 1000 * (rank + 1) + m)
+        # the multigrid halves a grid only while its sizes are even: sizes with an
+        # odd factor above 8 take PCG-Jacobi
+        solver = "multigrid" if nx % 32 == 0 and ny % 32 == 0 else "pcg_jacobi"
+        s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=args.seed + 1000 * (rank + 1) + m, solver_kind=solver)
         st = OceanStepper(s.params, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c,
-                          device=local_rank)
+                          device=local_rank, precision=prec)
         st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
         members.append(st)
         shapes.append((nx, ny, nz))
+        solvers.append(solver)
+        if prec == "mixed" and len(twins) < args.ens_check:
+            # an fp64 twin of the member, stepped as often, for the per-member error
+            tw = OceanStepper(s.params, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c,
+                              device=local_rank)
+            tw.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
+            twins.append((m, tw))
     cells = sum(nx * ny * nz for nx, ny, nz in shapes)
     tiling = [st.autotune() for st in members]
     stream = torch.cuda.Stream(device=local_rank)
@@ -653,13 +666,40 @@ def run_ensemble(args, rank, world, local_rank):
     diverged = sum(st.stats()["diverged"] for st in members)
     if failures or diverged:
         raise RuntimeError(f"ensemble run failed: {failures} solver failures, {diverged} diverged members")
+    # HBM roofline of the ensemble step: every member's minimal-pass bytes (fp64
+    # accounting) over the batched step's time
+    hbm = None
+    if prec == "fp64":
+        alg = 0.0
+        for st, (nx, ny, nz) in zip(members, shapes):
+            sts = st.stats()
+            alg += step_algorithmic_bytes(st.p, sts["solver_iterations"] / max(sts["steps"], 1))
+        peak, src = measured_hbm_peak()
+        achieved = alg / (ms / steps / 1e3) / 1e9
+        hbm = {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+               "algorithmic_bytes_per_step": alg, "peak_source": src}
+    errors = None
+    if twins:
+        total = warm + 2 + steps + 2 + steps
+        errors = []
+        for m, tw in twins:
+            tw.step(total, stream=stream, graph=True)
+            stream.synchronize()
+            a = members[m].get_state(fields=("eta", "u", "v", "T", "S"))
+            b = tw.get_state(fields=("eta", "u", "v", "T", "S"))
+            rel = {f: float(np.linalg.norm(a[f] - b[f]) / max(np.linalg.norm(b[f]), 1e-300)) for f in a}
+            errors.append({"member": m, "grid": list(shapes[m]), "rel_l2_vs_fp64": rel})
+            tw.close()
     line = {"metric": METRIC, "value": world * cells * steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
             "steps": steps, "warmup": warm, "ms_per_step": ms / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded seamount-basin recipe per member; inputs generated on the host)",
-            "config": {"workload": f"ensemble of {len(members)} seamount basins, nx, ny multiples of 32 in 128..384, "
-                                   "nz in {24, 32, 48}, theta=0.6 + multigrid, TKE, TVD3, polyTEOS10",
-                       "members": len(members), "cells": cells,
+            "config": {"workload": f"ensemble of {len(members)} seamount basins, nx, ny "
+                                   + ("uniform in 128..384" if args.ens_sizes == "any" else "multiples of 32 in 128..384")
+                                   + ", nz in {24, 32, 48}, theta=0.6 + multigrid (PCG-Jacobi on sizes the multigrid "
+                                   "cannot halve), TKE, TVD3, polyTEOS10",
+                       "members": len(members), "cells": cells, "precision": prec,
+                       "solvers": {k: solvers.count(k) for k in sorted(set(solvers))},
                        "grids": [list(g) for g in shapes[:8]] + (["..."] if len(shapes) > 8 else []),
                        "parallelism": "replicas x1"},
             "sequential": {"value": world * cells * steps / (ms_seq / 1e3), "unit": UNIT,
@@ -668,6 +708,13 @@ def run_ensemble(args, rank, world, local_rank):
             "tiling": {"levels_per_cta_momentum": sorted(set(t[0] for t in tiling)),
                        "levels_per_cta_tracers": sorted(set(t[1] for t in tiling))},
             "clocks": clk}
+    if hbm:
+        line["roofline"] = hbm
+    if errors:
+        line["member_errors"] = errors
+        line["worst_member_rel_l2"] = {f: max(e["rel_l2_vs_fp64"][f] for e in errors) for f in errors[0]["rel_l2_vs_fp64"]}
+    if prec == "mixed":
+        line["dtype"] = "f32 (3D state and stencils) + f64 (b, pressure gradient, EOS, eta, Helmholtz)"
     if rank == 0:
         print(json.dumps(line), flush=True)
     ens.close()
@@ -788,6 +835,73 @@ def run_helmholtz(args, rank, world, local_rank):
     return 0
 
 
+def run_adjoint(args, rank, world, local_rank):
+    """--workload adjoint: the gradient form. The seamount recipe with the
+    closure off (the adjoint's scope) at 256 x 256 x 32, 20 steps with a
+    checkpoint every 5: the forward run (steps back to back, the state fetched
+    at the checkpoints), the gradient of the mean temperature of the top three
+    levels with respect to the initial temperature and the x-stress field
+    (segments recomputed from their checkpoints, then walked back with
+    oc_adjoint_step), their ratio and the peak device memory."""
+    import numpy as np
+    import torch
+
+    from hydrostatic_ocean_core_benchmark_b200 import cases
+    from hydrostatic_ocean_core_benchmark_b200.adjoint import OceanRollout, rollout_apply
+    torch.cuda.set_device(local_rank)
+    if rank != 0:
+        return 0
+    nx, ny, nz = (args.nx, args.ny, args.nz) if "--nx" in sys.argv else (256, 256, 32)
+    n_steps = args.steps if "--steps" in sys.argv else 20
+    every = 5
+    s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=args.seed, closure="none", advection="up3_tvd")
+    dev = f"cuda:{local_rank}"
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)  # noqa: E731
+    fixed = {"eta": T(s.eta), "u": T(s.u), "v": T(s.v), "S": T(s.S)}
+    T0, taux = T(s.T), T(s.taux_c)
+    w = torch.zeros(s.params.nz, ny, nx, dtype=torch.float64, device=dev)
+    w[:3] = 1.0 / (3 * nx * ny)
+    ro = OceanRollout(s.params, s.H, s.mask, dzr=s.dzr, n_steps=n_steps, every=every, device=local_rank)
+    state0 = {"eta": fixed["eta"], "u": fixed["u"], "v": fixed["v"], "T": T0, "S": fixed["S"]}
+    fwd, bwd = [], []
+    torch.cuda.reset_peak_memory_stats(local_rank)
+    free0 = torch.cuda.mem_get_info(local_rank)[0]
+    low = free0
+    for it in range(args.warmup + 3):
+        t0 = T0.clone().requires_grad_(True)
+        tx = taux.clone().requires_grad_(True)
+        out = rollout_apply(ro, t0, tx, fixed)
+        low = min(low, torch.cuda.mem_get_info(local_rank)[0])
+        (w * out["T"]).sum().backward()
+        if it >= args.warmup:
+            fwd.append(ro.timing["forward_s"])
+            bwd.append(ro.timing["backward_s"])
+        del out, t0, tx
+    plain = []
+    for _ in range(3):
+        ro.forward(state0, taux)
+        plain.append(ro.timing["forward_s"])
+    lib_bytes = int(ro.st.stats()["device_bytes"])
+    peak = int(torch.cuda.max_memory_allocated(local_rank))
+    ro.close()
+    cells = nx * ny * s.params.nz
+    f_s, b_s = float(np.median(fwd)), float(np.median(bwd))
+    line = {"metric": "adjoint / forward wall time of the gradient of a 20-step run",
+            "value": b_s / f_s, "unit": "x", "n_gpus": 1, "steps": n_steps, "warmup": args.warmup,
+            "ms_per_step": b_s / n_steps * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded seamount-basin recipe, closure off)",
+            "config": {"workload": f"seamount_basin {nx}x{ny}x{s.params.nz}, TVD3 + polyTEOS10, closure off, "
+                                   f"theta={s.params.theta:g} + {s.params.solver_kind}, {n_steps} steps, "
+                                   f"checkpoint every {every}",
+                       "cells": cells, "variant": "gradient form (hand-written adjoint)"},
+            "forward_ms": f_s * 1e3, "adjoint_ms": b_s * 1e3, "forward_alone_ms": float(np.median(plain)) * 1e3,
+            "forward_cell_steps_per_s": cells * n_steps / f_s,
+            "adjoint_includes": "segment recomputation from the checkpoints + adjoint steps + EOS adjoint",
+            "peak_device_bytes": {"torch_tensors": peak, "library_handle": lib_bytes,
+                                  "process_delta_at_forward_end": int(free0 - low)}}
+    print(json.dumps(line), flush=True)
+    return 0
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -798,6 +912,8 @@ def main():
     ap.add_argument("--ny", type=int, default=512)
     ap.add_argument("--nz", type=int, default=50)
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--dt", type=float, default=None,
+                    help="time step in s (default 600; the precision workload's 1024x1024 grid takes 300)")
     ap.add_argument("--e2e-steps", type=int, default=12)
     ap.add_argument("--profile-steps", type=int, default=20,
                     help="steps of the per-kernel event region (kernel shares, roofline)")
@@ -807,17 +923,30 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-nx", type=int, default=128)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["seamount", "ensemble", "helmholtz", "precision"], default="seamount",
+    ap.add_argument("--workload", choices=["seamount", "ensemble", "helmholtz", "precision", "adjoint"], default="seamount",
                     help="seamount: the 512x512x50 basin (the headline line); ensemble: the "
                          "batched-ensemble form (its own line); helmholtz: the FP64 and the "
                          "FP32-inner/FP64-refined Helmholtz solvers alone (its own line); precision: "
-                         "the mixed FP32/FP64 step beside the fp64 one (default grid 1024x1024x64)")
+                         "the mixed FP32/FP64 step beside the fp64 one (default grid 1024x1024x64); "
+                         "adjoint: gradient of a run through the hand-written adjoint (256x256x32, "
+                         "--steps steps)")
     ap.add_argument("--mixed-steps", type=int, default=100,
                     help="timed steps of the mixed-precision leg of the headline line (0: skip it)")
     ap.add_argument("--ens-members", type=int, default=64)
+    ap.add_argument("--ens-sizes", choices=["mult32", "any"], default="mult32",
+                    help="member nx, ny: multiples of 32 in 128..384, or any integer in 128..384")
+    ap.add_argument("--ens-precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--ens-check", type=int, default=8,
+                    help="mixed members checked against an fp64 twin")
     ap.add_argument("--helm-sizes", default="512,1024,2048,4096",
                     help="grid sizes n of the n x n Helmholtz systems")
     args = ap.parse_args()
+    if args.workload == "precision" and "--nx" not in sys.argv:
+        args.nx, args.ny, args.nz = 1024, 1024, 64
+    if args.dt is None:
+        # at dx = 1.95 km (1024 x 1024) the explicit baroclinic terms take dt <= ~400 s:
+        # the recipe's 600 s grows u threefold per step there; 768^2 and 512^2 run 600 s
+        args.dt = 300.0 if args.nx >= 1024 else 600.0
     rank = env_int("RANK", 0)
     world = env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)
@@ -827,9 +956,9 @@ def main():
         return run_ensemble(args, rank, world, local_rank)
     if args.workload == "helmholtz":
         return run_helmholtz(args, rank, world, local_rank)
+    if args.workload == "adjoint":
+        return run_adjoint(args, rank, world, local_rank)
     if args.workload == "precision":
-        if "--nx" not in sys.argv:
-            args.nx, args.ny, args.nz = 1024, 1024, 64
         return run_precision(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 

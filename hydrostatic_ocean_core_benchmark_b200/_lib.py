@@ -18,7 +18,7 @@ ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "unsupported option", 4: "c
           5: "device-side wait timed out", 6: "I/O error", 7: "request above a fixed buffer size"}
 
 SCHEMES = {"fb": 0, "theta": 1, "split_explicit": 2}
-SOLVERS = {"pcg_jacobi": 0, "pcg_rbgs": 1, "rbgs": 2, "multigrid": 3}
+SOLVERS = {"pcg_jacobi": 0, "pcg_rbgs": 1, "rbgs": 2, "multigrid": 3, "pcg_mg": 5}
 BCS = {"periodic": 0, "closed": 1}
 FACE_RULES = {"min": 0, "mean": 1, "harmonic": 2}
 EOS = {"linear": 0, "seos": 1, "teos10": 2}
@@ -92,6 +92,7 @@ _SIGNATURES = {
     "oc_set_state": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.c_int32]),
     "oc_set_state_async": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.c_int32, C.c_void_p]),
     "oc_reset_mixing": (C.c_int, [C.c_void_p]),
+    "oc_set_wait_bound": (C.c_int, [C.c_void_p, C.c_int64]),
     "oc_bind_state": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.POINTER(OcStateView)]),
     "oc_state_parity": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "oc_get_state": (C.c_int, [C.c_void_p, C.POINTER(OcStateView), C.c_int32]),

@@ -57,18 +57,34 @@ class OceanRollout:
         t = taux.detach().cpu().numpy()
         self.st.set_forcing(t, np.zeros_like(t))
 
-    def _advance(self, state: dict, b_given: bool = True) -> dict:
-        """One step from `state` (device tensors); returns the new state."""
+    def _stream(self):
+        import torch
+        return torch.cuda.current_stream(self.device)
+
+    def _fetch(self) -> dict:
+        """The current state into new tensors, enqueued on the current stream."""
+        out = {k: v for k, v in zip(STATE, self._empty())}
+        self.st.get_state_async(self._stream(), out)
+        return out
+
+    def _empty(self):
+        import torch
+        dev = f"cuda:{self.device}"
+        return [torch.empty(s, dtype=torch.float64, device=dev) for s in self._shapes().values()]
+
+    def _segment(self, state: dict, n: int) -> list:
+        """The n states after `state` (which carries its b), one per step."""
         st = self.st
-        st.set_state(eta=state["eta"], u=state["u"], v=state["v"], b=state["b"] if b_given else None,
-                     T=state["T"], S=state["S"])
-        st.step(1)
-        out = self._zeros()
-        st.get_state(out=out, fields=STATE)
+        st.set_state(eta=state["eta"], u=state["u"], v=state["v"], b=state["b"], T=state["T"], S=state["S"])
+        out = []
+        for _ in range(n):
+            st.step(1, stream=self._stream())
+            out.append(self._fetch())
         return out
 
     def forward(self, state0: dict, taux) -> dict:
-        """state0: eta, u, v, T, S (device tensors; b is diagnosed from T and S)."""
+        """state0: eta, u, v, T, S (device tensors; b is diagnosed from T and S).
+        The steps run back to back; the state is fetched at the checkpoints only."""
         import torch
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -78,10 +94,14 @@ class OceanRollout:
         cur = self._zeros()
         st.get_state(out=cur, fields=STATE)
         self.checkpoints = {0: cur}
-        for n in range(self.n):
-            cur = self._advance(cur)
-            if (n + 1) % self.every == 0 and n + 1 < self.n:
-                self.checkpoints[n + 1] = cur
+        done = 0
+        while done < self.n:
+            m = min(self.every, self.n - done)
+            st.step(m, stream=self._stream())
+            done += m
+            cur = self._fetch()
+            if done < self.n:
+                self.checkpoints[done] = cur
         torch.cuda.synchronize()
         self.timing["forward_s"] = time.perf_counter() - t0
         return cur
@@ -113,9 +133,7 @@ class OceanRollout:
         for si in range(len(starts) - 1, -1, -1):
             s0 = starts[si]
             s1 = starts[si + 1] if si + 1 < len(starts) else self.n
-            states = [self.checkpoints[s0]]
-            for _ in range(s0, s1):
-                states.append(self._advance(states[-1]))
+            states = [self.checkpoints[s0]] + self._segment(self.checkpoints[s0], s1 - s0)
             for t in range(s1 - s0 - 1, -1, -1):
                 cot = self._adjoint_step(states[t], states[t + 1], cot, taux_b)
             del states

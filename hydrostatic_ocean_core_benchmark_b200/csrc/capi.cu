@@ -99,7 +99,8 @@ int validate(const oc_config* c, std::string& err) {
         return err = "theta must lie in (0,1]", OC_ERR_ARG;
     if (c->n_picard < 1) return err = "n_picard must be >= 1", OC_ERR_ARG;
     if (!(c->dt > 0.0)) return err = "dt must be > 0", OC_ERR_ARG;
-    if (c->solver < 0 || c->solver > 3) return err = "unknown Helmholtz solver", OC_ERR_ARG;
+    if (c->solver < 0 || (c->solver > 3 && c->solver != OC_SOLVER_PCG_MG))
+        return err = "unknown Helmholtz solver", OC_ERR_ARG;
     if (c->max_iter < 1) return err = "max_iter must be >= 1", OC_ERR_ARG;
     if (c->bc_x < 0 || c->bc_x > 1 || c->bc_y < 0 || c->bc_y > 1)
         return err = "bc must be periodic|closed (open boundaries are not supported)", OC_ERR_UNSUPPORTED;
@@ -769,10 +770,7 @@ static int set_domain_impl(oc_handle* h, const double* Hh, const double* maskh, 
     if (h->cfg.scheme == OC_SCHEME_THETA) {
         h->solver = new HelmSolver();
         const double coef = h->cfg.g * std::pow(h->cfg.theta, 2.0) * std::pow(h->cfg.dt, 2.0);
-        // the mixed-precision step needs no reference iteration counts: where the
-        // configuration names the stationary multigrid it solves by MG-preconditioned CG
-        const int kind = (h->mixed && h->cfg.solver == OC_SOLVER_MULTIGRID) ? OC_SOLVER_PCG_MG : h->cfg.solver;
-        rc = h->solver->init(nx, ny, h->cfg.lx / nx, h->cfg.ly / ny, coef, kind, h->cfg.rtol,
+        rc = h->solver->init(nx, ny, h->cfg.lx / nx, h->cfg.ly / ny, coef, h->cfg.solver, h->cfg.rtol,
                              h->cfg.max_iter, h->mask.data(), h->Ku, h->Kv, 4096, h->d_status, h->err);
         if (rc) return rc;
     }
@@ -1631,6 +1629,18 @@ int oc_get_solve_log(oc_handle* h, int32_t* iterations, int32_t capacity, int32_
     if (iterations && capacity > 0 && n > 0)
         cudaMemcpy(iterations, h->solver->d_log_iters(), std::min(n, capacity) * sizeof(int),
                    cudaMemcpyDeviceToHost);
+    return OC_OK;
+}
+
+int oc_set_wait_bound(oc_handle* h, int64_t cycles) {
+    if (!h) return OC_ERR_ARG;
+    if (cycles < 1) return fail(h, OC_ERR_ARG, "the wait bound must be at least one cycle");
+    if (!h->has_domain) return fail(h, OC_ERR_STATE, "set the domain first");
+    cudaSetDevice(h->cfg.device);
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(h, e, "oc_set_wait_bound");
+    if (h->solver) h->solver->set_wait_cycles(cycles);
+    drop_graphs(h);  // recorded solve launches carry the old bound
     return OC_OK;
 }
 

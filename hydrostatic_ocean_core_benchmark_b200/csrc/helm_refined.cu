@@ -274,6 +274,7 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
         res = sqrt(s.x);
         rz = s.y;
     }
+    grid_sync_end(R.bar_count, blockIdx.x == 0);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         R.report[0] = inner;
         R.report[1] = conv ? 1 : 0;

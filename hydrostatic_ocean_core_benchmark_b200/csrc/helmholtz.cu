@@ -64,7 +64,7 @@ static __shared__ SolveGrid s_grid;
 __device__ __forceinline__ void grid_sync_begin(const HelmParams& H) { grid_sync_begin(H.status); }
 
 __device__ __forceinline__ bool grid_sync(const HelmParams& H) {
-    return grid_sync(H.bar_count, H.status, (unsigned)s_grid.ncta);
+    return grid_sync(H.bar_count, H.status, (unsigned)s_grid.ncta, H.wait_cycles);
 }
 
 // ------------------------------------------------------------------ level operators
@@ -262,9 +262,64 @@ __device__ double fold_blocks(const HelmParams& H, const double* leaf, double* b
     return r;
 }
 
+// The same fold when NumPy's tree over the leaves is perfect (2^m leaves, node
+// (i, i + 2^h) at height h; H.perfect_lanes = P > 0): each lane folds P
+// consecutive leaves in registers, the lanes of a warp fold their subtrees by
+// shuffles, and warp 0 folds the warps' subtrees. Every addition is the tree's
+// (left + right), so the result is bit-identical to tree_fold's, with two CTA
+// barriers instead of one per height.
+template <int P>
+__device__ __forceinline__ double lane_tree(const double* v) {
+    if constexpr (P == 1)
+        return v[0];
+    else
+        return lane_tree<P / 2>(v) + lane_tree<P / 2>(v + P / 2);
+}
+
+template <int P>
+__device__ double perfect_fold(int n, const double* leaf, double* sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwa = n / (32 * P);  // warps in use: a power of two, at most the CTA's
+    if (warp < nwa) {
+        double v[P];
+        const double* src = leaf + warp * 32 * P + lane * P;
+#pragma unroll
+        for (int q = 0; q < P; ++q) v[q] = __ldcg(src + q);
+        double x = lane_tree<P>(v);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_down_sync(0xffffffffu, x, o);
+            if ((lane & (2 * o - 1)) == 0) x = x + y;
+        }
+        if (lane == 0) sm[warp] = x;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        double x = lane < nwa ? sm[lane] : 0.0;
+        for (int o = 1; o < nwa; o <<= 1) {
+            const double y = __shfl_down_sync(0xffffffffu, x, o);
+            if ((lane & (2 * o - 1)) == 0) x = x + y;
+        }
+        __syncwarp();
+        if (lane == 0) sm[0] = x;
+    }
+    __syncthreads();
+    const double r = sm[0];
+    __syncthreads();
+    return r;
+}
+
 // the sum of one of the leaf buffers (leafA, leafB or leafC) in NumPy's order
 __device__ __forceinline__ double fold_sum(const HelmParams& H, const FoldPlan& F, const double* leaf, double* sm,
                                            bool& ok) {
+    switch (H.perfect_lanes) {
+        case 1: return perfect_fold<1>(H.n_leaves, leaf, sm);
+        case 2: return perfect_fold<2>(H.n_leaves, leaf, sm);
+        case 4: return perfect_fold<4>(H.n_leaves, leaf, sm);
+        case 8: return perfect_fold<8>(H.n_leaves, leaf, sm);
+        case 16: return perfect_fold<16>(H.n_leaves, leaf, sm);
+        default: break;
+    }
     if (!H.big_fold) return tree_fold(H, F, leaf, sm);
     double* broot = leaf == H.leafA ? H.broot : (leaf == H.leafB ? H.broot + H.n_blocks : H.broot + 2 * H.n_blocks);
     return fold_blocks(H, leaf, broot, sm, ok);
@@ -978,6 +1033,7 @@ __device__ __forceinline__ void helm_solve_body(const HelmParams& H, double* sme
         }
     }
 done:
+    grid_sync_end(H.bar_count, s_grid.cta == 0);
     if (s_grid.cta == 0 && threadIdx.x == 0) {
         const int idx = *H.log_count;
         if (idx < H.log_cap) {
@@ -988,11 +1044,18 @@ done:
     }
 }
 
+// The parameters are read through a reference throughout the solve: a copy in
+// shared memory, made once per CTA (a reference to the kernel parameter itself
+// would give every thread a copy of its own in local memory).
 __global__ void __launch_bounds__(512) k_helm_solve(HelmParams H) {
     extern __shared__ double smem_all[];
+    __shared__ HelmParams sH;
     if (threadIdx.x == 0) s_grid = SolveGrid{(int)blockIdx.x, (int)gridDim.x};
+    const int* src = reinterpret_cast<const int*>(&H);
+    int* dst = reinterpret_cast<int*>(&sH);
+    for (int t = threadIdx.x; t < (int)(sizeof(HelmParams) / sizeof(int)); t += blockDim.x) dst[t] = src[t];
     __syncthreads();
-    helm_solve_body(H, smem_all);
+    helm_solve_body(sH, smem_all);
 }
 
 // Several systems in one cooperative launch: system m runs on CTAs
@@ -1072,6 +1135,27 @@ static PwNode pairwise_build(long start, long n, std::vector<int>& leaves,
     if ((int)by_height.size() < height) by_height.resize(height);
     by_height[height - 1].push_back(make_int2(a.lo, b.lo));
     return {a.lo, height};
+}
+
+// P > 0 when the tree over the leaves is perfect -- 2^m leaves, the nodes of
+// height h (0: pairs of leaves) exactly (i, i + 2^h) for i a multiple of 2^(h+1)
+// -- with at least 32 leaves: the leaves per lane of perfect_fold for `warps`
+// warps (at most 16); 0 otherwise
+static int perfect_lanes(int n, const std::vector<std::vector<int2>>& by_height, int warps) {
+    if (n < 32 || (n & (n - 1)) != 0) return 0;
+    int m = 0;
+    while ((1 << m) < n) ++m;
+    if ((int)by_height.size() != m) return 0;
+    for (int h = 0; h < m; ++h) {
+        std::vector<int2> ops = by_height[h];
+        const int step = 1 << (h + 1);
+        if ((int)ops.size() != n / step) return 0;
+        std::sort(ops.begin(), ops.end(), [](int2 a, int2 b) { return a.x < b.x; });
+        for (int q = 0; q < (int)ops.size(); ++q)
+            if (ops[q].x != q * step || ops[q].y != q * step + (1 << h)) return 0;
+    }
+    const int P = std::max(1, n / (32 * warps));
+    return P <= 16 ? P : 0;
 }
 
 // leaves of NumPy's pairwise tree over n contiguous elements
@@ -1235,6 +1319,7 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     }
     H.n_leaves = (int)leaves.size() - 1;
     H.n_heights = (int)by_height.size();
+    H.perfect_lanes = H.big_fold ? 0 : perfect_lanes(H.n_leaves, by_height, block_ / 32);
     int* d_leaves = (int*)dalloc(sizeof(int) * leaves.size());
     int* d_hstart = (int*)dalloc(sizeof(int) * hstart.size());
     int2* d_ops = (int2*)dalloc(sizeof(int2) * std::max<size_t>(1, ops.size()));
@@ -1259,6 +1344,7 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
     H.ops = d_ops;
     H.n_ops = (int)ops.size();
     H.bar_count = bar;
+    H.wait_cycles = kBarrierCycles;
     size_t fold_doubles = (size_t)H.n_leaves;  // shared memory the fold needs
     if (H.big_fold) {
         H.n_blocks = (int)two.blocks.size();

@@ -42,6 +42,7 @@ struct HelmParams {
     const int2* ops;          // (lo, mid): value[lo] += value[mid]
     int n_ops;
     int ops_smem;             // doubles of shared memory holding a copy of ops and height_start (0: none)
+    int perfect_lanes;        // > 0: the tree is perfect, folded with this many leaves per lane (perfect_fold)
     double* leafA;
     double* leafB;
     double* leafC;
@@ -58,6 +59,7 @@ struct HelmParams {
     // grid barrier and status
     unsigned long long* bar_count;  // grid barrier arrivals (only grows)
     int* status;
+    long long wait_cycles;          // bound of a barrier wait in SM clock cycles
     // per-solve log
     int* log_iters;
     int* log_conv;
@@ -83,6 +85,8 @@ class HelmSolver {
     int* d_log_conv() const { return hp_.log_conv; }
     int* d_log_count() const { return hp_.log_count; }
     int grow_log(int cap, cudaStream_t s, std::string& err);
+    // bound of the solve's barrier waits in SM clock cycles (default ~1 s)
+    void set_wait_cycles(long long cycles) { hp_.wait_cycles = cycles; }
     // this solver's system for a batched launch (helm_batch_*): the parameters
     // of x = A^-1 rhs without the one-CTA-per-tile assumptions, and the dynamic
     // shared memory it needs

@@ -27,6 +27,30 @@ struct Nbr {
     __device__ __forceinline__ int at(int dj, int di) const { return jy[dj + 3] + ix[di + 3]; }
 };
 
+// asynchronous copy of one 4- or 8-byte element from global to shared memory
+// (cp.async: no register round trip, so a level plane's staging runs while the
+// previous level is computed); committed in groups, waited for by group
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T* sdst, const T* gsrc) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "cp.async copies 4, 8 or 16 bytes");
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gsrc), "n"(sizeof(T)) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N of this thread's committed groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// a column's values strided across the threads of a CTA in shared memory
+template <class T>
+struct StridedCol {
+    T* p;
+    int stride;
+    __device__ __forceinline__ T& operator[](int k) const { return p[k * stride]; }
+};
+
 #define COLUMN_PROLOGUE                                  \
     const int i = blockIdx.x * blockDim.x + threadIdx.x; \
     const int j = blockIdx.y * blockDim.y + threadIdx.y; \

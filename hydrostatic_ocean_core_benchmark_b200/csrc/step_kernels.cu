@@ -44,7 +44,11 @@ typedef double wide;
 // 128 threads, k_mom_column 512 and k_tracer_rhs 256 per CTA. The bits of the
 // results do not depend on them.
 #ifndef OC_MINB_CLOSURE
+#ifdef OC_MIXED
+#define OC_MINB_CLOSURE 4
+#else
 #define OC_MINB_CLOSURE 8
+#endif
 #endif
 #ifndef OC_MINB_MOM
 #define OC_MINB_MOM 2
@@ -152,12 +156,25 @@ __global__ void __launch_bounds__(128, OC_MINB_CLOSURE) k_closure(KPR P, const r
                                                  const wide* __restrict__ b,
                                                  real* __restrict__ e, real* __restrict__ km,
                                                  real* __restrict__ kh, real* __restrict__ q) {
+#ifdef OC_MIXED
+    // FP32 build: N^2 of the column on its interfaces, which the Gaspar length
+    // marches read O(nz) times per interface, lives in shared memory: interface k
+    // of the CTA's thread t at [k * threads + t] (dynamic, (nz + 1) x threads
+    // values). Measured at 512 x 512 x 50: 0.52 against 0.57 ms for the local
+    // array; the fp64 build keeps the local array (0.81 against 1.07 ms).
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    const StridedCol<real> nn2{reinterpret_cast<real*>(s_dyn) + threadIdx.y * blockDim.x + threadIdx.x,
+                               (int)(blockDim.x * blockDim.y)};
+#endif
     COLUMN_PROLOGUE
     const int nz = P.nz;
     const int c = nb.c;
     const size_t cw = nb.at(0, -1), cs_ = nb.at(-1, 0);
     const ColGeoR g = ColGeoR::load(P, c);
-    real nn2[NZM + 1], sh2[NZM + 1], lk[NZM + 1], le[NZM + 1], cst[NZM + 1];
+#ifndef OC_MIXED
+    real nn2[NZM + 1];
+#endif
+    real sh2[NZM + 1], lk[NZM + 1], le[NZM + 1], cst[NZM + 1];
     real depth = real(0.0);
     for (int k = 0; k < nz; ++k) {
         real m;
@@ -663,7 +680,7 @@ __global__ void __launch_bounds__(MOM_TX * MOM_TY * 2, OC_MINB_MOM) k_mom_column
     real* __restrict__ avpu, real* __restrict__ dzu, real* __restrict__ dzv,
     real* __restrict__ stu, real* __restrict__ stv) {
     __shared__ int s_g[MOM_RN], s_ku[MOM_RN], s_kv[MOM_RN];
-    __shared__ real s_u[MOM_RN], s_v[MOM_RN];
+    __shared__ real s_u[2][MOM_RN], s_v[2][MOM_RN];  // level planes, double-buffered
     // threadIdx.z selects the component: 0 the u terms at the column's east face,
     // 1 the v terms at its north face (whole warps, so no divergence)
     const int tx = threadIdx.x, ty = threadIdx.y, comp = threadIdx.z;
@@ -725,17 +742,33 @@ __global__ void __launch_bounds__(MOM_TX * MOM_TY * 2, OC_MINB_MOM) k_mom_column
             df = diff_flux(km[(size_t)kbeg * n2 + c], x_m1, x_0, dz_m1, dz_0, bot);
         }
     }
+    // level k's u and v of the region go to buffer (k - kbeg) & 1; level k + 1's
+    // copies are in flight while level k is computed (each thread copies the
+    // region cells whose s_g it wrote itself)
+    auto stage = [&](int k) {
+        const size_t o = (size_t)k * n2;
+        const int buf = (k - kbeg) & 1;
+        for (int r = tid; r < MOM_RN; r += nthreads) {
+            cp_async_elem(&s_u[buf][r], u + o + s_g[r]);
+            cp_async_elem(&s_v[buf][r], v + o + s_g[r]);
+        }
+        cp_async_commit();
+    };
+    stage(kbeg);
     for (int k = kbeg; k < kend; ++k) {
         const size_t o = (size_t)k * n2;
-        // stage the level's u and v of the region (the previous level is done)
+        // every thread is done with the previous level, whose buffer level k + 1 takes
         __syncthreads();
-        for (int r = tid; r < MOM_RN; r += nthreads) {
-            s_u[r] = u[o + s_g[r]];
-            s_v[r] = v[o + s_g[r]];
+        if (k + 1 < kend) {
+            stage(k + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
         if (!live) continue;
-        const TileLevel lv{s_u, s_v, s_ku, s_kv, rc, k};
+        const int buf = (k - kbeg) & 1;
+        const TileLevel lv{s_u[buf], s_v[buf], s_ku, s_kv, rc, k};
         const real x_p2 = Xc(k + 2);
         const real dz_p1 = dzf_at(k + 1);
         const real K_1 = km[o + n2 + c];
@@ -1035,9 +1068,13 @@ __global__ void __launch_bounds__(TRX * TRY, OC_MINB_TRACER) k_tracer_rhs(KPR P,
     // The tile's columns plus a 2-column ring: flat 2D index and compact geometry
     // (once), then each level's tracers and face velocities (staged per level)
     constexpr int RX = TRX + 4, RY = TRY + 4, RNC = RX * RY;
-    __shared__ int s_g[RNC], s_kf[RNC], s_kb[RNC], s_ku[RNC], s_kv[RNC];
+    // level indices are at most 128: the column's (kf, kb) and its faces' wet
+    // levels (ku, kv) fit one byte each
+    __shared__ int s_g[RNC];
+    __shared__ uchar4 s_k[RNC];
     __shared__ real s_d0[RNC], s_d1[RNC];
-    __shared__ real s_f[2][RNC], s_u[RNC], s_v[RNC];
+    // level planes, double-buffered: [buffer][field] tracers, [buffer] face velocities
+    __shared__ real s_f[2][2][RNC], s_u[2][RNC], s_v[2][RNC];
     __shared__ real sfx[2][TRY][TRX + 1];  // [field][row][west face of column]
     __shared__ real sfy[2][TRY + 1][TRX];  // [field][south face of row][column]
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -1064,22 +1101,20 @@ __global__ void __launch_bounds__(TRX * TRY, OC_MINB_TRACER) k_tracer_rhs(KPR P,
         const int2 ki = P.kinfo[gc], kfc = P.kface[gc];
         const auto dx = P.dzx[gc];
         s_g[r] = gc;
-        s_kf[r] = ki.x;
-        s_kb[r] = ki.y;
-        s_ku[r] = kfc.x;
-        s_kv[r] = kfc.y;
+        s_k[r] = make_uchar4((unsigned char)ki.x, (unsigned char)ki.y, (unsigned char)kfc.x, (unsigned char)kfc.y);
         s_d0[r] = dx.x;
         s_d1[r] = dx.y;
     }
     // thickness and wet flag of region column r at level k (col_dz from the staged geometry)
     auto sdz = [&](int r, int k, real& m3) {
-        if (k >= s_kb[r]) {
+        const uchar4 q = s_k[r];
+        if (k >= q.y) {
             m3 = real(0.0);
             return real(0.0);
         }
         m3 = real(1.0);
-        if (k < s_kf[r]) return P.dzr[k];
-        return k == s_kf[r] ? s_d0[r] : s_d1[r];
+        if (k < q.x) return P.dzr[k];
+        return k == q.x ? s_d0[r] : s_d1[r];
     };
     // flux through a face with stencil cells (cm, c0, c1, cp) of the region,
     // normal velocity vel and face wet levels kfa (tracer_flux from shared memory)
@@ -1091,8 +1126,8 @@ __global__ void __launch_bounds__(TRX * TRY, OC_MINB_TRACER) k_tracer_rhs(KPR P,
         if (P.advection == 1)
             val = real(0.5) * (a + b);
         else if (P.advection >= 3)
-            val = kappa_face(P, F[cm], a, b, F[cp], vel, k < s_kb[cm] ? real(1.0) : real(0.0), k < s_kb[cp] ? real(1.0) : real(0.0),
-                             P.advection == 4);
+            val = kappa_face(P, F[cm], a, b, F[cp], vel, k < s_k[cm].y ? real(1.0) : real(0.0),
+                             k < s_k[cp].y ? real(1.0) : real(0.0), P.advection == 4);
         else
             val = vel > real(0.0) ? a : b;
         return dzf * vel * val;
@@ -1117,28 +1152,46 @@ __global__ void __launch_bounds__(TRX * TRY, OC_MINB_TRACER) k_tracer_rhs(KPR P,
         w_k = w[(size_t)kbeg * n2 + c];
         kh_k = kh[(size_t)kbeg * n2 + c];
     }
+    // level k's planes go to buffer (k - kbeg) & 1; level k + 1's copies are in
+    // flight while level k is computed (each thread copies the region cells
+    // whose s_g it wrote itself)
+    auto stage = [&](int k) {
+        const size_t o = (size_t)k * n2;
+        const int buf = (k - kbeg) & 1;
+        for (int r = tid; r < RNC; r += TRX * TRY) {
+            const size_t g = o + s_g[r];
+            cp_async_elem(&s_f[buf][0][r], C0 + g);
+            if (ts) cp_async_elem(&s_f[buf][1][r], S + g);
+            cp_async_elem(&s_u[buf][r], u + g);
+            cp_async_elem(&s_v[buf][r], v + g);
+        }
+        cp_async_commit();
+    };
+    if (adv) stage(kbeg);
     for (int k = kbeg; k < kend; ++k) {
         const size_t o = (size_t)k * n2;
         if (adv) {
-            // stage the level (the previous level's faces and cells are done)
+            // every thread is done with the previous level, whose buffer level k + 1 takes
             __syncthreads();
-            for (int r = tid; r < RNC; r += TRX * TRY) {
-                const size_t g = o + s_g[r];
-                s_f[0][r] = C0[g];
-                if (ts) s_f[1][r] = S[g];
-                s_u[r] = u[g];
-                s_v[r] = v[g];
+            if (k + 1 < kend) {
+                stage(k + 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
             }
             __syncthreads();
+            const int buf = (k - kbeg) & 1;
+            const real* su = s_u[buf];
+            const real* sv = s_v[buf];
 #pragma unroll 1
             for (int f = 0; f < nf; ++f) {
-                const real* F = s_f[f];
+                const real* F = s_f[buf][f];
                 // west face of this cell (cells rc-2 .. rc+1), south face (rc-2RX .. rc+RX)
-                sfx[f][ty][tx] = sflux(F, rc - 2, rc - 1, rc, rc + 1, s_u[rc - 1], s_ku[rc - 1], k);
-                sfy[f][ty][tx] = sflux(F, rc - 2 * RX, rc - RX, rc, rc + RX, s_v[rc - RX], s_kv[rc - RX], k);
-                if (xextra) sfx[f][tx][TRX] = sflux(F, rce - 1, rce, rce + 1, rce + 2, s_u[rce], s_ku[rce], k);
+                sfx[f][ty][tx] = sflux(F, rc - 2, rc - 1, rc, rc + 1, su[rc - 1], s_k[rc - 1].z, k);
+                sfy[f][ty][tx] = sflux(F, rc - 2 * RX, rc - RX, rc, rc + RX, sv[rc - RX], s_k[rc - RX].w, k);
+                if (xextra) sfx[f][tx][TRX] = sflux(F, rce - 1, rce, rce + 1, rce + 2, su[rce], s_k[rce].z, k);
                 if (yextra)
-                    sfy[f][TRY][tx] = sflux(F, rcn - RX, rcn, rcn + RX, rcn + 2 * RX, s_v[rcn], s_kv[rcn], k);
+                    sfy[f][TRY][tx] = sflux(F, rcn - RX, rcn, rcn + RX, rcn + 2 * RX, sv[rcn], s_k[rcn].w, k);
             }
             __syncthreads();
         }
@@ -1343,9 +1396,26 @@ __global__ void k_transport(KPR P, const real* __restrict__ u, const real* __res
 void launch_qsolve(const KPR& P, const real* km, real* q, cudaStream_t s) {
     NZ_DISPATCH(P.nz, (k_qsolve<NZM><<<col_grid(P), col_block(), 0, s>>>(P, km, q)));
 }
+template <int NZM>
+static void closure_nzm(const KPR& P, const real* u, const real* v, const wide* b, real* e, real* km, real* kh,
+                        real* q, cudaStream_t s) {
+    const dim3 blk = col_block();
+#ifdef OC_MIXED
+    const size_t smem = (size_t)(P.nz + 1) * blk.x * blk.y * sizeof(real);
+    static bool opted = false;  // above 48 KB a kernel's dynamic shared memory is opt-in
+    if (!opted) {
+        cudaFuncSetAttribute(k_closure<NZM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)((size_t)(NZM + 1) * blk.x * blk.y * sizeof(real)));
+        opted = true;
+    }
+#else
+    const size_t smem = 0;
+#endif
+    k_closure<NZM><<<col_grid(P), blk, smem, s>>>(P, u, v, b, e, km, kh, q);
+}
 void launch_closure(const KPR& P, const real* u, const real* v, const wide* b, real* e,
                     real* km, real* kh, real* q, cudaStream_t s) {
-    NZ_DISPATCH(P.nz, (k_closure<NZM><<<col_grid(P), col_block(), 0, s>>>(P, u, v, b, e, km, kh, q)));
+    NZ_DISPATCH(P.nz, (closure_nzm<NZM>(P, u, v, b, e, km, kh, q, s)));
 }
 void launch_kukv(const KPR& P, const real* q, wide* Ku, wide* Kv, cudaStream_t s) {
     k_kukv<<<col_grid(P), col_block(), 0, s>>>(P, q, Ku, Kv);

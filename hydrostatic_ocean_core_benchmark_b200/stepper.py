@@ -245,6 +245,10 @@ class OceanStepper:
         sp = getattr(stream, "cuda_stream", stream)
         self._call("oc_unpack_rows", self.lib.oc_unpack_rows, self.h, int(j0), int(nrows), ptr, sp)
 
+    def set_wait_bound(self, cycles: int):
+        """Bound of the solve's device-side waits in SM clock cycles (oc_set_wait_bound)."""
+        self._call("oc_set_wait_bound", self.lib.oc_set_wait_bound, self.h, int(cycles))
+
     def reset_mixing(self):
         self._call("oc_reset_mixing", self.lib.oc_reset_mixing, self.h)
 

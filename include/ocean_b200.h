@@ -53,8 +53,9 @@ enum { OC_SOLVER_PCG_JACOBI = 0, OC_SOLVER_PCG_RBGS = 1, OC_SOLVER_RBGS = 2, OC_
  * inner PCG-Jacobi inside FP64 iterative refinement */
 enum { OC_SOLVER_PCG_REFINED = 4 };
 /* no reference counterpart: CG preconditioned by one symmetric V(2,2) cycle of
- * the multigrid hierarchy, fp64. The mixed-precision step solves with it where
- * the configuration names multigrid; the standalone solver offers it too. */
+ * the multigrid hierarchy, fp64, for the step (either precision, through the C
+ * ABI and Python; the namelist protocol keeps the reference's four) and the
+ * standalone solver. */
 enum { OC_SOLVER_PCG_MG = 5 };
 enum { OC_BC_PERIODIC = 0, OC_BC_CLOSED = 1 };
 enum { OC_FACE_MIN = 0, OC_FACE_MEAN = 1, OC_FACE_HARMONIC = 2 };
@@ -268,6 +269,15 @@ int oc_get_solve_log(oc_handle* h, int32_t* iterations, int32_t capacity, int32_
 
 /* Zero the counters and the solve log (the state is kept). */
 int oc_reset_stats(oc_handle* h);
+
+/* Bound of the step's device-side waits (the grid barriers of its Helmholtz
+ * solve) in SM clock cycles; the default, 2e9, is about 1 s. A wait that runs
+ * out sets OC_ERR_TIMEOUT in the handle's status, every CTA leaves the solve and
+ * the next synchronous call (oc_get_state, oc_get_stats) returns it; the status
+ * stays set. A bound of a few hundred cycles makes the waits run out, which is
+ * how the failure path is tested. Recorded graphs are dropped. No reference
+ * counterpart: the reference's solves have no device-side waits. */
+int oc_set_wait_bound(oc_handle* h, int64_t cycles);
 
 /* One Helmholtz solve with the current face coefficients: x = A^-1 rhs on
  * device buffers [ny][nx]. *iterations receives the count (synchronises). */

@@ -62,6 +62,7 @@ def test_entry_points_refuse_null_arguments_without_a_gpu():
         "oc_set_state_async": lambda: lib.oc_set_state_async(None, None, 0, None),
         "oc_reset_mixing": lambda: lib.oc_reset_mixing(None),
         "oc_bind_state": lambda: lib.oc_bind_state(None, None, None),
+        "oc_set_wait_bound": lambda: lib.oc_set_wait_bound(None, 1000),
         "oc_state_parity": lambda: lib.oc_state_parity(None, None),
         "oc_get_state": lambda: lib.oc_get_state(None, None, 0),
         "oc_get_state_async": lambda: lib.oc_get_state_async(None, None, 0, None),

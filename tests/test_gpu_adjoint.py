@@ -1,21 +1,22 @@
 """The hand-written adjoint of the step (oc_adjoint_step) on the GPU.
 
-Pins, as the north star of the differentiation form asks: a float64 torch
-restatement of the step (tests/torch_step.py, whose forward matches the
-oracle) differentiated by torch.autograd, and centred finite differences of
-the GPU forward (epsilon = 1e-6, seeded random directions). The objective is
-the volume-weighted mean temperature of the top three levels after the run;
-the inputs are the initial temperature and the surface x-stress field.
-The configuration is the benchmark recipe with the closure off (the adjoint's
-scope): stretched levels, double-gyre wind field, polyTEOS10, theta = 0.6 +
-multigrid, with the TVD3 advection or its unlimited kappa = 1/3 form.
+Two pins: a float64 torch restatement of the step (tests/torch_step.py, whose
+forward matches the oracle) differentiated by torch.autograd, and centred
+finite differences of the GPU forward (epsilon = 1e-6, seeded random
+directions). The objective is the volume-weighted mean temperature of the top
+three levels after the run; the inputs are the initial temperature and the
+surface x-stress field. The configuration is the benchmark recipe with the
+closure off (the adjoint's scope): stretched levels, double-gyre wind field,
+polyTEOS10, theta = 0.6 + multigrid, with the TVD3 advection, its unlimited
+kappa = 1/3 form or centred advection.
 
-The adjoint is the exact derivative of the step with the limiter branches the
-forward values select (torch.autograd agrees to ~1e-9). With TVD advection the
-step itself is not differentiable: random directions at epsilon = 1e-6 move a
-fraction of ~1e-4 of the faces across a kink of the Superbee limiter, so the
-finite differences of the TVD step agree to ~1e-3 only; the unlimited
-advection is differentiable and agrees to 1e-6.
+The adjoint is the exact derivative of the step with the branches the forward
+values select (torch.autograd agrees to ~1e-9). The step is smooth only with
+centred advection, whose finite differences agree to 1e-6. The kappa = 1/3
+faces switch their upwind side where a velocity changes sign, and the TVD faces
+also at the kinks of the Superbee limiter: random directions at epsilon = 1e-6
+carry some faces across those switches, so the finite differences of those
+forms agree to ~1e-4 and ~1e-3.
 """
 
 import numpy as np
@@ -33,10 +34,10 @@ def _cuda():
     torch.cuda.set_device(0)
 
 
-def _setup(nx, ny, nz, seed, steps, every, advection="up3_tvd"):
+def _setup(nx, ny, nz, seed, steps, every, advection="up3_tvd", **over):
     import torch
     from hydrostatic_ocean_core_benchmark_b200.adjoint import OceanRollout
-    s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=seed, closure="none", advection=advection)
+    s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=seed, closure="none", advection=advection, **over)
     ro = OceanRollout(s.params, s.H, s.mask, dzr=s.dzr, n_steps=steps, every=every)
     dev = "cuda:0"
     T = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)  # noqa: E731
@@ -83,13 +84,18 @@ def test_adjoint_matches_torch_autograd_of_the_restated_step(advection):
     rel_T = float(torch.linalg.vector_norm(gT - T0r.grad) / torch.linalg.vector_norm(T0r.grad))
     rel_tau = float(torch.linalg.vector_norm(gtau - txr.grad) / torch.linalg.vector_norm(txr.grad))
     print(f"adjoint vs autograd ({advection}): T0 {rel_T:.3e}, tau {rel_tau:.3e}")
-    assert rel_T < 1e-8 and rel_tau < 1e-6, (rel_T, rel_tau)
+    # the restatement's forward agrees with the GPU's to ~1e-12, not bit for bit, so
+    # near a kink of the Superbee limiter the two can take different branches; with
+    # TVD advection the stress gradient then agrees to a few 1e-6 (measured 1.6e-6)
+    bound_tau = 5e-6 if advection == "up3_tvd" else 1e-6
+    assert rel_T < 1e-8 and rel_tau < bound_tau, (rel_T, rel_tau)
     ro.close()
 
 
 @pytest.mark.parametrize("nx,ny,nz,steps,every,ndir,advection,bound", [
-    (40, 32, 10, 6, 3, 8, "up3", 1e-6),
-    (256, 256, 32, 20, 5, 32, "up3", 1e-6),
+    (40, 32, 10, 6, 3, 8, "centered2", 1e-6),
+    (256, 256, 32, 20, 5, 32, "centered2", 1e-6),
+    (256, 256, 32, 20, 5, 32, "up3", 3e-4),
     (256, 256, 32, 20, 5, 32, "up3_tvd", 5e-3),
 ])
 def test_adjoint_agrees_with_centred_finite_differences(nx, ny, nz, steps, every, ndir, advection, bound):
@@ -98,7 +104,11 @@ def test_adjoint_agrees_with_centred_finite_differences(nx, ny, nz, steps, every
     config-4 size is 256 x 256 x 32, 20 steps, checkpoints every 5 steps, 32
     directions."""
     import torch
-    s, ro, fixed, T0, taux, w = _setup(nx, ny, nz, 11, steps=steps, every=every, advection=advection)
+    # the forward's Helmholtz solves to rtol 1e-14: a solve stopped at rtol r moves
+    # eta by up to ~r |eta| in a way that is not smooth in the inputs, which the
+    # difference quotient divides by eps (1e-12 / 1e-6 would leave ~1e-6 of noise)
+    s, ro, fixed, T0, taux, w = _setup(nx, ny, nz, 11, steps=steps, every=every, advection=advection,
+                                       rtol=1e-14, max_iter=400)
     gT, gtau, _ = _grad(ro, fixed, T0, taux, w)
     gen = torch.Generator(device="cuda:0").manual_seed(2026)
     eps = 1e-6
@@ -114,5 +124,6 @@ def test_adjoint_agrees_with_centred_finite_differences(nx, ny, nz, steps, every
         worst = max(worst, abs(fd - ad) / abs(ad))
     del m3
     print(f"adjoint vs finite differences ({advection}, {nx}x{ny}x{nz}, {ndir} directions): worst {worst:.3e}")
+    assert ro.st.stats()["solver_failures"] == 0
     assert worst < bound, worst
     ro.close()

@@ -93,3 +93,30 @@ def test_max_iter_one_counts_solver_failures(tmp_path, solver):
     assert st.solve_log() == ref.solve_log
     assert np.array_equal(st.get_state(fields=("eta",))["eta"], state.eta)
     st.close()
+
+
+def test_a_barrier_wait_that_runs_out_returns_timeout_and_the_device_stays_usable():
+    """The solve's grid barriers spin with a bound; a bound of 200 cycles runs
+    out on the first barrier a CTA reaches before the others. Every CTA then
+    leaves the solve, the handle reports OC_ERR_TIMEOUT, and a fresh handle on
+    the same device steps normally."""
+    from hydrostatic_ocean_core_benchmark_b200._lib import OceanError
+    from hydrostatic_ocean_core_benchmark_b200.stepper import OceanStepper
+    s = cases.seamount_basin(nx=128, ny=128, nz=6, seed=7)
+
+    def fresh():
+        st = OceanStepper(s.params, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+        st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
+        return st
+
+    st = fresh()
+    st.set_wait_bound(200)
+    st.step(1)
+    with pytest.raises(OceanError, match="timed out"):
+        st.stats()
+    st.close()
+    ok = fresh()
+    ok.step(2)
+    stats = ok.stats()
+    assert stats["device_status"] == 0 and stats["solver_failures"] == 0 and not stats["diverged"]
+    ok.close()

@@ -2,8 +2,7 @@
 
 The mixed path keeps the 3D state and stencils in FP32 and the buoyancy, the
 pressure gradient, the EOS, the surface elevation and the Helmholtz solve in
-fp64; where the configuration names the stationary multigrid it solves by
-MG-preconditioned CG to the same fp64 tolerance. It has no reference
+fp64 (the configured solver, to the same fp64 tolerance). It has no reference
 counterpart, so its pins are the oracle (the fp64 path equals it bit for bit)
 and the error bounds below, measured on the benchmark recipe: relative L2 of
 every field against the oracle after a run.

@@ -1,6 +1,6 @@
 """The float64 torch restatement of the step (the adjoint's reference
-gradient) against the oracle, on CPU: the north star asks that the torch
-reference's forward match the oracle before its gradient is trusted."""
+gradient) against the oracle, on CPU: the restatement's forward must match the
+oracle before its gradient is trusted."""
 
 import numpy as np
 
