@@ -159,10 +159,13 @@ def mg_level_cells(nx, ny, min_size=8):
 def helm_bytes_per_iteration(p):
     """Algorithmic bytes of one Helmholtz iteration: PCG-Jacobi 15 arrays per
     column, MG V(2,2) 32 arrays per cell of every level plus 4 fine arrays for the
-    residual check."""
+    residual check, MG-preconditioned CG the V-cycle plus 13 fine arrays (A p, the
+    updates of x, r, p and the copies around the cycle)."""
     n0 = p.nx * p.ny
     if p.solver_kind == "multigrid":
         return 8 * (32 * sum(mg_level_cells(p.nx, p.ny)) + 4 * n0)
+    if p.solver_kind == "pcg_mg":
+        return 8 * (32 * sum(mg_level_cells(p.nx, p.ny)) + 13 * n0)
     return 8 * 15 * n0
 
 
@@ -267,7 +270,7 @@ def run_reference_arm(args, rank):
 MIXED_FIELDS = ("eta", "u", "v", "b", "T", "S", "e", "km", "kh")
 
 
-def precision_leg(s, local_rank, steps, warmup, time_fp64=False):
+def precision_leg(s, local_rank, steps, warmup, time_fp64=False, mixed_solver="configured"):
     """The mixed-precision step beside the fp64 one on the same initial state.
 
     Both advance warmup + steps steps (two-step CUDA graphs) from the state of
@@ -283,7 +286,8 @@ def precision_leg(s, local_rank, steps, warmup, time_fp64=False):
     out, rate, ms, logs = {}, {}, {}, {}
     stream = torch.cuda.Stream(device=local_rank)
     for prec in ("fp64", "mixed"):
-        st = OceanStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c, device=local_rank,
+        pp = p if prec == "fp64" or mixed_solver == "configured" else p.replace(solver_kind=mixed_solver)
+        st = OceanStepper(pp, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c, device=local_rank,
                           precision=prec)
         st.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
         st.step(warmup, stream=stream, graph=True)
@@ -312,10 +316,13 @@ def precision_leg(s, local_rank, steps, warmup, time_fp64=False):
         den = float(torch.linalg.vector_norm(b))
         rel[f] = float(torch.linalg.vector_norm(a - b)) / den if den > 0 else float(torch.linalg.vector_norm(a))
     la, lb = logs["fp64"], logs["mixed"]
+    msolver = p.solver_kind if mixed_solver == "configured" else mixed_solver
     leg = {"steps": warmup + steps, "timed_steps": steps, "ms_per_step": ms["mixed"], "value": rate["mixed"],
            "unit": UNIT, "rel_l2_vs_fp64": rel, "worst_field": max(rel, key=rel.get),
-           "multigrid_cycles": {"fp64": sum(la), "mixed": sum(lb), "solves": len(lb),
-                                "max_per_solve_difference": max((abs(x - y) for x, y in zip(la, lb)), default=0)}}
+           "solvers": {"fp64": p.solver_kind, "mixed": msolver},
+           "solver_iterations": {"fp64": sum(la), "mixed": sum(lb), "solves": len(lb)}}
+    if msolver == p.solver_kind:
+        leg["solver_iterations"]["max_per_solve_difference"] = max((abs(x - y) for x, y in zip(la, lb)), default=0)
     if time_fp64:
         leg["fp64"] = {"ms_per_step": ms["fp64"], "value": rate["fp64"]}
         leg["speedup_vs_fp64"] = ms["fp64"] / ms["mixed"]
@@ -333,7 +340,7 @@ def run_precision(args, rank, world, local_rank):
         return 0
     s = workload(args)
     p = s.params
-    leg = precision_leg(s, local_rank, args.steps, args.warmup, time_fp64=True)
+    leg = precision_leg(s, local_rank, args.steps, args.warmup, time_fp64=True, mixed_solver=args.mixed_solver)
     line = {"metric": "cell-steps/s, mixed FP32/FP64 step vs fp64 (rel L2 vs fp64 per field)",
             "value": leg["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": leg["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -343,7 +350,8 @@ def run_precision(args, rank, world, local_rank):
                                    f"theta={p.theta:g} + {p.solver_kind}, dt={p.dt:g} s",
                        "cells": p.nx * p.ny * p.nz, "variant": "precision form (mixed vs fp64)"},
             "fp64": leg["fp64"], "speedup_vs_fp64": leg["speedup_vs_fp64"],
-            "rel_l2_vs_fp64": leg["rel_l2_vs_fp64"], "multigrid_cycles": leg["multigrid_cycles"]}
+            "rel_l2_vs_fp64": leg["rel_l2_vs_fp64"], "solvers": leg["solvers"],
+            "solver_iterations": leg["solver_iterations"]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -546,7 +554,7 @@ def run_ours(args, rank, world, local_rank):
     # run from the same initial state (errors per field against the fp64 path)
     mixed = None
     if args.mixed_steps > 0:
-        mixed = precision_leg(s, local_rank, args.mixed_steps, args.warmup)
+        mixed = precision_leg(s, local_rank, args.mixed_steps, args.warmup, mixed_solver=args.mixed_solver)
         mixed["speedup_vs_fp64"] = (ms_max / args.steps) / mixed["ms_per_step"]
         mixed["fp64_ms_per_step"] = ms_max / args.steps
 
@@ -616,9 +624,10 @@ def run_ensemble(args, rank, world, local_rank):
         else:
             nx, ny = (32 * int(x) for x in rng.integers(4, 13, 2))
         nz = int(rng.choice([24, 32, 48]))
-        # the multigrid halves a grid only while its sizes are even: sizes with an
-        # odd factor above 8 take PCG-Jacobi
-        solver = "multigrid" if nx % 32 == 0 and ny % 32 == 0 else "pcg_jacobi"
+        # the stationary multigrid halves a grid only while its sizes are even, and on
+        # a large odd coarsest level it needs thousands of cycles: other sizes take CG
+        # preconditioned by the same V-cycle (pcg_mg)
+        solver = "multigrid" if nx % 32 == 0 and ny % 32 == 0 else "pcg_mg"
         s = cases.seamount_basin(nx=nx, ny=ny, nz=nz, seed=args.seed + 1000 * (rank + 1) + m, solver_kind=solver)
         st = OceanStepper(s.params, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c,
                           device=local_rank, precision=prec)
@@ -633,7 +642,8 @@ def run_ensemble(args, rank, world, local_rank):
             tw.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
             twins.append((m, tw))
     cells = sum(nx * ny * nz for nx, ny, nz in shapes)
-    tiling = [st.autotune() for st in members]
+    # the autotuner times the fp64 kernels; mixed members keep the default tiling
+    tiling = [st.autotune() for st in members] if prec == "fp64" else []
     stream = torch.cuda.Stream(device=local_rank)
     steps = args.steps + (args.steps % 2)
     warm = max(args.warmup, 3)
@@ -696,8 +706,8 @@ def run_ensemble(args, rank, world, local_rank):
             "data": "synthetic (seeded seamount-basin recipe per member; inputs generated on the host)",
             "config": {"workload": f"ensemble of {len(members)} seamount basins, nx, ny "
                                    + ("uniform in 128..384" if args.ens_sizes == "any" else "multiples of 32 in 128..384")
-                                   + ", nz in {24, 32, 48}, theta=0.6 + multigrid (PCG-Jacobi on sizes the multigrid "
-                                   "cannot halve), TKE, TVD3, polyTEOS10",
+                                   + ", nz in {24, 32, 48}, theta=0.6 + multigrid (MG-preconditioned CG on sizes the "
+                                   "multigrid cannot halve to 8), TKE, TVD3, polyTEOS10",
                        "members": len(members), "cells": cells, "precision": prec,
                        "solvers": {k: solvers.count(k) for k in sorted(set(solvers))},
                        "grids": [list(g) for g in shapes[:8]] + (["..."] if len(shapes) > 8 else []),
@@ -706,7 +716,7 @@ def run_ensemble(args, rank, world, local_rank):
                            "ms_per_step": ms_seq / steps,
                            "path": "members one after another, each with its own recorded graphs"},
             "tiling": {"levels_per_cta_momentum": sorted(set(t[0] for t in tiling)),
-                       "levels_per_cta_tracers": sorted(set(t[1] for t in tiling))},
+                       "levels_per_cta_tracers": sorted(set(t[1] for t in tiling))} if tiling else "default",
             "clocks": clk}
     if hbm:
         line["roofline"] = hbm
@@ -932,6 +942,9 @@ def main():
                          "--steps steps)")
     ap.add_argument("--mixed-steps", type=int, default=100,
                     help="timed steps of the mixed-precision leg of the headline line (0: skip it)")
+    ap.add_argument("--mixed-solver", choices=["configured", "pcg_refined", "pcg_mg"], default="configured",
+                    help="Helmholtz solver of the mixed-precision step (configured: the recipe's multigrid; "
+                         "pcg_refined needs ~600 inner iterations per solve on the recipe's systems)")
     ap.add_argument("--ens-members", type=int, default=64)
     ap.add_argument("--ens-sizes", choices=["mult32", "any"], default="mult32",
                     help="member nx, ny: multiples of 32 in 128..384, or any integer in 128..384")

@@ -18,7 +18,7 @@ ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "unsupported option", 4: "c
           5: "device-side wait timed out", 6: "I/O error", 7: "request above a fixed buffer size"}
 
 SCHEMES = {"fb": 0, "theta": 1, "split_explicit": 2}
-SOLVERS = {"pcg_jacobi": 0, "pcg_rbgs": 1, "rbgs": 2, "multigrid": 3, "pcg_mg": 5}
+SOLVERS = {"pcg_jacobi": 0, "pcg_rbgs": 1, "rbgs": 2, "multigrid": 3, "pcg_refined": 4, "pcg_mg": 5}
 BCS = {"periodic": 0, "closed": 1}
 FACE_RULES = {"min": 0, "mean": 1, "harmonic": 2}
 EOS = {"linear": 0, "seos": 1, "teos10": 2}

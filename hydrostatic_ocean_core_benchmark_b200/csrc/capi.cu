@@ -99,8 +99,9 @@ int validate(const oc_config* c, std::string& err) {
         return err = "theta must lie in (0,1]", OC_ERR_ARG;
     if (c->n_picard < 1) return err = "n_picard must be >= 1", OC_ERR_ARG;
     if (!(c->dt > 0.0)) return err = "dt must be > 0", OC_ERR_ARG;
-    if (c->solver < 0 || (c->solver > 3 && c->solver != OC_SOLVER_PCG_MG))
-        return err = "unknown Helmholtz solver", OC_ERR_ARG;
+    if (c->solver < 0 || c->solver > OC_SOLVER_PCG_MG) return err = "unknown Helmholtz solver", OC_ERR_ARG;
+    if (c->solver == OC_SOLVER_PCG_REFINED && c->precision != OC_PRECISION_MIXED)
+        return err = "the FP32-inner refined solver serves the mixed-precision step only", OC_ERR_ARG;
     if (c->max_iter < 1) return err = "max_iter must be >= 1", OC_ERR_ARG;
     if (c->bc_x < 0 || c->bc_x > 1 || c->bc_y < 0 || c->bc_y > 1)
         return err = "bc must be periodic|closed (open boundaries are not supported)", OC_ERR_UNSUPPORTED;
@@ -1288,9 +1289,13 @@ struct oc_ensemble {
     std::vector<oc_handle::Counters> delta;     // each member's counter increments per replay
     int device = 0;
     std::string err;
-    // one cooperative launch per solve of the recorded steps, every member's system
-    // at once, when all members run the theta scheme with the same Picard count
+    // batched solves, when all members run the theta scheme with the same Picard
+    // count: the members fall into groups whose systems fill the GPU together
+    // (groups[g] lists its members); each solve of the recorded steps is one
+    // cooperative launch per group, the groups one after another. plans[q * G + g]
+    // is group g's launch for solve q.
     bool batched = false;
+    std::vector<std::vector<int>> groups;
     std::vector<oc::HelmBatch> plans;
     ~oc_ensemble() {
         for (auto& b : plans) oc::helm_batch_free(b);
@@ -1351,24 +1356,42 @@ int ensemble_record(oc_ensemble* e) {
         batched = h->solver && h->cfg.scheme == OC_SCHEME_THETA && h->cfg.n_picard == e->members[0]->cfg.n_picard;
     }
     std::string why;
+    e->groups.clear();
     if (batched) {
-        const int np = e->members[0]->cfg.n_picard;
-        std::vector<HelmSolver*> sv(n);
-        std::vector<const double*> rh(n);
-        std::vector<double*> xs(n);
-        for (int q = 0; q < 2 * np && batched; ++q) {
-            for (size_t m = 0; m < n; ++m) {
-                oc_handle* h = e->members[m];
-                sv[m] = h->solver;
-                rh[m] = h->rhs2;
-                xs[m] = h->ETA[q < np ? 1 - h->cur : h->cur];
+        // groups: members in order, each group's preferred CTAs (a member's solve
+        // keeps about one CTA per 2048 cells of its grid busy) adding up to at most
+        // the batched launch's grid
+        const int grid = helm_batch_grid();
+        int used = 0;
+        for (size_t m = 0; m < n; ++m) {
+            const int want = e->members[m]->solver->preferred_ctas();
+            if (e->groups.empty() || used + want > grid) {
+                e->groups.emplace_back();
+                used = 0;
             }
-            e->plans.emplace_back();
-            std::string perr;
-            if (helm_batch_plan(sv.data(), rh.data(), xs.data(), (int)n, e->plans.back(), perr) != OC_OK) {
-                batched = false;  // e.g. more members than co-resident CTAs: chained solves instead
-                for (auto& b : e->plans) helm_batch_free(b);
-                e->plans.clear();
+            e->groups.back().push_back((int)m);
+            used += want;
+        }
+        const int np = e->members[0]->cfg.n_picard;
+        for (int q = 0; q < 2 * np && batched; ++q) {
+            for (const auto& grp : e->groups) {
+                std::vector<HelmSolver*> sv;
+                std::vector<const double*> rh;
+                std::vector<double*> xs;
+                for (int m : grp) {
+                    oc_handle* h = e->members[m];
+                    sv.push_back(h->solver);
+                    rh.push_back(h->rhs2);
+                    xs.push_back(h->ETA[q < np ? 1 - h->cur : h->cur]);
+                }
+                e->plans.emplace_back();
+                std::string perr;
+                if (helm_batch_plan(sv.data(), rh.data(), xs.data(), (int)sv.size(), e->plans.back(), perr) != OC_OK) {
+                    batched = false;  // e.g. a refined solver: chained solves instead
+                    for (auto& b : e->plans) helm_batch_free(b);
+                    e->plans.clear();
+                    break;
+                }
             }
         }
     }
@@ -1397,59 +1420,72 @@ int ensemble_record(oc_ensemble* e) {
                 h->profiling = prof;
                 if (rc) why = "member " + std::to_string(m) + ": " + h->err;
             }
-        // the batched solves: solve q waits for every member's placeholder before it
-        std::vector<cudaGraphNode_t> solve_nodes;
+        // the batched solves: group g's launch for solve q waits for its members'
+        // placeholders before the solve and for the previous launch (two cooperative
+        // grids never compete for the SMs)
+        const size_t G = e->groups.size();
+        const size_t rounds = G ? e->plans.size() / G : 0;
+        std::vector<cudaGraphNode_t> solve_nodes;  // [q * G + g]
         if (batched && rc == OC_OK) {
-            for (size_t q = 0; q < e->plans.size() && rc == OC_OK; ++q) {
-                std::vector<cudaGraphNode_t> pre(n);
-                for (size_t m = 0; m < n && rc == OC_OK; ++m) {
-                    if (rec.per_member[m].size() != e->plans.size() || rec.per_member[m][q].rhs != e->members[m]->rhs2 ||
-                        rec.per_member[m][q].x != e->members[m]->ETA[q < e->plans.size() / 2 ? 1 - cur[m] : cur[m]]) {
-                        rc = OC_ERR_STATE;
-                        why = "member " + std::to_string(m) + ": its solves differ from the batched plan";
+            cudaGraphNode_t prev = nullptr;
+            for (size_t q = 0; q < rounds && rc == OC_OK; ++q)
+                for (size_t gi = 0; gi < G && rc == OC_OK; ++gi) {
+                    std::vector<cudaGraphNode_t> pre;
+                    for (int m : e->groups[gi]) {
+                        if (rec.per_member[m].size() != rounds || rec.per_member[m][q].rhs != e->members[m]->rhs2 ||
+                            rec.per_member[m][q].x != e->members[m]->ETA[q < rounds / 2 ? 1 - cur[m] : cur[m]]) {
+                            rc = OC_ERR_STATE;
+                            why = "member " + std::to_string(m) + ": its solves differ from the batched plan";
+                            break;
+                        }
+                        pre.push_back(rec.per_member[m][q].pre);
                     }
-                    pre[m] = rc == OC_OK ? rec.per_member[m][q].pre : nullptr;
-                }
-                if (rc) break;
-                ce = cudaStreamUpdateCaptureDependencies(e->capture, pre.data(), n, cudaStreamSetCaptureDependencies);
-                if (ce == cudaSuccess) {
-                    std::string lerr;
-                    if (helm_batch_launch(e->plans[q], e->capture, lerr) != OC_OK) {
-                        rc = OC_ERR_CUDA;
-                        why = lerr;
-                    }
-                } else {
-                    rc = OC_ERR_CUDA;
-                    why = std::string("batched solve dependencies: ") + cudaGetErrorString(ce);
-                }
-                if (rc == OC_OK) {
-                    cudaStreamCaptureStatus cs;
-                    const cudaGraphNode_t* d = nullptr;
-                    size_t nd = 0;
-                    ce = cudaStreamGetCaptureInfo(e->capture, &cs, nullptr, nullptr, &d, &nd);
-                    if (ce != cudaSuccess || nd != 1) {
-                        rc = OC_ERR_CUDA;
-                        why = "batched solve node not found in the recording";
+                    if (rc) break;
+                    if (prev) pre.push_back(prev);
+                    ce = cudaStreamUpdateCaptureDependencies(e->capture, pre.data(), pre.size(),
+                                                             cudaStreamSetCaptureDependencies);
+                    if (ce == cudaSuccess) {
+                        std::string lerr;
+                        if (helm_batch_launch(e->plans[q * G + gi], e->capture, lerr) != OC_OK) {
+                            rc = OC_ERR_CUDA;
+                            why = lerr;
+                        }
                     } else {
-                        solve_nodes.push_back(d[0]);
+                        rc = OC_ERR_CUDA;
+                        why = std::string("batched solve dependencies: ") + cudaGetErrorString(ce);
+                    }
+                    if (rc == OC_OK) {
+                        cudaStreamCaptureStatus cs;
+                        const cudaGraphNode_t* d = nullptr;
+                        size_t nd = 0;
+                        ce = cudaStreamGetCaptureInfo(e->capture, &cs, nullptr, nullptr, &d, &nd);
+                        if (ce != cudaSuccess || nd != 1) {
+                            rc = OC_ERR_CUDA;
+                            why = "batched solve node not found in the recording";
+                        } else {
+                            solve_nodes.push_back(d[0]);
+                            prev = d[0];
+                        }
                     }
                 }
-            }
         }
         for (size_t m = 0; m < n; ++m) {
             cudaEventRecord(e->joins[m], e->streams[m]);
             cudaStreamWaitEvent(e->capture, e->joins[m], 0);
         }
         ce = cudaStreamEndCapture(e->capture, &g);
-        // each member's work after solve q waits for the batched solve q
-        for (size_t q = 0; q < solve_nodes.size() && rc == OC_OK && ce == cudaSuccess; ++q)
-            for (size_t m = 0; m < n && rc == OC_OK; ++m) {
-                const cudaError_t ae = cudaGraphAddDependencies(g, &solve_nodes[q], &rec.per_member[m][q].post, 1);
+        // each member's work after solve q waits for its group's launch of solve q
+        for (size_t k = 0; k < solve_nodes.size() && rc == OC_OK && ce == cudaSuccess; ++k) {
+            const size_t q = k / G, gi = k % G;
+            for (int m : e->groups[gi]) {
+                const cudaError_t ae = cudaGraphAddDependencies(g, &solve_nodes[k], &rec.per_member[m][q].post, 1);
                 if (ae != cudaSuccess) {
                     rc = OC_ERR_CUDA;
                     why = std::string("batched solve edges: ") + cudaGetErrorString(ae);
+                    break;
                 }
             }
+        }
     } else {
         ce = cudaStreamEndCapture(e->capture, &g);
     }

@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
         start_inner(R, e, R.rhs[e] * R.mask[e], r2, rz0);
     }
     publish(R, 1, r2, rz0, sm);
-    bool ok = grid_sync(R.bar_count, R.status);
+    bool ok = grid_sync(R.bar_count, R.status, gridDim.x, R.wait_cycles);
     double2 s = gather(R, 1, sm);
     const double norm_b = sqrt(s.x), tol = R.rtol * norm_b;
     double res = norm_b, rz = s.y;
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
                 }
             }
             publish(R, 0, pap, 0.0, sm);
-            ok = grid_sync(R.bar_count, R.status);
+            ok = grid_sync(R.bar_count, R.status, gridDim.x, R.wait_cycles);
             if (!ok) break;
             s = gather(R, 0, sm);
             if (!(s.x > 0.0)) break;  // p = 0: the FP32 residual vanished
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
                 }
             }
             publish(R, 1, rr2, rzn, sm);
-            ok = grid_sync(R.bar_count, R.status);
+            ok = grid_sync(R.bar_count, R.status, gridDim.x, R.wait_cycles);
             if (!ok) break;
             s = gather(R, 1, sm);
             ++inner;
@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
         if (!ok) break;
         // the correction, in FP64
         for (int e = first; e < n; e += stride) R.x[e] += (double)R.d[e];
-        ok = grid_sync(R.bar_count, R.status);
+        ok = grid_sync(R.bar_count, R.status, gridDim.x, R.wait_cycles);
         if (!ok) break;
         // r = b - A x in FP64 starts the next inner solve
         r2 = 0.0;
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
         for (int e = first; e < n; e += stride)
             start_inner(R, e, R.rhs[e] * R.mask[e] - apply64(R, e, neighbours(e, nx, ny)), r2, rz0);
         publish(R, 1, r2, rz0, sm);
-        ok = grid_sync(R.bar_count, R.status);
+        ok = grid_sync(R.bar_count, R.status, gridDim.x, R.wait_cycles);
         if (!ok) break;
         s = gather(R, 1, sm);
         res = sqrt(s.x);
@@ -280,6 +280,14 @@ __global__ void __launch_bounds__(RT, 1) k_helm_refined(RefineParams R) {
         R.report[1] = conv ? 1 : 0;
         R.report[2] = outer;
         *R.relres = norm_b > 0.0 ? res / norm_b : 0.0;
+        if (R.log_count) {
+            const int idx = *R.log_count;
+            if (idx < R.log_cap) {
+                R.log_iters[idx] = ok ? inner : -1;
+                R.log_conv[idx] = (ok && conv) ? 1 : 0;
+            }
+            *R.log_count = idx + 1;
+        }
     }
 }
 
@@ -313,7 +321,8 @@ void* RefinedHelm::dalloc(size_t nbytes) {
 }
 
 int RefinedHelm::init(int nx, int ny, double dx, double dy, double coef, double rtol, int max_iter,
-                      const double* mask_host, const double* ku, const double* kv, std::string& err) {
+                      const double* mask_host, const double* ku, const double* kv, std::string& err,
+                      int* status) {
     if (nx < 2 || ny < 2 || (long long)nx * ny > (1LL << 30) || !(dx > 0.0) || !(dy > 0.0) || !(coef >= 0.0) ||
         !(rtol > 0.0) || max_iter < 1 || !mask_host || !ku || !kv) {
         err = "invalid refined-solver configuration";
@@ -358,7 +367,8 @@ int RefinedHelm::init(int nx, int ny, double dx, double dy, double coef, double 
     R.d = (float*)dalloc(n4);
     R.part = (double*)dalloc(4 * (size_t)grid_ * sizeof(double));
     R.bar_count = (unsigned long long*)dalloc(sizeof(unsigned long long));
-    R.status = (int*)dalloc(sizeof(int));
+    R.status = status ? status : (int*)dalloc(sizeof(int));
+    R.wait_cycles = kBarrierCycles;
     R.report = (int*)dalloc(3 * sizeof(int));
     R.relres = (double*)dalloc(sizeof(double));
     if (!mask || !ax || !ay || !diag || !dinv || !wet || !R.p || !R.p2 || !R.Ap || !R.rr || !R.z || !R.d || !R.part ||
@@ -368,7 +378,7 @@ int RefinedHelm::init(int nx, int ny, double dx, double dy, double coef, double 
     }
     cudaMemcpy(mask, mask_host, n8, cudaMemcpyHostToDevice);
     cudaMemset(R.bar_count, 0, sizeof(unsigned long long));
-    cudaMemset(R.status, 0, sizeof(int));
+    if (!status) cudaMemset(R.status, 0, sizeof(int));
     cudaMemset(R.report, 0, 3 * sizeof(int));
     cudaMemset(R.relres, 0, sizeof(double));  // a report before the first solve reads zeros
     R.mask = mask;
@@ -377,8 +387,9 @@ int RefinedHelm::init(int nx, int ny, double dx, double dy, double coef, double 
     R.diag = diag;
     R.dinv = dinv;
     R.wet = wet;
-    const double cx = coef * (1.0 / (dx * dx)), cy = coef * (1.0 / (dy * dy));
-    k_refine_setup<<<(n + 255) / 256, 256>>>(R, cx, cy, ax, ay, diag, dinv, wet);
+    cx_ = coef * (1.0 / (dx * dx));
+    cy_ = coef * (1.0 / (dy * dy));
+    k_refine_setup<<<(n + 255) / 256, 256>>>(R, cx_, cy_, ax, ay, diag, dinv, wet);
     const cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         err = std::string("refined solver setup: ") + cudaGetErrorString(e);
@@ -387,13 +398,31 @@ int RefinedHelm::init(int nx, int ny, double dx, double dy, double coef, double 
     return OC_OK;
 }
 
+void RefinedHelm::rebuild(cudaStream_t s) {
+    const RefineParams& R = rp_;
+    k_refine_setup<<<(R.n + 255) / 256, 256, 0, s>>>(R, cx_, cy_, const_cast<float*>(R.ax), const_cast<float*>(R.ay),
+                                                     const_cast<float*>(R.diag), const_cast<float*>(R.dinv),
+                                                     const_cast<unsigned char*>(R.wet));
+}
+
 int RefinedHelm::solve(const double* rhs, double* x, cudaStream_t s, std::string& err) {
     if (!rhs || !x) return OC_ERR_ARG;
     RefineParams R = rp_;
     R.rhs = rhs;
     R.x = x;
-    void* args[] = {&R};
-    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_helm_refined, dim3(grid_), dim3(RT), args, 0, s);
+    // a cooperative launch through the extensible launch API, which stream
+    // capture records into a graph (the step replays its solves in graphs)
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid_);
+    cfg.blockDim = dim3(RT);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_helm_refined, R);
     if (e != cudaSuccess) {
         err = std::string("refined Helmholtz solve launch: ") + cudaGetErrorString(e);
         return OC_ERR_CUDA;

@@ -1219,6 +1219,7 @@ void* HelmSolver::dalloc(size_t nbytes) {
 }
 
 HelmSolver::~HelmSolver() {
+    delete refined_;
     for (void* p : allocs_) cudaFree(p);
 }
 
@@ -1226,6 +1227,10 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
                      int max_iter, const double* mask_host, double* Ku, double* Kv, int log_cap,
                      int* status, std::string& err) {
     HelmParams& H = hp_;
+    // the refined solver keeps this solver's log, counters and level-0 arrays
+    // (built as for PCG-Jacobi) and runs its solves itself
+    const bool refined = kind == HK_REFINED;
+    if (refined) kind = HK_PCG_JACOBI;
     H.kind = kind;
     H.coef = coef;
     H.rtol = rtol;
@@ -1490,6 +1495,12 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
         err = std::string("Helmholtz init: ") + cudaGetErrorString(e);
         return OC_ERR_CUDA;
     }
+    if (refined) {
+        refined_ = new RefinedHelm();
+        const int rc = refined_->init(nx, ny, dx0, dy0, coef, rtol, max_iter, mask_host, Ku, Kv, err, status);
+        if (rc) return rc;
+        refined_->set_log(H.log_iters, H.log_conv, H.log_count, H.log_cap);
+    }
     return OC_OK;
 }
 
@@ -1514,10 +1525,15 @@ int HelmSolver::grow_log(int cap, cudaStream_t s, std::string& err) {
     hp_.log_iters = it;
     hp_.log_conv = cv;
     hp_.log_cap = cap;
+    if (refined_) refined_->set_log(hp_.log_iters, hp_.log_conv, hp_.log_count, hp_.log_cap);
     return OC_OK;
 }
 
 void HelmSolver::rebuild(cudaStream_t s) {
+    if (refined_) {
+        refined_->rebuild(s);
+        return;
+    }
     for (int l = 0; l < hp_.n_levels; ++l) {
         const HLevel& L = hp_.lv[l];
         const HLevel& F = hp_.lv[l > 0 ? l - 1 : 0];
@@ -1545,6 +1561,10 @@ int helm_batch_plan(HelmSolver* const* solvers, const double* const* rhs, double
     double total = 0.0;
     std::vector<HelmParams> hp(n);
     for (int m = 0; m < n; ++m) {
+        if (!solvers[m]->batchable()) {
+            err = "batched Helmholtz solve: the refined solver has no batched form";
+            return OC_ERR_UNSUPPORTED;
+        }
         hp[m] = solvers[m]->batched_params(rhs[m], x[m]);
         smem = std::max(smem, solvers[m]->batched_smem());
         total += solvers[m]->work_weight();
@@ -1615,6 +1635,13 @@ int helm_batch_plan(HelmSolver* const* solvers, const double* const* rhs, double
     return OC_OK;
 }
 
+int helm_batch_grid() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(1, sms);
+}
+
 int helm_batch_launch(const HelmBatch& b, cudaStream_t s, std::string& err) {
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(b.grid);
@@ -1642,6 +1669,7 @@ void helm_batch_free(HelmBatch& b) {
 }
 
 int HelmSolver::solve(const double* rhs, double* x, cudaStream_t s, std::string& err) {
+    if (refined_) return refined_->solve(rhs, x, s, err);
     HelmParams H = hp_;
     H.rhs = rhs;
     H.lv[0].x = x;

@@ -1,15 +1,19 @@
 // Variable-coefficient free-surface Helmholtz solver, A = I - c D[K G[.]].
 #pragma once
 
+#include <algorithm>
 #include <vector>
 
+#include "helm_refined.cuh"
 #include "oc_internal.cuh"
 
 namespace oc {
 
 // HK_PCG_MG (no reference counterpart): CG preconditioned by one symmetric
 // V(2,2) cycle of the multigrid hierarchy; the mixed-precision step's solver
-enum { HK_PCG_JACOBI = 0, HK_PCG_RBGS = 1, HK_RBGS = 2, HK_MULTIGRID = 3, HK_PCG_MG = 5 };
+// HK_REFINED (no reference counterpart): FP32 inner PCG-Jacobi inside FP64
+// refinement (RefinedHelm), for the mixed-precision step
+enum { HK_PCG_JACOBI = 0, HK_PCG_RBGS = 1, HK_RBGS = 2, HK_MULTIGRID = 3, HK_REFINED = 4, HK_PCG_MG = 5 };
 
 struct HLevel {
     int nx, ny, n;
@@ -86,17 +90,29 @@ class HelmSolver {
     int* d_log_count() const { return hp_.log_count; }
     int grow_log(int cap, cudaStream_t s, std::string& err);
     // bound of the solve's barrier waits in SM clock cycles (default ~1 s)
-    void set_wait_cycles(long long cycles) { hp_.wait_cycles = cycles; }
+    void set_wait_cycles(long long cycles) {
+        hp_.wait_cycles = cycles;
+        if (refined_) refined_->set_wait_cycles(cycles);
+    }
+    // false for the refined solver, which has no batched form
+    bool batchable() const { return refined_ == nullptr; }
+    // CTAs a solve of this grid keeps busy: about one per 2048 cells (a 128 x 16
+    // tile of level 0), at least one, at most the solve's own grid
+    int preferred_ctas() const {
+        const long long want = ((long long)hp_.lv[0].n + 2047) / 2048;
+        return (int)std::max(1LL, std::min<long long>(want, grid_ > 0 ? grid_ : want));
+    }
     // this solver's system for a batched launch (helm_batch_*): the parameters
     // of x = A^-1 rhs without the one-CTA-per-tile assumptions, and the dynamic
     // shared memory it needs
     HelmParams batched_params(const double* rhs, double* x) const;
     size_t batched_smem() const { return smem_batched_; }
     double work_weight() const { return (double)hp_.lv[0].n; }
-    size_t bytes() const { return bytes_; }
+    size_t bytes() const { return bytes_ + (refined_ ? refined_->bytes() : 0); }
 
    private:
     HelmParams hp_{};
+    RefinedHelm* refined_ = nullptr;  // kind HK_REFINED: the solves go here
     std::vector<void*> allocs_;
     int grid_ = 0, block_ = 512;
     size_t smem_ = 0, smem_batched_ = 0;
@@ -117,6 +133,8 @@ struct HelmBatch {
 int helm_batch_plan(HelmSolver* const* solvers, const double* const* rhs, double* const* x, int n, HelmBatch& b,
                     std::string& err);
 int helm_batch_launch(const HelmBatch& b, cudaStream_t s, std::string& err);
+// CTAs of one batched launch at the least (one per SM of the current device)
+int helm_batch_grid();
 void helm_batch_free(HelmBatch& b);
 
 }  // namespace oc

@@ -113,11 +113,12 @@ class OceanParams:
         if self.dt <= 0.0:
             bad.append("dt must be > 0")
         # only the theta scheme owns an elliptic solve (reference model3d_v05.py:99-101);
-        # pcg_mg (CG preconditioned by one V(2,2) cycle) has no reference counterpart
+        # pcg_mg (CG preconditioned by one V(2,2) cycle) and pcg_refined (FP32 inner
+        # PCG inside FP64 refinement, mixed-precision step only) have no reference counterpart
         if self.scheme_name == "theta" and self.solver_kind not in (
-                "pcg_jacobi", "pcg_rbgs", "rbgs", "multigrid", "pcg_mg"):
+                "pcg_jacobi", "pcg_rbgs", "rbgs", "multigrid", "pcg_mg", "pcg_refined"):
             bad.append(f"unknown variable-coefficient solver {self.solver_kind!r} "
-                       "(expected pcg_jacobi|pcg_rbgs|rbgs|multigrid|pcg_mg)")
+                       "(expected pcg_jacobi|pcg_rbgs|rbgs|multigrid|pcg_mg|pcg_refined)")
         if self.vcoord != "zlevel":
             bad.append("vcoord must be zlevel")
         for name in ("bc_x", "bc_y"):

@@ -49,8 +49,9 @@ enum {
 /* option codes (the namelist strings of tools/toml2nml.py:209-264) */
 enum { OC_SCHEME_FB = 0, OC_SCHEME_THETA = 1, OC_SCHEME_SPLIT = 2 };
 enum { OC_SOLVER_PCG_JACOBI = 0, OC_SOLVER_PCG_RBGS = 1, OC_SOLVER_RBGS = 2, OC_SOLVER_MULTIGRID = 3 };
-/* standalone Helmholtz solver only (oc_helm_*), no reference counterpart: FP32
- * inner PCG-Jacobi inside FP64 iterative refinement */
+/* no reference counterpart: FP32 inner PCG-Jacobi inside FP64 iterative
+ * refinement, for the standalone solver (oc_helm_*) and the mixed-precision step
+ * (fp64 handles refuse it); the stopping test stays |b - A x| <= rtol |b| in FP64 */
 enum { OC_SOLVER_PCG_REFINED = 4 };
 /* no reference counterpart: CG preconditioned by one symmetric V(2,2) cycle of
  * the multigrid hierarchy, fp64, for the step (either precision, through the C

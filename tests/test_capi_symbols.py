@@ -44,6 +44,21 @@ def test_library_refuses_invalid_config_without_a_gpu():
     assert not h.value
 
 
+def test_fp64_handles_refuse_the_refined_solver_without_a_gpu():
+    """The FP32-inner refined solve serves the mixed-precision step only: an
+    fp64 handle must reproduce the reference's solves."""
+    import ctypes as C
+    from hydrostatic_ocean_core_benchmark_b200.params import OceanParams
+    lib = _lib.load()
+    p = OceanParams(dt=1.0, scheme_name="theta", solver_kind="pcg_refined")
+    h = C.c_void_p()
+    assert lib.oc_create(C.byref(_lib.config_from_params(p, 0, "fp64")), C.byref(h)) == 1
+    assert not h.value
+    cfg = _lib.config_from_params(p, 0, "fp64")
+    cfg.solver = 6
+    assert lib.oc_create(C.byref(cfg), C.byref(h)) == 1
+
+
 def test_entry_points_refuse_null_arguments_without_a_gpu():
     """Every entry point answers a null handle or a missing required pointer
     with OC_ERR_ARG before it touches a device; the error-string calls and

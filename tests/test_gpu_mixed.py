@@ -48,11 +48,15 @@ def _mixed(s, steps, graph=False):
     return out, log, stats
 
 
-def test_mixed_step_stays_within_its_bounds_of_the_oracle():
-    s = cases.seamount_basin(nx=48, ny=40, nz=12, seed=3)
+@pytest.mark.parametrize("solver", ["multigrid", "pcg_refined"])
+def test_mixed_step_stays_within_its_bounds_of_the_oracle(solver):
+    """With the configured multigrid, or the FP32-inner solve under FP64
+    refinement (pcg_refined) to the same FP64 stopping test."""
+    s = cases.seamount_basin(nx=48, ny=40, nz=12, seed=3, solver_kind=solver)
     p = s.params
     steps = 10
     got, log, stats = _mixed(s, steps)
+    p = p.replace(solver_kind="multigrid")  # the oracle runs the reference's solver
     geo = orc.Geometry(p, s.H, s.mask, s.dzr)
     b = orc.buoyancy(p.eos, s.T, s.S, geo.zc, p.g, p.rho0, p.alpha_t, p.beta_s, p.t0, p.s0) * geo.mask3
     ref = orc.OracleStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
@@ -70,8 +74,9 @@ def test_mixed_step_stays_within_its_bounds_of_the_oracle():
     assert len(log) == len(ref.solve_log)
 
 
-def test_mixed_graph_replay_equals_plain_steps():
-    s = cases.seamount_basin(nx=40, ny=36, nz=10, seed=5)
+@pytest.mark.parametrize("solver", ["multigrid", "pcg_refined"])
+def test_mixed_graph_replay_equals_plain_steps(solver):
+    s = cases.seamount_basin(nx=40, ny=36, nz=10, seed=5, solver_kind=solver)
     a, la, _ = _mixed(s, 6, graph=False)
     b, lb, _ = _mixed(s, 6, graph=True)
     for f in a:
