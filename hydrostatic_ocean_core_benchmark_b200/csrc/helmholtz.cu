@@ -67,6 +67,20 @@ __device__ __forceinline__ bool grid_sync(const HelmParams& H) {
     return grid_sync(H.bar_count, H.status, (unsigned)s_grid.ncta, H.wait_cycles);
 }
 
+// ------------------------------------------------------------------ asynchronous copies
+// cp.async into shared memory without a register round trip, so a thread's
+// copies are all in flight at once. The 8-byte form goes through L1, which is not
+// coherent with other SMs' writes, so it serves only arrays that stay constant
+// during the solve (the level coefficients); b and x, which other CTAs of the
+// launch write, are read through L2 (__ldcg).
+__device__ __forceinline__ void cpa_ca8(double* sdst, const double* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cpa_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // ------------------------------------------------------------------ level operators
 struct Cell {
     int e, ie, iw, jn, js;  // flat index and its four neighbours (periodic)
@@ -372,26 +386,26 @@ __device__ __forceinline__ void tile_load_chunks(const HLevel& L, int i0, int j0
                                                  const HLevel* C, TileRefs t) {
     const int nt = blockDim.x;
     for (int base = threadIdx.x; base < S::RN; base += CH * nt) {
-        double xv[CH], bv[CH], mv[CH], kuv[CH], kvv[CH], idv[CH];
+        double xv[CH], bv[CH];
 #pragma unroll
         for (int q = 0; q < CH; ++q) {
             const int r = base + q * nt;
-            xv[q] = bv[q] = mv[q] = kuv[q] = kvv[q] = idv[q] = 0.0;
+            xv[q] = bv[q] = 0.0;
             if (r < S::RN) {
                 const int rj = r / S::RW, ri = r - rj * S::RW;
                 const int gi = wrap_any(i0 - HALO + ri, L.nx), gj = wrap_any(j0 - HALO + rj, L.ny);
                 const int g = gj * L.nx + gi;
-                const double m = COEF ? L.mask[g] : t.m[r];
+                if (COEF) {
+                    // the coefficients, constant during the solve: asynchronous copies
+                    cpa_ca8(t.ku + r, L.Ku + g);
+                    cpa_ca8(t.kv + r, L.Kv + g);
+                    cpa_ca8(t.id + r, L.inv_diag + g);
+                    cpa_ca8(t.m + r, L.mask + g);
+                }
                 double x = xin ? __ldcg(xin + g) : 0.0;
-                if (C) x = x + __ldcg(C->x + (gj >> 1) * C->nx + (gi >> 1)) * m;
+                if (C) x = x + __ldcg(C->x + (gj >> 1) * C->nx + (gi >> 1)) * (COEF ? L.mask[g] : t.m[r]);
                 xv[q] = x;
                 bv[q] = __ldcg(L.b + g);
-                mv[q] = m;
-                if (COEF) {
-                    kuv[q] = L.Ku[g];
-                    kvv[q] = L.Kv[g];
-                    idv[q] = L.inv_diag[g];
-                }
             }
         }
 #pragma unroll
@@ -400,15 +414,10 @@ __device__ __forceinline__ void tile_load_chunks(const HLevel& L, int i0, int j0
             if (r < S::RN) {
                 t.x[r] = xv[q];
                 t.b[r] = bv[q];
-                if (COEF) {
-                    t.ku[r] = kuv[q];
-                    t.kv[r] = kvv[q];
-                    t.id[r] = idv[q];
-                    t.m[r] = mv[q];
-                }
             }
         }
     }
+    if (COEF) cpa_wait_all();
 }
 
 template <class S>
@@ -437,12 +446,17 @@ __device__ __forceinline__ TileRefs tile_refs_persist(double* persist, double* w
     return t;
 }
 
+// With a CTA of its own for every level-0 tile, the tiles go to the last CTAs
+// (tile = CTA - (CTAs - tiles)), so CTA 0, which runs the coarse levels, keeps
+// its persistent region for their coefficients (H.coarse_persist).
+__device__ __forceinline__ int level0_tile_of_cta(int tiles) { return s_grid.cta - (s_grid.ncta - tiles); }
+
 __device__ void persist_level0(const HelmParams& H, double* persist) {
     using S = TileWide;
     const HLevel& L = H.lv[0];
     const int tx = (L.nx + S::TX - 1) / S::TX;
-    const int tile = s_grid.cta;
-    if (tile >= tx * ((L.ny + S::TY - 1) / S::TY)) return;
+    const int tile = level0_tile_of_cta(tx * ((L.ny + S::TY - 1) / S::TY));
+    if (tile < 0) return;
     const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
     for (int r = threadIdx.x; r < S::RN; r += blockDim.x) {
         const int rj = r / S::RW, ri = r - rj * S::RW;
@@ -537,7 +551,8 @@ __device__ void mg_down(const HelmParams& H, int l, const double* xin, double* x
     const int tx = (L.nx + S::TX - 1) / S::TX, ty = (L.ny + S::TY - 1) / S::TY;
     const bool keep = persist != nullptr;
     TileRefs t = keep ? tile_refs_persist<S>(persist, smem) : tile_refs<S>(smem);
-    for (int tile = s_grid.cta; tile < tx * ty; tile += s_grid.ncta) {
+    for (int tile = keep ? level0_tile_of_cta(tx * ty) : s_grid.cta; tile < tx * ty; tile += s_grid.ncta) {
+        if (tile < 0) continue;  // CTA-uniform: this CTA holds no persistent tile
         const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
         tile_load<S>(L, i0, j0, xin, nullptr, t, !keep);
         tile_four_half_sweeps<S>(L, i0, j0, t, 0);
@@ -588,7 +603,8 @@ __device__ void mg_up(const HelmParams& H, int l, const double* xin, const HLeve
     const int tx = (L.nx + S::TX - 1) / S::TX, ty = (L.ny + S::TY - 1) / S::TY;
     const bool keep = persist != nullptr;
     TileRefs t = keep ? tile_refs_persist<S>(persist, smem) : tile_refs<S>(smem);
-    for (int tile = s_grid.cta; tile < tx * ty; tile += s_grid.ncta) {
+    for (int tile = keep ? level0_tile_of_cta(tx * ty) : s_grid.cta; tile < tx * ty; tile += s_grid.ncta) {
+        if (tile < 0) continue;  // CTA-uniform: this CTA holds no persistent tile
         const int i0 = (tile % tx) * S::TX, j0 = (tile / tx) * S::TY;
         tile_load<S>(L, i0, j0, xin, &C, t, !keep);
         tile_four_half_sweeps<S>(L, i0, j0, t, 1);
@@ -626,20 +642,39 @@ __device__ __forceinline__ double* coarse_scratch(const HelmParams& H, double* b
     return base + 6 * tot;
 }
 
-__device__ __forceinline__ CoarseRefs coarse_refs(const HelmParams& H, double* base, int l) {
+// coef: where ku, kv, id and m live when they persist for the solve (CTA 0's
+// persistent region), else null (they follow x and b in `base`)
+__device__ __forceinline__ CoarseRefs coarse_refs(const HelmParams& H, double* base, int l,
+                                                  double* coef = nullptr) {
     int off = 0, tot = 0;
     for (int q = H.coarse_from; q < H.n_levels; ++q) {
         if (q < l) off += H.lv[q].n;
         tot += H.lv[q].n;
     }
+    double* cb = coef ? coef : base + 2 * tot;
     CoarseRefs c;
     c.x = base + off;
     c.b = base + tot + off;
-    c.ku = base + 2 * tot + off;
-    c.kv = base + 3 * tot + off;
-    c.id = base + 4 * tot + off;
-    c.m = base + 5 * tot + off;
+    c.ku = cb + off;
+    c.kv = cb + tot + off;
+    c.id = cb + 2 * tot + off;
+    c.m = cb + 3 * tot + off;
     return c;
+}
+
+// the coarse levels' coefficients into `coef` (asynchronous copies; the caller
+// waits for them before its next CTA barrier)
+__device__ void coarse_coef_load(const HelmParams& H, double* coef, double* base) {
+    for (int l = H.coarse_from; l < H.n_levels; ++l) {
+        const HLevel& L = H.lv[l];
+        CoarseRefs s = coarse_refs(H, base, l, coef);
+        for (int e = threadIdx.x; e < L.n; e += blockDim.x) {
+            cpa_ca8(s.ku + e, L.Ku + e);
+            cpa_ca8(s.kv + e, L.Kv + e);
+            cpa_ca8(s.id + e, L.inv_diag + e);
+            cpa_ca8(s.m + e, L.mask + e);
+        }
+    }
 }
 
 // Gauss-Seidel update of coarse cell (i, j) = e; with C, the neighbours carry
@@ -701,33 +736,36 @@ __device__ double coarse_residual(const HLevel& L, double coef, CoarseRefs s, in
 
 // the V-cycle below and including level cf, by CTA 0 alone; reads level cf's b
 // (and x when cf is the finest level) from global memory, writes level cf's x
-__device__ void mg_coarse(const HelmParams& H, double* smem, const double* xin_cf, double* xout_cf) {
+// coef: the coarse coefficients kept for the whole solve (coarse_coef_load at its
+// start), or null to load them here
+__device__ void mg_coarse(const HelmParams& H, double* smem, const double* xin_cf, double* xout_cf,
+                          double* coef = nullptr) {
     const int cf = H.coarse_from, nl = H.n_levels;
-    for (int l = cf; l < nl; ++l) {
-        const HLevel& L = H.lv[l];
-        CoarseRefs s = coarse_refs(H, smem, l);
+    // the level coefficients (constant during the solve) by asynchronous copies, all
+    // in flight at once; level cf's b and x (written by this launch) through L2
+    if (!coef) coarse_coef_load(H, nullptr, smem);
+    {
+        const HLevel& L = H.lv[cf];
+        CoarseRefs s = coarse_refs(H, smem, cf, coef);
         for (int e = threadIdx.x; e < L.n; e += blockDim.x) {
-            s.ku[e] = L.Ku[e];
-            s.kv[e] = L.Kv[e];
-            s.id[e] = L.inv_diag[e];
-            s.m[e] = L.mask[e];
-            if (l == cf) {
-                s.b[e] = __ldcg(L.b + e);
-                s.x[e] = xin_cf ? __ldcg(xin_cf + e) : 0.0;
-            }
+            const double bv = __ldcg(L.b + e);
+            const double xv = xin_cf ? __ldcg(xin_cf + e) : 0.0;
+            s.b[e] = bv;
+            s.x[e] = xv;
         }
     }
+    cpa_wait_all();
     __syncthreads();
     for (int l = cf; l < nl; ++l) {
         const HLevel& L = H.lv[l];
-        CoarseRefs s = coarse_refs(H, smem, l);
+        CoarseRefs s = coarse_refs(H, smem, l, coef);
         for (int h = 0; h < 4; ++h) coarse_half_sweep(L, s, h & 1, nullptr, nullptr);
         if (l + 1 < nl) {
             // the residual of every cell of level l (a coarser level exists only
             // below an even-sized one, so they are exactly the 2x2 children),
             // then the children's mean per coarse cell
             const HLevel& C = H.lv[l + 1];
-            CoarseRefs c = coarse_refs(H, smem, l + 1);
+            CoarseRefs c = coarse_refs(H, smem, l + 1, coef);
             double* res = coarse_scratch(H, smem);
             for (int f = threadIdx.x; f < L.n; f += blockDim.x) res[f] = coarse_residual(L, H.coef, s, f);
             __syncthreads();
@@ -742,20 +780,20 @@ __device__ void mg_coarse(const HelmParams& H, double* smem, const double* xin_c
     }
     {  // the coarsest level: its reverse sweeps follow the forward ones directly
         const HLevel& L = H.lv[nl - 1];
-        CoarseRefs s = coarse_refs(H, smem, nl - 1);
+        CoarseRefs s = coarse_refs(H, smem, nl - 1, coef);
         for (int h = 0; h < 4; ++h) coarse_half_sweep(L, s, 1 - (h & 1), nullptr, nullptr);
     }
     for (int l = nl - 2; l >= cf; --l) {
         const HLevel& L = H.lv[l];
-        CoarseRefs s = coarse_refs(H, smem, l);
-        CoarseRefs c = coarse_refs(H, smem, l + 1);
+        CoarseRefs s = coarse_refs(H, smem, l, coef);
+        CoarseRefs c = coarse_refs(H, smem, l + 1, coef);
         coarse_half_sweep(L, s, 1, &c, &H.lv[l + 1]);
         coarse_half_sweep(L, s, 0, nullptr, nullptr);
         coarse_half_sweep(L, s, 1, nullptr, nullptr);
         coarse_half_sweep(L, s, 0, nullptr, nullptr);
     }
     const HLevel& L = H.lv[cf];
-    CoarseRefs s = coarse_refs(H, smem, cf);
+    CoarseRefs s = coarse_refs(H, smem, cf, coef);
     for (int e = threadIdx.x; e < L.n; e += blockDim.x) xout_cf[e] = s.x[e];
     __syncthreads();
 }
@@ -783,6 +821,8 @@ __device__ void mg_smooth(const HelmParams& H, int l, const double* xin, double*
 __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* x0b, double* smem, double* persist,
                                 bool& ok) {
     const int cf = H.coarse_from, nl = H.n_levels;
+    // CTA 0 keeps the coarse coefficients in its persistent region when it holds no level-0 tile
+    double* ccoef = (H.coarse_persist && s_grid.cta == 0) ? persist : nullptr;
     if (cf == 0) {
         if (s_grid.cta == 0) mg_coarse(H, smem, x0, x0b);
         ok = grid_sync(H);
@@ -803,7 +843,7 @@ __device__ double* vcycle_tiled(const HelmParams& H, double* x0, double* x0b, do
     }
     if (!ok) return x0;
     if (cf < nl) {
-        if (s_grid.cta == 0) mg_coarse(H, smem, nullptr, H.lv[cf].x2);
+        if (s_grid.cta == 0) mg_coarse(H, smem, nullptr, H.lv[cf].x2, ccoef);
         ok = grid_sync(H);
     } else {
         const int l = nl - 1;
@@ -874,6 +914,11 @@ __device__ __forceinline__ void helm_solve_body(const HelmParams& H, double* sme
     ok = grid_sync(H);
     const double norm_b = ok ? sqrt(fold_sum(H, fold, H.leafA, sm, ok)) : 0.0;
     if (persist) persist_level0(H, persist);  // the coefficients are fixed during the solve
+    if (H.coarse_persist && s_grid.cta == 0) {
+        coarse_coef_load(H, persist, sm);
+        cpa_wait_all();
+        __syncthreads();
+    }
     if (!ok || norm_b == 0.0) goto done;
     {
         const double tol = H.rtol * norm_b;
@@ -1490,6 +1535,15 @@ int HelmSolver::init(int nx, int ny, double dx0, double dy0, double coef, int ki
         return OC_ERR_CUDA;
     }
     grid_ = sms * std::min(per_sm, 2);
+    // CTA 0 holds no level-0 tile when there are more CTAs than tiles: its
+    // persistent region then keeps the coarse levels' four coefficient arrays
+    {
+        size_t ccells = 0;
+        for (int l = H.coarse_from; l < H.n_levels; ++l) ccells += (size_t)H.lv[l].n;
+        const int tiles0 = ((nx + TileWide::TX - 1) / TileWide::TX) * ((ny + TileWide::TY - 1) / TileWide::TY);
+        H.coarse_persist = (H.persist0 && mg_levels && H.coarse_from > 0 && H.coarse_from < H.n_levels &&
+                            grid_ > tiles0 && ccells <= (size_t)TileWide::RN) ? 1 : 0;
+    }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         err = std::string("Helmholtz init: ") + cudaGetErrorString(e);
@@ -1546,6 +1600,7 @@ HelmParams HelmSolver::batched_params(const double* rhs, double* x) const {
     H.rhs = rhs;
     H.lv[0].x = x;
     H.persist0 = 0;
+    H.coarse_persist = 0;
     H.ops_smem = 0;
     return H;
 }

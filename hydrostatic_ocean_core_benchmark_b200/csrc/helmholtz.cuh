@@ -34,6 +34,7 @@ struct HelmParams {
     int wide0;      // level 0 runs 128 x 16 tiles
     int fused_res;  // ... whose rows are NumPy's leaves: the up phase forms the residual sums
     int persist0;   // ... one per CTA: their coefficients stay in shared memory for the solve
+    int coarse_persist;  // CTA 0 (no level-0 tile) keeps the coarse levels' coefficients in its region
     double coef, rtol;
     HLevel lv[OC_MAX_LEVELS];
     double *r, *z, *p, *Ap;  // level-0 work vectors
