@@ -54,7 +54,11 @@ typedef double wide;
 #define OC_MINB_MOM 2
 #endif
 #ifndef OC_MINB_TRACER
+#ifdef OC_MIXED
+#define OC_MINB_TRACER 6  // FP32: 0.56 against 0.59 ms per step at 512 x 512 x 50
+#else
 #define OC_MINB_TRACER 4
+#endif
 #endif
 using KPR = KPT<real>;
 using ColGeoR = ColGeoT<real>;

