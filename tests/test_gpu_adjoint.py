@@ -93,7 +93,7 @@ def test_adjoint_matches_torch_autograd_of_the_restated_step(advection):
     ro.close()
 
 
-@pytest.mark.parametrize("nx,ny,nz,steps,every,ndir,advection,bound", [
+@pytest.mark.parametrize("nx,ny,nz,steps,every,ndir,advection,bound,median_bound", [
     (40, 32, 10, 6, 3, 8, "centered2", 1e-6, 1e-7),
     (256, 256, 32, 20, 5, 32, "centered2", 3e-6, 1e-7),
     (256, 256, 32, 20, 5, 32, "up3", 3e-4, 1e-5),
