@@ -22,6 +22,8 @@
 //   k_tracer_solve    model3d_v05.py:514-533 + eos.py:68-133
 //   2D kernels        model3d_v05.py:290-335, 376-384, 396-400, 410-413, 440-461
 
+#include <atomic>
+
 #include "oc_internal.cuh"
 #include "step_common.cuh"
 #include "step_kernels.cuh"
@@ -1406,11 +1408,15 @@ static void closure_nzm(const KPR& P, const real* u, const real* v, const wide* 
     const dim3 blk = col_block();
 #ifdef OC_MIXED
     const size_t smem = (size_t)(P.nz + 1) * blk.x * blk.y * sizeof(real);
-    static bool opted = false;  // above 48 KB a kernel's dynamic shared memory is opt-in
-    if (!opted) {
+    // above 48 KB a kernel's dynamic shared memory is opt-in, once per device
+    static std::atomic<unsigned long long> opted{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ULL << (dev & 63);
+    if (!(opted.load() & bit)) {
         cudaFuncSetAttribute(k_closure<NZM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)((size_t)(NZM + 1) * blk.x * blk.y * sizeof(real)));
-        opted = true;
+        opted.fetch_or(bit);
     }
 #else
     const size_t smem = 0;
