@@ -774,6 +774,7 @@ static int set_domain_impl(oc_handle* h, const double* Hh, const double* maskh, 
         rc = h->solver->init(nx, ny, h->cfg.lx / nx, h->cfg.ly / ny, coef, h->cfg.solver, h->cfg.rtol,
                              h->cfg.max_iter, h->mask.data(), h->Ku, h->Kv, 4096, h->d_status, h->err);
         if (rc) return rc;
+        h->solver->set_warm_start(h->mixed);  // the fp64 step starts from zero, as the reference
     }
     rc = build_coefficients(h, 0, false);
     if (rc) return rc;

@@ -907,7 +907,7 @@ __device__ __forceinline__ void helm_solve_body(const HelmParams& H, double* sme
                    const double r = rhs[e] * L0.mask[e];
                    b0[e] = r;
                    if (H.kind <= HK_PCG_RBGS || H.kind == HK_PCG_MG) H.r[e] = r;
-                   x[e] = 0.0;
+                   if (!H.warm) x[e] = 0.0;
                    return make_double2(r * r, 0.0);
                },
                H.leafA, nullptr);
@@ -1601,6 +1601,7 @@ HelmParams HelmSolver::batched_params(const double* rhs, double* x) const {
     H.lv[0].x = x;
     H.persist0 = 0;
     H.coarse_persist = 0;
+    H.warm = (warm_ && H.kind == HK_MULTIGRID) ? 1 : 0;
     H.ops_smem = 0;
     return H;
 }
@@ -1728,6 +1729,7 @@ int HelmSolver::solve(const double* rhs, double* x, cudaStream_t s, std::string&
     HelmParams H = hp_;
     H.rhs = rhs;
     H.lv[0].x = x;
+    H.warm = (warm_ && H.kind == HK_MULTIGRID) ? 1 : 0;
     // a cooperative launch (every CTA resident, for the grid barriers) through
     // the extensible launch API, which stream capture records into a graph
     cudaLaunchConfig_t cfg{};

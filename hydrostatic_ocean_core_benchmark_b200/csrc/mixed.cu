@@ -331,6 +331,10 @@ int step_once_mixed(oc_handle* h, cudaStream_t s) {
             { Prof pr(h, s, "helm_rhs"); launch_helm_rhs(P, eta, h->div_old, h->Ug, h->Vg, h->rhs2, s); }
             int rc = ensure_log(h, h->solves + 1, s);
             if (rc) return rc;
+            // the mixed step owes the reference no iteration counts: its multigrid
+            // starts from the current eta (first pass) or the first pass's solution
+            // (the solver's warm start), under the same stopping test
+            if (m == 0) cudaMemcpyAsync(etan, eta, h->n2 * sizeof(double), cudaMemcpyDeviceToDevice, s);
             if (h->batch_rec) {
                 // an ensemble recording its batched graph: the solve becomes a pair of
                 // placeholder nodes the batched solve is later wired between
