@@ -906,7 +906,9 @@ __device__ __forceinline__ void helm_solve_body(const HelmParams& H, double* sme
                [&](int e) {
                    const double r = rhs[e] * L0.mask[e];
                    b0[e] = r;
-                   if (H.kind <= HK_PCG_RBGS || H.kind == HK_PCG_MG) H.r[e] = r;
+                   // the CG residual of the starting iterate: b, or b - A x with a warm start
+                   if (H.kind <= HK_PCG_RBGS || H.kind == HK_PCG_MG)
+                       H.r[e] = H.warm ? r - apply_at(L0, H.coef, x, cell_of(L0, e)) : r;
                    if (!H.warm) x[e] = 0.0;
                    return make_double2(r * r, 0.0);
                },
@@ -1601,7 +1603,7 @@ HelmParams HelmSolver::batched_params(const double* rhs, double* x) const {
     H.lv[0].x = x;
     H.persist0 = 0;
     H.coarse_persist = 0;
-    H.warm = (warm_ && H.kind == HK_MULTIGRID) ? 1 : 0;
+    H.warm = warm_ ? 1 : 0;
     H.ops_smem = 0;
     return H;
 }
@@ -1729,7 +1731,7 @@ int HelmSolver::solve(const double* rhs, double* x, cudaStream_t s, std::string&
     HelmParams H = hp_;
     H.rhs = rhs;
     H.lv[0].x = x;
-    H.warm = (warm_ && H.kind == HK_MULTIGRID) ? 1 : 0;
+    H.warm = warm_ ? 1 : 0;
     // a cooperative launch (every CTA resident, for the grid barriers) through
     // the extensible launch API, which stream capture records into a graph
     cudaLaunchConfig_t cfg{};

@@ -31,7 +31,7 @@ struct HLevel {
 
 struct HelmParams {
     int n_levels, kind, max_iter, coarse_from;
-    int warm;       // the stationary multigrid starts from the x it is given (else from zero)
+    int warm;       // the solve starts from the x it is given (else from zero)
     int wide0;      // level 0 runs 128 x 16 tiles
     int fused_res;  // ... whose rows are NumPy's leaves: the up phase forms the residual sums
     int persist0;   // ... one per CTA: their coefficients stay in shared memory for the solve
@@ -85,8 +85,8 @@ class HelmSolver {
     void rebuild(cudaStream_t s);
     // x = A^-1 rhs on the device, iteration count appended to the log
     int solve(const double* rhs, double* x, cudaStream_t s, std::string& err);
-    // warm start: the stationary multigrid starts from the x it is given instead of
-    // zero (the reference starts from zero; the mixed-precision step warm-starts)
+    // warm start: the solve starts from the x it is given instead of zero (the
+    // reference starts from zero; the mixed-precision step warm-starts)
     void set_warm_start(bool w) { warm_ = w; }
     int n_levels() const { return hp_.n_levels; }
     int log_capacity() const { return hp_.log_cap; }

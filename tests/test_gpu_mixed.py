@@ -48,10 +48,11 @@ def _mixed(s, steps, graph=False):
     return out, log, stats
 
 
-@pytest.mark.parametrize("solver", ["multigrid", "pcg_refined"])
+@pytest.mark.parametrize("solver", ["multigrid", "pcg_refined", "pcg_mg"])
 def test_mixed_step_stays_within_its_bounds_of_the_oracle(solver):
-    """With the configured multigrid, or the FP32-inner solve under FP64
-    refinement (pcg_refined) to the same FP64 stopping test."""
+    """With the configured multigrid (warm-started), the FP32-inner solve under
+    FP64 refinement (pcg_refined), or MG-preconditioned CG (warm-started), all to
+    the same FP64 stopping test."""
     s = cases.seamount_basin(nx=48, ny=40, nz=12, seed=3, solver_kind=solver)
     p = s.params
     steps = 10
@@ -74,7 +75,7 @@ def test_mixed_step_stays_within_its_bounds_of_the_oracle(solver):
     assert len(log) == len(ref.solve_log)
 
 
-@pytest.mark.parametrize("solver", ["multigrid", "pcg_refined"])
+@pytest.mark.parametrize("solver", ["multigrid", "pcg_refined", "pcg_mg"])
 def test_mixed_graph_replay_equals_plain_steps(solver):
     s = cases.seamount_basin(nx=40, ny=36, nz=10, seed=5, solver_kind=solver)
     a, la, _ = _mixed(s, 6, graph=False)
