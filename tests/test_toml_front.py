@@ -123,3 +123,28 @@ def test_verify_builds_the_reference_stepper_of_the_run():
         o = ref.step(o)
     for f in ("eta", "u", "v", "b", "T", "S"):
         assert np.array_equal(getattr(s0, f), getattr(o, f)), f
+
+
+LADDER = json.loads((Path(__file__).resolve().parent / "golden" / "ladder_case.json").read_text())
+
+
+@pytest.mark.parametrize("case", LADDER, ids=[c["name"] for c in LADDER])
+def test_ladder_case_matches_the_reference_tree(case, tmp_path):
+    """The reference's hardware-ladder case (lock_exchange, theta 0.5, 50 steps),
+    bundled by the reference's tool on the reference's own tree, is what this
+    package's tree gives under the same flags plus `extra`."""
+    config = tf.apply_overrides(tf.load_config(CONFIG), case["overrides"] + case["extra"])
+    run = tf.resolve_run(config, nx=case["nx"], nz=case["nz"], case=case["case"], cfl=case["cfl"],
+                         n_steps=case["steps"])
+    prefix = str(tmp_path / "b")
+    nml = write_bundle(prefix, run.params.replace(n_repeat=1, n_warmup=0), run.H, run.mask, run.state)
+    ours = parse_namelist_text(Path(nml).read_text())
+    compared = 0
+    for key, raw in case["namelist"].items():
+        if key in NOT_COMPARED or key not in ours:
+            continue
+        assert _value(ours[key]) == _value(raw), (key, ours[key], raw)
+        compared += 1
+    assert compared >= 50
+    assert _sha(prefix + "_domain.bin") == case["domain_sha256"]
+    assert _sha(prefix + "_init.bin") == case["init_sha256"]
