@@ -534,10 +534,13 @@ def run_ours(args, rank, world, local_rank):
     top = max(ktimes.items(), key=lambda kv: kv[1][1])
     name, (nlaunch, tot_ms) = top
     iters_per_solve = (sum(log) / len(log)) if log else 0.0
-    if name == "helm_solve":
-        alg = helm_bytes_per_iteration(p) * iters_per_solve
-    else:
-        alg = 8 * ACCESSES_PER_CELL.get(name, 0) * n3
+
+    def alg_bytes(kernel):
+        if kernel == "helm_solve":
+            return helm_bytes_per_iteration(p) * iters_per_solve
+        return 8 * ACCESSES_PER_CELL.get(kernel, 0) * n3
+
+    alg = alg_bytes(name)
     per_launch_ms = tot_ms / max(1, nlaunch)
     achieved = alg / (per_launch_ms / 1e3) / 1e9
     traffic = dram_traffic_from_profiles(name)
@@ -547,8 +550,16 @@ def run_ours(args, rank, world, local_rank):
     iters_per_step = sum(log) / (args.steps + args.profile_steps)  # both timed regions
     bstep = step_algorithmic_bytes(p, iters_per_step)
     step_gbs = bstep / (ms / args.steps / 1e3) / 1e9
-    kernel_share = {k: {"launches": v[0], "ms": v[1], "share": v[1] / max(1e-12, sum(x[1] for x in ktimes.values()))}
-                    for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1][1])}
+    kernel_share = {}
+    for k, (nl, kms) in sorted(ktimes.items(), key=lambda kv: -kv[1][1]):
+        row = {"launches": nl, "ms": kms, "share": kms / max(1e-12, sum(x[1] for x in ktimes.values()))}
+        kb = alg_bytes(k)
+        if kb > 0 and nl > 0 and kms > 0:
+            # algorithmic bytes per launch over the launch's average duration, against the HBM peak
+            gbs = kb / (kms / nl / 1e3) / 1e9
+            row.update({"algorithmic_bytes_per_launch": kb, "achieved_gbs": gbs, "frac": gbs / peak,
+                        "dram_bytes_per_launch": dram_traffic_from_profiles(k)})
+        kernel_share[k] = row
 
     # the mixed-precision step on the same recipe and grid, beside a fresh fp64
     # run from the same initial state (errors per field against the fp64 path)
