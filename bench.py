@@ -654,8 +654,8 @@ def run_ensemble(args, rank, world, local_rank):
             tw.set_state(eta=s.eta, u=s.u, v=s.v, T=s.T, S=s.S)
             twins.append((m, tw))
     cells = sum(nx * ny * nz for nx, ny, nz in shapes)
-    # the autotuner times the fp64 kernels; mixed members keep the default tiling
-    tiling = [st.autotune() for st in members] if prec == "fp64" else []
+    # each member's tile shapes timed on its own kernels (FP32 ones for mixed members)
+    tiling = [st.autotune() for st in members]
     stream = torch.cuda.Stream(device=local_rank)
     steps = args.steps + (args.steps % 2)
     warm = max(args.warmup, 3)

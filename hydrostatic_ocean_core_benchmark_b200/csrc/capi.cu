@@ -910,9 +910,7 @@ int oc_set_tiling(oc_handle* h, int32_t mom_levels, int32_t tracer_levels) {
 int oc_autotune(oc_handle* h, int32_t* mom_levels, int32_t* tracer_levels) {
     if (!h) return OC_ERR_ARG;
     if (!h->has_state) return fail(h, OC_ERR_STATE, "set the state before tuning");
-    if (h->mixed) return fail(h, OC_ERR_UNSUPPORTED, "the autotuner times the fp64 kernels only");
     cudaSetDevice(h->cfg.device);
-    KP P = h->P;
     const int c = h->cur, nz = h->nz;
     std::vector<int> cand;
     for (int kl : {2, 3, 4, 5, 6, 8, 10, 13, 17, 25, nz})
@@ -921,28 +919,17 @@ int oc_autotune(oc_handle* h, int32_t* mom_levels, int32_t* tracer_levels) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    launch_phi(P, h->B[c], h->phi, s);  // the explicit momentum terms read phi
-    // time one kernel class over the candidates; the outputs are scratch that
-    // the next step writes again before reading
-    auto tune = [&](bool mom) {
-        int best = mom ? P.mom_kl : P.tr_kl;
+    // time one kernel class over the candidates (run(kl) launches it with kl levels
+    // per CTA); the outputs are scratch that the next step writes again before reading
+    auto best_of = [&](int start, auto run) {
+        int best = start;
         float best_ms = 1e30f;
         for (int kl : cand) {
-            KP Q = P;
-            (mom ? Q.mom_kl : Q.tr_kl) = kl;
-            auto run = [&]() {
-                if (mom)
-                    launch_mom_explicit(Q, h->U[c], h->V[c], h->B[c], h->phi, h->w, h->km, h->pgx, h->pgy, h->avpv,
-                                        h->avpu, h->dzu, h->dzv, h->stu, h->stv, s);
-                else
-                    launch_tracer_rhs(Q, h->cfg.tracers == OC_TRACERS_TS ? h->Tt[c] : h->B[c], h->Ss[c], h->U[c],
-                                      h->V[c], h->w, h->kh, h->pgx, h->pgy, s);
-            };
-            run();
+            run(kl);
             float ms = 1e30f;
             for (int r = 0; r < 3; ++r) {
                 cudaEventRecord(e0, s);
-                run();
+                run(kl);
                 cudaEventRecord(e1, s);
                 cudaEventSynchronize(e1);
                 float t = 0.0f;
@@ -956,13 +943,47 @@ int oc_autotune(oc_handle* h, int32_t* mom_levels, int32_t* tracer_levels) {
         }
         return best;
     };
-    const int mk = tune(true), tk = tune(false);
+    int mk, tk;
+    if (h->mixed) {
+        // the FP32 kernels of the mixed path on its FP32 fields (TS tracers)
+        const KPT<float>& P = h->P32;
+        launch_phi(P, h->B[c], h->phi, s);  // the explicit momentum terms read phi
+        mk = best_of(P.mom_kl, [&](int kl) {
+            KPT<float> Q = P;
+            Q.mom_kl = kl;
+            launch_mom_explicit(Q, h->U32[c], h->V32[c], h->B[c], h->phi, h->w32, h->km32, h->pgx32, h->pgy32,
+                                h->avpv32, h->avpu32, h->dzu32, h->dzv32, h->stu32, h->stv32, s);
+        });
+        tk = best_of(P.tr_kl, [&](int kl) {
+            KPT<float> Q = P;
+            Q.tr_kl = kl;
+            launch_tracer_rhs(Q, h->T32[c], h->S32[c], h->U32[c], h->V32[c], h->w32, h->kh32, h->pgx32, h->pgy32,
+                              s);
+        });
+    } else {
+        const KP& P = h->P;
+        launch_phi(P, h->B[c], h->phi, s);
+        mk = best_of(P.mom_kl, [&](int kl) {
+            KP Q = P;
+            Q.mom_kl = kl;
+            launch_mom_explicit(Q, h->U[c], h->V[c], h->B[c], h->phi, h->w, h->km, h->pgx, h->pgy, h->avpv, h->avpu,
+                                h->dzu, h->dzv, h->stu, h->stv, s);
+        });
+        tk = best_of(P.tr_kl, [&](int kl) {
+            KP Q = P;
+            Q.tr_kl = kl;
+            launch_tracer_rhs(Q, h->cfg.tracers == OC_TRACERS_TS ? h->Tt[c] : h->B[c], h->Ss[c], h->U[c], h->V[c],
+                              h->w, h->kh, h->pgx, h->pgy, s);
+        });
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     const int rc = check_launch(h, "oc_autotune");
     if (rc) return rc;
     h->P.mom_kl = mk;
     h->P.tr_kl = tk;
+    h->P32.mom_kl = mk;
+    h->P32.tr_kl = tk;
     drop_graphs(h);
     if (mom_levels) *mom_levels = mk;
     if (tracer_levels) *tracer_levels = tk;

@@ -172,8 +172,9 @@ int oc_set_domain_slab(oc_handle* h, const double* H, const double* mask, const 
  * kernels (1..nz; 10 or nz by default). Every value gives the same results bit
  * for bit; only the speed depends on it. oc_set_tiling sets both; oc_autotune
  * times each kernel on the current state over a candidate list, keeps the
- * fastest and returns the choice (synchronous). No reference counterpart:
- * the tile shapes of the batched-ensemble form. */
+ * fastest and returns the choice (synchronous; on a mixed-precision handle it
+ * times the FP32 kernels). No reference counterpart: the tile shapes of the
+ * batched-ensemble form. */
 int oc_set_tiling(oc_handle* h, int32_t mom_levels, int32_t tracer_levels);
 int oc_autotune(oc_handle* h, int32_t* mom_levels, int32_t* tracer_levels);
 

@@ -55,6 +55,21 @@ def test_levels_per_cta_change_no_bit():
         st.close()
 
 
+def test_mixed_autotuned_tiling_changes_no_bit():
+    """On a mixed-precision handle the autotuner times the FP32 kernels; its choice,
+    like a tiling set by hand, leaves every bit of the FP32 step unchanged."""
+    a, b, c = (_member(40, 36, 12, 7, precision="mixed") for _ in range(3))
+    b.set_tiling(3, 5)
+    mk, tk = c.autotune()
+    assert 1 <= mk <= 12 and 1 <= tk <= 12
+    for st in (a, b, c):
+        st.step(4)
+    _same(a, b, "mixed, levels per CTA 3 / 5")
+    _same(a, c, f"mixed, autotuned levels per CTA {mk} / {tk}")
+    for st in (a, b, c):
+        st.close()
+
+
 def test_ensemble_equals_members_stepped_alone():
     from hydrostatic_ocean_core_benchmark_b200.stepper import OceanEnsemble
     together = [_member(*m) for m in MEMBERS]
