@@ -62,3 +62,19 @@ def test_seeded_helmholtz_systems():
         assert not (rhs * (1 - mask)).any()
         a = bench.helmholtz_system(n, 7)
         assert all(np.array_equal(x, y) for x, y in zip(a[2:], (ku, kv, mask, rhs)))
+
+
+def test_profile_traffic_for_every_counted_kernel():
+    """The committed ncu summary gives the DRAM bytes per launch of every kernel the
+    accounting counts (and of the solve), which bench.py reads into its line."""
+    for kernel in list(bench.ACCESSES_PER_CELL) + ["helm_solve"]:
+        t = bench.dram_traffic_from_profiles(kernel)
+        assert t is not None and t > 0, kernel
+    assert bench.dram_traffic_from_profiles("no_such_kernel") is None
+    # the column solves move about twice their algorithmic bytes, the streaming kernels about once
+    n3 = 512 * 512 * 50
+
+    def ratio(k):
+        return bench.dram_traffic_from_profiles(k) / (8 * bench.ACCESSES_PER_CELL[k] * n3)
+
+    assert 1.9 < ratio("momentum_solve") < 2.1 and 0.8 < ratio("backsub") < 1.1
