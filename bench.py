@@ -169,11 +169,17 @@ def helm_bytes_per_iteration(p):
     return 8 * 15 * n0
 
 
-def step_algorithmic_bytes(p, iterations_per_step):
-    """Minimal-pass bytes of one step (44 or 29 accesses per cell + the solver)."""
+def step_algorithmic_bytes(p, iterations_per_step, word=8):
+    """Minimal-pass bytes of one step (44 or 29 accesses per cell + the solver).
+
+    word = 4 counts the mixed-precision step: its 3D fields are FP32, except the
+    buoyancy b, whose accesses (read by the closure and both predictor passes,
+    written by the tracer pass; 3 without the closure) stay 8 B, as do the
+    solver's 2D arrays."""
     n3 = p.nx * p.ny * p.nz
     a3 = 44 if p.closure == "tke" else 29
-    return 8 * a3 * n3 + helm_bytes_per_iteration(p) * iterations_per_step
+    nb = 0 if word == 8 else (4 if p.closure == "tke" else 3)
+    return (word * (a3 - nb) + 8 * nb) * n3 + helm_bytes_per_iteration(p) * iterations_per_step
 
 
 def dram_traffic_from_profiles(kernel: str):
@@ -327,6 +333,15 @@ def precision_leg(s, local_rank, steps, warmup, time_fp64=False, mixed_solver="c
     if time_fp64:
         leg["fp64"] = {"ms_per_step": ms["fp64"], "value": rate["fp64"]}
         leg["speedup_vs_fp64"] = ms["fp64"] / ms["mixed"]
+    if msolver in ("multigrid", "pcg_mg", "pcg_jacobi"):
+        # the mixed step's minimal-pass bytes (FP32 3D fields) over its measured step time,
+        # with the solve's iterations averaged over every step of the run
+        peak, src = measured_hbm_peak()
+        pm = p if msolver == p.solver_kind else p.replace(solver_kind=msolver)
+        bstep = step_algorithmic_bytes(pm, sum(lb) / (warmup + steps), word=4)
+        gbs = bstep / (ms["mixed"] / 1e3) / 1e9
+        leg["step_roofline"] = {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                                "peak_source": src, "algorithmic_bytes_per_step": bstep}
     del out
     torch.cuda.empty_cache()
     return leg

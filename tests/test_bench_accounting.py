@@ -41,6 +41,11 @@ def test_step_bytes_per_cell():
     assert bench.step_algorithmic_bytes(_p(closure="none"), 0) == 8 * 29 * n3 == 232 * n3
     assert (bench.step_algorithmic_bytes(_p(), 22) - bench.step_algorithmic_bytes(_p(), 0)
             == 22 * bench.helm_bytes_per_iteration(_p()))
+    # mixed precision: FP32 3D fields, b and the solver's arrays in fp64
+    assert bench.step_algorithmic_bytes(_p(), 0, word=4) == (4 * 40 + 8 * 4) * n3
+    assert bench.step_algorithmic_bytes(_p(closure="none"), 0, word=4) == (4 * 26 + 8 * 3) * n3
+    assert (bench.step_algorithmic_bytes(_p(), 9, word=4) - bench.step_algorithmic_bytes(_p(), 0, word=4)
+            == 9 * bench.helm_bytes_per_iteration(_p()))
 
 
 def test_refined_solve_bytes():
