@@ -330,18 +330,23 @@ def precision_leg(s, local_rank, steps, warmup, time_fp64=False, mixed_solver="c
            "solver_iterations": {"fp64": sum(la), "mixed": sum(lb), "solves": len(lb)}}
     if msolver == p.solver_kind:
         leg["solver_iterations"]["max_per_solve_difference"] = max((abs(x - y) for x, y in zip(la, lb)), default=0)
+    # minimal-pass bytes of a step over its measured time, the solve's iterations
+    # averaged over every step of the run (FP32 3D fields on the mixed path)
+    peak, src = measured_hbm_peak()
+
+    def step_roofline(pp, log, step_ms, word):
+        bstep = step_algorithmic_bytes(pp, sum(log) / (warmup + steps), word=word)
+        gbs = bstep / (step_ms / 1e3) / 1e9
+        return {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                "peak_source": src, "algorithmic_bytes_per_step": bstep}
+
     if time_fp64:
-        leg["fp64"] = {"ms_per_step": ms["fp64"], "value": rate["fp64"]}
+        leg["fp64"] = {"ms_per_step": ms["fp64"], "value": rate["fp64"],
+                       "step_roofline": step_roofline(p, la, ms["fp64"], 8)}
         leg["speedup_vs_fp64"] = ms["fp64"] / ms["mixed"]
     if msolver in ("multigrid", "pcg_mg", "pcg_jacobi"):
-        # the mixed step's minimal-pass bytes (FP32 3D fields) over its measured step time,
-        # with the solve's iterations averaged over every step of the run
-        peak, src = measured_hbm_peak()
         pm = p if msolver == p.solver_kind else p.replace(solver_kind=msolver)
-        bstep = step_algorithmic_bytes(pm, sum(lb) / (warmup + steps), word=4)
-        gbs = bstep / (ms["mixed"] / 1e3) / 1e9
-        leg["step_roofline"] = {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
-                                "peak_source": src, "algorithmic_bytes_per_step": bstep}
+        leg["step_roofline"] = step_roofline(pm, lb, ms["mixed"], 4)
     del out
     torch.cuda.empty_cache()
     return leg
@@ -366,6 +371,7 @@ def run_precision(args, rank, world, local_rank):
                                    f"theta={p.theta:g} + {p.solver_kind} at rtol {p.rtol:g}, dt={p.dt:g} s",
                        "cells": p.nx * p.ny * p.nz, "rtol": p.rtol, "variant": "precision form (mixed vs fp64)"},
             "fp64": leg["fp64"], "speedup_vs_fp64": leg["speedup_vs_fp64"],
+            "step_roofline": leg.get("step_roofline"),
             "rel_l2_vs_fp64": leg["rel_l2_vs_fp64"], "solvers": leg["solvers"],
             "solver_iterations": leg["solver_iterations"]}
     print(json.dumps(line), flush=True)
