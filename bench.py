@@ -242,31 +242,124 @@ def host_cpu() -> dict:
     return {"nproc": os.cpu_count(), "usable": usable, "cpu_model": model}
 
 
-def reference_sample_nx(args) -> int:
-    """Largest sample (columns per side) whose W + K oracle steps fit ~150 s."""
+def reference_sample_nx(args, budget_s=150.0) -> int:
+    """Largest sample (columns per side) whose W + K oracle steps fit the budget."""
     per_step_64 = 1.1 * args.nz / 50.0          # seconds per step at 64 x 64 columns
     for nx in (128, 96, 64, 48, 32, 16):
-        if per_step_64 * (nx / 64.0) ** 2 * (args.steps + args.warmup) <= 150.0:
+        if per_step_64 * (nx / 64.0) ** 2 * (args.steps + args.warmup) <= budget_s:
             return nx
     return 16
 
 
+def _oracle_replica(cpu_nx, nz, seed, steps, warmup, barrier, out):
+    """One replica of the CPU oracle, in a process of its own: the warm-up steps,
+    a start common to all replicas, then the timed steps on the host's monotonic
+    clock (the same clock in every process)."""
+    import numpy as np
+
+    from hydrostatic_ocean_core_benchmark_b200 import cases
+    from oracle import ocean_oracle as orc
+    s = cases.seamount_basin(nx=cpu_nx, ny=cpu_nx, nz=nz, seed=seed)
+    p = s.params
+    geo = orc.Geometry(p, s.H, s.mask, s.dzr)
+    b = orc.buoyancy(p.eos, s.T, s.S, geo.zc, p.g, p.rho0, p.alpha_t, p.beta_s, p.t0, p.s0) * geo.mask3
+    st = orc.OracleStepper(p, s.H, s.mask, dzr=s.dzr, taux_c=s.taux_c, tauy_c=s.tauy_c)
+    state = orc.OracleState(s.u, s.v, b, s.eta, s.T, s.S)
+    for _ in range(warmup):
+        state = st.step(state)
+    try:
+        barrier.wait(timeout=1800)
+    except Exception:  # another replica failed before the start
+        out.put(None)
+        return
+    t0 = time.monotonic()
+    for _ in range(steps):
+        state = st.step(state)
+    t1 = time.monotonic()
+    out.put((t0, t1, bool(np.all(np.isfinite(state.eta)))))
+
+
+def oracle_replicas(args) -> int:
+    """Replicas of the CPU oracle the host can run at once: one per usable core,
+    within half the available memory (about 200 MB per 64 x 64 x 50 sample)."""
+    cores = host_cpu()["usable"] or 1
+    per_replica = 200e6 * (args.cpu_nx / 64.0) ** 2 * args.nz / 50.0
+    avail = None
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable:"):
+                avail = float(ln.split()[1]) * 1024.0
+                break
+    except OSError:
+        pass
+    by_mem = int(0.5 * avail / per_replica) if avail else cores
+    return max(1, min(cores, by_mem, 128))
+
+
+def cpu_oracle_rate_parallel(args, steps: int, warmup: int, replicas: int):
+    """cell-steps/s of `replicas` independent CPU oracles on the same bounded sample,
+    each single-threaded in a spawned process, timed from the common start to the
+    last replica's end. Returns (aggregate rate, seconds, median replica rate)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(replicas)
+    out = ctx.Queue()
+    keys = ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")
+    saved = {k: os.environ.get(k) for k in keys}
+    os.environ.update({k: "1" for k in keys})  # one thread per replica (the children inherit it)
+    procs = [ctx.Process(target=_oracle_replica, args=(args.cpu_nx, args.nz, args.seed, steps, warmup, barrier, out))
+             for _ in range(replicas)]
+    try:
+        for pr in procs:
+            pr.start()
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    res = []
+    while len(res) < replicas:
+        try:
+            res.append(out.get(timeout=10))
+        except Exception:  # queue.Empty: every replica still alive keeps the wait going
+            if not any(pr.is_alive() for pr in procs):
+                break
+    for pr in procs:
+        pr.join(timeout=60)
+    if len(res) < replicas or any(r is None or not r[2] for r in res):
+        raise RuntimeError(f"CPU oracle replicas failed ({len(res)} of {replicas} reported)")
+    span = max(r[1] for r in res) - min(r[0] for r in res)
+    cells = args.cpu_nx * args.cpu_nx * args.nz
+    single = statistics.median(cells * steps / (r[1] - r[0]) for r in res)
+    return replicas * cells * steps / span, span, single
+
+
 def run_reference_arm(args, rank):
+    """The reference arm: the CPU oracle (a bit-identical NumPy port of the
+    reference's stepper) on every usable host core, one single-threaded replica
+    per core, on a bounded sample of the workload."""
     if rank != 0:
         return 0
-    args.cpu_nx = min(args.cpu_nx, reference_sample_nx(args))
-    rate, secs, p = cpu_oracle_rate(args, args.steps, args.warmup)
-    sample = (f"seamount-basin recipe at {p.nx}x{p.ny}x{p.nz} (same physics, solver and seed "
-              f"as the {args.nx}x{args.ny}x{args.nz} workload), {args.warmup} warm-up + "
-              f"{args.steps} timed steps, {secs:.1f} s")
+    # a single replica's W + K steps fit ~90 s; sharing the host's memory bandwidth
+    # slows each replica (1.4x with 8 replicas on an 8-core host)
+    args.cpu_nx = min(args.cpu_nx, reference_sample_nx(args, budget_s=90.0))
+    replicas = oracle_replicas(args)
+    rate, secs, single = cpu_oracle_rate_parallel(args, args.steps, args.warmup, replicas)
+    n = args.cpu_nx
+    sample = (f"{replicas} replicas (one per usable host core, single-threaded NumPy each) of the "
+              f"seamount-basin recipe at {n}x{n}x{args.nz} (same physics, solver and seed as the "
+              f"{args.nx}x{args.ny}x{args.nz} workload), {args.warmup} warm-up + {args.steps} timed "
+              f"steps each; {secs:.1f} s from the common start to the last replica's end; "
+              f"{single:.4g} cell-steps/s per replica (median)")
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * secs / max(1, args.steps), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"seamount_basin {args.nx}x{args.ny}x{args.nz}",
-                       "sample": f"{p.nx}x{p.ny}x{p.nz}"},
-            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": sample, "host": host_cpu()},
+                       "sample": f"{n}x{n}x{args.nz}", "replicas": replicas},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": replicas, "kind": "port",
+                             "sample": sample, "host": host_cpu(), "per_core_value": single},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -83,3 +83,13 @@ def test_profile_traffic_for_every_counted_kernel():
         return bench.dram_traffic_from_profiles(k) / (8 * bench.ACCESSES_PER_CELL[k] * n3)
 
     assert 1.9 < ratio("momentum_solve") < 2.1 and 0.8 < ratio("backsub") < 1.1
+
+
+def test_reference_arm_replicas_on_the_host_cores():
+    """The reference arm's CPU oracle runs as independent single-threaded replicas in
+    spawned processes; their aggregate rate counts every replica's cell-steps."""
+    args = SimpleNamespace(cpu_nx=16, nz=6, seed=20261203, steps=1, warmup=1)
+    assert 1 <= bench.oracle_replicas(args) <= max(1, bench.host_cpu()["usable"])
+    rate, span, single = bench.cpu_oracle_rate_parallel(args, 1, 1, 2)
+    assert span > 0 and single > 0
+    assert rate == 2 * 16 * 16 * 6 / span
