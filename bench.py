@@ -22,7 +22,8 @@ Multi-GPU: replicas only (the theta step does not shard); each rank advances
 its own replica, ``scaling`` is "weak".
 
 ``--impl reference`` times the reference's own CPU implementation of the path
-(its NumPy stepper, as the bit-identical port) on the host's cores instead.
+(its NumPy stepper, as the bit-identical port) on the host's cores instead: one
+single-threaded replica per usable core, started together, on a bounded sample.
 """
 
 from __future__ import annotations
